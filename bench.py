@@ -1,0 +1,313 @@
+#!/usr/bin/env python
+"""Benchmark of the fused uniform-grid hydro step: zone-updates/s and the HBM roofline fraction.
+
+Workload: the 3D Taylor-Green vortex at 512^3 (periodic [0, 2 pi]^3, rho = 1, p0 = 100,
+gamma = 5/3), PPM + HLLC, float32 state, CFL 0.4 — the configuration the headline metric
+(512^3 HLLC FP32) is quoted on. Synthetic data: the analytic initial condition, generated on the
+host in float64 and rounded once to float32.
+
+  value   zone-updates/s of `--steps` steps with the state resident in HBM, timed with CUDA events
+          on the library's stream (max over ranks; N ranks run N replicas: the single-grid step is
+          not sharded, each GPU advances its own grid).
+  e2e     the same metric through the C ABI with host buffers: upload of the state from pinned
+          host memory, the configuration's full run of 200 steps with the clock read back between
+          batches (shz_run), download of the final state.
+  roofline  the sweep kernel: 64 algorithmic bytes per zone-update (read the float32 state once,
+          write it once) / its mean CUDA-event duration, against the measured HBM copy bandwidth.
+  cpu_baseline  the float64 oracle (a C++ port of the reference's CPU scheme) on a bounded sample
+          of the same workload, on the host's cores.
+
+`--impl reference` times that CPU oracle alone (the reference's own CPU path is TypeScript and has
+no runtime here) and prints its line with "impl": "reference".
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "zone-updates/s (512^3 HLLC FP32)"
+UNIT = "zone-updates/s"
+BYTES_PER_ZU = 64  # read u1, u2 (32 B) + write u1', u2' (32 B) per cell per step
+L2_BYTES = 126 * 2**20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=512, help="cells per side")
+    ap.add_argument("--recon", default="ppm")
+    ap.add_argument("--e2e-steps", type=int, default=200)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload(n: int, recon: str):
+    from shaderous_b200 import Config, Problem
+
+    cfg = Config(n=(n, n, n), dx=2 * math.pi / n, gamma=5 / 3, cfl=0.4, recon=recon, riemann="hllc",
+                 isentropic=(recon != "ppm"))
+    prob = Problem("tgv", a=(1.0, 100.0, 1.0))
+    return cfg, prob
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(recon: str):
+    """Per-cell DRAM traffic of the sweep kernel from the committed ncu summary, if present."""
+    f = ROOT / "profiles" / f"sweep_3d_{recon}.md"
+    if not f.exists():
+        return None
+    m = re.search(r"dram_bytes_per_cell:\s*([0-9.]+)", f.read_text())
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled every 200 ms while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"shz_clocks_{os.getpid()}.csv"
+
+    def __enter__(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.gpu)], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        if self.proc is None or not self.path.exists():
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        try:
+            self.path.unlink()
+        except OSError:
+            pass
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_sample(recon: str, min_seconds: float = 10.0, max_steps: int = 40):
+    """The float64 oracle on a bounded sample of the workload: TGV at 128^3 (the oracle resolution of
+    the configuration), as many steps as fill ~10 s, all host threads."""
+    from oracle.oracle import RefHydro
+    from shaderous_b200 import problem_prims
+
+    n = 128
+    cfg, prob = workload(n, recon)
+    prims = problem_prims(cfg, prob)
+    threads = os.cpu_count() or 1
+    h = RefHydro(n=cfg.n, dx=cfg.dx, gamma=cfg.gamma, bc_lo=(0, 0, 0), bc_hi=(0, 0, 0), cfl=cfg.cfl, limiter=recon,
+                 isentropic=cfg.isentropic and recon != "ppm", threads=threads)
+    h.init_prims(prims)
+    h.step()  # untimed first step (allocations)
+    t0 = time.perf_counter()
+    steps = 0
+    while steps < max_steps and (steps < 2 or time.perf_counter() - t0 < min_seconds):
+        h.step()
+        steps += 1
+    dt = time.perf_counter() - t0
+    return {"value": n ** 3 * steps / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"TGV {n}^3 {recon.upper()}+HLLC, {steps} float64 steps of the C++ oracle (a port of "
+                      f"src/reference/hydro.ts), {threads} threads, {dt:.1f} s"}
+
+
+def run_reference(args, rank, world):
+    """The reference arm: the CPU oracle on the host's cores, one bounded sample step per bench step."""
+    if rank != 0:
+        return
+    from oracle.oracle import RefHydro
+    from shaderous_b200 import problem_prims
+
+    n = 128
+    cfg, prob = workload(n, args.recon)
+    threads = os.cpu_count() or 1
+    h = RefHydro(n=cfg.n, dx=cfg.dx, gamma=cfg.gamma, bc_lo=(0, 0, 0), bc_hi=(0, 0, 0), cfl=cfg.cfl,
+                 limiter=args.recon, isentropic=cfg.isentropic and args.recon != "ppm", threads=threads)
+    h.init_prims(problem_prims(cfg, prob))
+    for _ in range(args.warmup):
+        h.step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        h.step()
+    dt = time.perf_counter() - t0
+    v = n ** 3 * args.steps / dt
+    sample = (f"TGV {n}^3 {args.recon.upper()}+HLLC per step (bounded sample of the {args.n}^3 workload), float64 "
+              f"C++ oracle ported from src/reference/hydro.ts (the TypeScript original has no runtime here), "
+              f"{threads} threads")
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000 * dt / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"taylor-green {args.n}^3 periodic, {args.recon}+hllc, cfl 0.4",
+                       "sample_cells": n ** 3},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    import ctypes as C
+
+    from shaderous_b200 import Sim, problem_prims, prims_to_state
+    from shaderous_b200 import _abi
+
+    cfg, prob = workload(args.n, args.recon)
+    cfg.device = local
+    ncell = cfg.ncell
+    sim = Sim(cfg)
+    sim.reset(prob)
+    lib = sim._lib
+
+    # warm-up: W untimed steps
+    sim.profile(max(args.warmup, 1))
+    sim.sync()
+    if dist:
+        dist.barrier()
+    launches0 = sim.kernel_launches
+    visible = [v for v in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if v.strip()]
+    gpu_index = visible[local] if local < len(visible) else local
+    with ClockSampler(gpu_index) as clocks:
+        prof = sim.profile(args.steps)  # synchronizes on the last event
+    launches = sim.kernel_launches - launches0
+    total_ms = prof["total_ms"]
+    sweep_ms = prof["sweep_ms"]
+    if dist:
+        t = torch.tensor([total_ms, sweep_ms], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms, sweep_ms = float(t[0]), float(t[1])
+    value = ncell * args.steps * world / (total_ms / 1000.0)
+    sweep_avg_s = sweep_ms / args.steps / 1000.0
+    peak, peak_kind = measured_peaks()
+    achieved = BYTES_PER_ZU * ncell / sweep_avg_s / 1e9
+    tr = profile_traffic(args.recon)
+
+    # end to end through the C ABI with pinned host buffers
+    u1_0, u2_0 = prims_to_state(problem_prims(cfg, prob), cfg.gamma)
+    h_in1 = torch.from_numpy(u1_0).pin_memory()
+    h_in2 = torch.from_numpy(u2_0).pin_memory()
+    h_out1 = torch.empty_like(h_in1).pin_memory()
+    h_out2 = torch.empty_like(h_in2).pin_memory()
+    del u1_0, u2_0
+    e2e_steps = args.e2e_steps
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    sim._ok(lib.shz_set_state(sim._h, h_in1.data_ptr(), h_in2.data_ptr(), ncell))
+    sim.set_clock(0.0, 0)
+    res = sim.run(steps=e2e_steps)
+    sim._ok(lib.shz_get_state(sim._h, h_out1.data_ptr(), h_out2.data_ptr(), ncell))
+    e2e_s = time.perf_counter() - t0
+    assert res.taken == e2e_steps, res
+    if dist:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t[0])
+    e2e_value = ncell * e2e_steps * world / e2e_s
+    state_bytes = 2 * ncell * 16
+    if not np.isfinite(h_out1[:: max(1, ncell // 4096)].numpy()).all():
+        raise RuntimeError("non-finite state after the end-to-end run")
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu = cpu_sample(args.recon)
+    sim.destroy()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"taylor-green {args.n}^3 periodic [0,2pi]^3, rho 1, p0 100, gamma 5/3, "
+                               f"{args.recon}+hllc, cfl 0.4",
+                   "cells": ncell, "parallelism": f"replicas x{world}" if world > 1 else "single grid",
+                   "l2": f"inputs larger than L2 ({2 * ncell * 16 / 1e9:.2f} GB state vs {L2_BYTES / 1e6:.0f} MB L2)"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": (tr * ncell) if tr else None, "kernel": "sweep_kernel",
+                     "algorithmic_bytes_per_zu": BYTES_PER_ZU, "peak_source": f"{peak_kind} hbm_gbs",
+                     "sweep_ms_per_step": sweep_ms / args.steps},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": state_bytes / e2e_steps,
+                "d2h_bytes_per_step": (state_bytes + 64 * math.ceil(math.log2(e2e_steps + 1))) / e2e_steps,
+                "steps": e2e_steps, "seconds": e2e_s},
+        "gpu_launches": launches,
+        "clocks": clocks.summary(),
+    }
+    if cpu:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,211 @@
+/*
+ * shaderous_b200 — C ABI of a B200-native compressible-hydro step.
+ *
+ * This is the drop-in boundary for the reference's simulation driver. In the reference
+ * (guillochon/shaderous), TypeScript callers hold a `Simulation` (src/sim.ts:465-628) created by
+ * `createSim` (src/create.ts:58-61) and drive it with `run({steps, until, timeoutMs})`
+ * (src/ui/api.ts:188-210, 538). The functions below are what a Node N-API addon binds in its
+ * place; every one is plain C: POD structs, host pointers and sizes, an int status.
+ *
+ * Conventions
+ *  - Every function returns 0 on success or a negative SHZ_E* code; shz_last_error() gives the
+ *    message of the last failure on a handle (UTF-8, owned by the handle).
+ *  - Host buffers belong to the caller; device memory belongs to the handle. No device pointer
+ *    escapes except through shz_state_device(), documented there.
+ *  - A handle is not re-entrant: callers serialise calls on one handle, as the reference's API
+ *    serialises every call (src/ui/api.ts:1414-1416). Different handles may be used from
+ *    different threads; each owns one CUDA stream.
+ *  - State layout: two float4 arrays per cell, x fastest then y then z, as the reference's
+ *    readState() returns them (src/sim.ts:3790-3808):
+ *      u1 = (rho, rho vx, rho vy, rho vz), u2 = (E, e_int, rho s, solid flag = 0).
+ */
+#ifndef SHADEROUS_B200_H
+#define SHADEROUS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define SHZ_OK 0
+#define SHZ_E_CONFIG (-1)    /* a configuration or argument the library refuses */
+#define SHZ_E_OOM (-2)       /* device memory could not be allocated */
+#define SHZ_E_NAN (-3)       /* the clock became NaN (src/sim.ts:3708; api.ts settle) */
+#define SHZ_E_CUDA (-4)      /* a CUDA call failed; the message names it */
+#define SHZ_E_TIMEOUT (-5)   /* a device-side bounded wait ran out */
+#define SHZ_E_CANCELLED (-6) /* a request was cancelled */
+#define SHZ_E_NODEV (-7)     /* no usable sm_100 device */
+
+/* Boundary codes, as src/problems/boundaries.ts:20-24 and src/reference/hydro.ts:216-220. */
+#define SHZ_BC_PERIODIC 0
+#define SHZ_BC_OUTFLOW 1
+#define SHZ_BC_REFLECT 2
+
+/* Reconstructions: the reference's limiters (src/reference/hydro.ts:30-46) plus PPM. */
+#define SHZ_RECON_MINMOD 0
+#define SHZ_RECON_MC 1
+#define SHZ_RECON_VANLEER 2
+#define SHZ_RECON_KOREN 3
+#define SHZ_RECON_PPM 4 /* Colella & Woodward 1984 edge values; no counterpart in the reference */
+
+#define SHZ_RIEMANN_HLLC 0
+#define SHZ_RIEMANN_HLL 1
+
+/*
+ * Run configuration: the hot-path subset of the reference's SimConfig (src/sim.ts:48-265),
+ * with the reference's defaults from configFor (src/sim.ts:645-742) set by shz_config_default().
+ */
+typedef struct shz_config {
+  int32_t n[3];         /* cells along x, y, z; 1 along a collapsed axis (1D: ny = nz = 1; 2D: nz = 1) */
+  double dx;            /* cell size (the reference's box / n) */
+  double gamma;         /* ideal-gas adiabatic index (src/eos/ideal.wgsl) */
+  int32_t bc_lo[3];     /* SHZ_BC_* per axis, lower face */
+  int32_t bc_hi[3];     /* SHZ_BC_* per axis, upper face */
+  double cfl;           /* Courant number (default 0.8) */
+  double rho_floor;     /* default 1e-10 */
+  double p_floor;       /* default 1e-14 */
+  double eta_dual;      /* dual-energy switch (default 1e-3) */
+  double shock_thresh;  /* shock flag's relative pressure jump (default 0.5) */
+  int32_t riemann;      /* SHZ_RIEMANN_* (default HLLC) */
+  int32_t recon;        /* SHZ_RECON_* (default KOREN) */
+  int32_t isentropic;   /* density along the adiabat (default 1; ignored with PPM) */
+  int32_t signal_dims;  /* multiple of c in the signal rate: 3 as src/reference/hydro.ts:254 (default) */
+  double t_end;         /* the clock stops here (default +inf) */
+  double dt_max;        /* largest step (default +inf) */
+  int32_t device;       /* CUDA device ordinal the handle lives on (default 0) */
+} shz_config;
+
+/* run() options and result, as RunOptions / RunResult (src/ui/api.ts:188-210). */
+typedef struct shz_run_opts {
+  int64_t steps;      /* take at most this many steps; < 0 for no limit */
+  double until;       /* run until the clock reads this time; NaN for none */
+  double timeout_ms;  /* give up after this much wall time; <= 0 for none */
+} shz_run_opts;
+
+#define SHZ_STOP_STEPS 0
+#define SHZ_STOP_TIME 1
+#define SHZ_STOP_END 2
+#define SHZ_STOP_TIMEOUT 3
+
+typedef struct shz_run_result {
+  double t;        /* clock after the call */
+  double dt;       /* step the clock would take next (0 when held at a stop) */
+  int64_t steps;   /* steps taken since the last reset */
+  int64_t taken;   /* steps taken by this call */
+  double seconds;  /* wall time of the call */
+  int32_t stopped; /* SHZ_STOP_* */
+  double last_dt;  /* length of the last step taken */
+} shz_run_result;
+
+/* Conservation totals in float64 (compensated sums), as the reference's Diagnostics
+ * (src/sim.ts:1810-1862, channels of src/hydro/diagnostics.wgsl). dV = dx^ndim. */
+typedef struct shz_diag {
+  double t, dt;
+  int64_t steps;
+  double mass;         /* sum rho dV */
+  double momentum[3];  /* sum rho v dV */
+  double e_kin;        /* sum 1/2 rho v^2 dV */
+  double e_int;        /* sum (E - 1/2 rho v^2) dV */
+  double e_tot;        /* sum E dV */
+  double max_mach;     /* max |v| / c */
+  double floored;      /* cells at the density or pressure floor */
+} shz_diag;
+
+/* Built-in problems, initialised on the host in float64 at cell centres (box centred on 0, as
+ * src/reference/hydro.ts:200 and src/domain.ts:15) and rounded once to float32. */
+#define SHZ_PROB_SOD 0       /* shock tube along `axis`: left (a[0..2] = rho,u,p) for x<0, right (a[3..5]); s = 1 on the left */
+#define SHZ_PROB_KH 1        /* Kelvin-Helmholtz slab: rho_in a[0], rho_out a[1], v a[2], p a[3], kick a[4], noise sigma a[5] */
+#define SHZ_PROB_TGV 2       /* Taylor-Green vortex on [0, 2 pi]^3: rho a[0], p0 a[1], amplitude a[2] */
+#define SHZ_PROB_SEDOV 3     /* point blast: rho a[0], p a[1], energy a[2], radius in cells a[3] */
+#define SHZ_PROB_ADVECT 4    /* smooth density wave: rho = a[0] + a[1] sin(2 pi x / L), v = (a[2], a[3], a[4]), p = a[5] */
+#define SHZ_PROB_BLAST 5     /* pressure sphere: rho_in a[0], p_in a[1], rho_out a[2], p_out a[3], radius (box units) a[4] */
+#define SHZ_PROB_GAUSS 6     /* gaussian pulse in 3D: rho = a[0] + exp(-r2/a[1]), v = (a[2],a[3],a[4]) , p = a[5] + 0.5 exp(-r2/a[6]) */
+
+typedef struct shz_problem {
+  int32_t kind;    /* SHZ_PROB_* */
+  int32_t axis;    /* SOD: normal axis */
+  uint64_t seed;   /* KH noise */
+  double a[8];     /* parameters, per kind above */
+} shz_problem;
+
+typedef struct shz_sim shz_sim;
+
+/* Fill `cfg` with the reference's defaults for an n[0] x n[1] x n[2] grid of cell size dx. */
+int shz_config_default(shz_config* cfg, int32_t nx, int32_t ny, int32_t nz, double dx);
+
+/* Replaces createSim / Sim.create (src/create.ts:58-61, src/sim.ts:2283): validates the
+ * configuration, allocates the device state and builds the step. */
+int shz_create(const shz_config* cfg, shz_sim** out);
+
+/* Replaces Simulation.destroy (src/sim.ts:465-628). */
+void shz_destroy(shz_sim* sim);
+
+/* Message of the last failure on `sim` (or of the last shz_create failure when sim is NULL). */
+const char* shz_last_error(const shz_sim* sim);
+
+/* Replaces Sim.reset with a built-in problem (src/sim.ts:2704-2848): the clock goes to 0. */
+int shz_reset_problem(shz_sim* sim, const shz_problem* prob);
+
+/* Host float64 primitives (rho, vx, vy, vz, p, s per cell, x fastest) of planes k0..k1-1 of a
+ * problem on the grid of `cfg`: the same numbers shz_reset_problem() rounds to float32. */
+int shz_problem_prims(const shz_config* cfg, const shz_problem* prob, int32_t k0, int32_t k1, double* prims);
+
+/* Replaces Simulation.setState (src/sim.ts:3031): host float32 state, `ncell` cells, layout above.
+ * Keeps the clock. */
+int shz_set_state(shz_sim* sim, const float* u1, const float* u2, size_t ncell);
+
+/* Replaces Simulation.readState (src/sim.ts:3790-3808): copies the state into host buffers. */
+int shz_get_state(shz_sim* sim, float* u1, float* u2, size_t ncell);
+
+/* Replaces encodeSteps + submit (src/sim.ts:3187-3328): enqueue `n` steps; returns at once.
+ * Steps past t_end hold the clock (dt = 0) and leave the state as it is. */
+int shz_step(shz_sim* sim, int32_t n);
+
+/* Replaces run() (src/ui/api.ts:538): steps until `steps`, `until` or the timeout, whichever
+ * comes first; the step that reaches `until` is shortened to land on it. Blocking. */
+int shz_run(shz_sim* sim, const shz_run_opts* opts, shz_run_result* res);
+
+/* Replaces readDiagnostics (src/sim.ts:3602-3650). Blocking. */
+int shz_diagnostics(shz_sim* sim, shz_diag* out);
+
+/* The device clock (src/hydro/common.wgsl Clock): t, the next dt and the steps taken. Blocking. */
+int shz_clock(shz_sim* sim, double* t, double* dt, int64_t* steps);
+
+/* Set the clock (a restart, RestartState src/sim.ts:1865). */
+int shz_set_clock(shz_sim* sim, double t, int64_t steps);
+
+/* Change the stop time t_end (the reference's writeParams with cfg.tEnd). */
+int shz_set_t_end(shz_sim* sim, double t_end);
+
+/* Wait for the handle's queued work. */
+int shz_sync(shz_sim* sim);
+
+/* Device pointers of the current state (two float4 arrays, layout above), valid until the next
+ * step or destroy; for callers that keep data on the device (benchmarks, interop). */
+int shz_state_device(shz_sim* sim, void** u1, void** u2);
+
+/* Per-pass timing of `n` steps with CUDA events on the handle's stream, as the reference's
+ * Sim.profile(reps) (src/sim.ts:3541) and its per-pass timestamps (src/gpu/timing.ts:232):
+ * total device time of the steps, and the summed time of the sweep kernels alone. Blocking. */
+typedef struct shz_profile_result {
+  int32_t steps;
+  double total_ms;   /* first clock kernel's start to last sweep's end */
+  double sweep_ms;   /* sum over the n sweeps of each sweep's own duration */
+  int64_t launches;  /* kernels launched for the n steps */
+} shz_profile_result;
+int shz_profile(shz_sim* sim, int32_t n, shz_profile_result* out);
+
+/* Launches of the library's own kernels on this handle since creation. */
+int64_t shz_kernel_launches(const shz_sim* sim);
+
+/* Library version string. */
+const char* shz_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SHADEROUS_B200_H */

@@ -1,0 +1,133 @@
+"""ctypes declarations of the C ABI in ``include/shaderous_b200.h``.
+
+The library is loaded from the package directory (built in-tree by ``shaderous_b200.build``).
+There is no fallback: if the shared library is missing or fails to load, importing the
+simulation API raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libshaderous_b200.so"
+
+SHZ_OK = 0
+SHZ_E_CONFIG = -1
+SHZ_E_OOM = -2
+SHZ_E_NAN = -3
+SHZ_E_CUDA = -4
+SHZ_E_TIMEOUT = -5
+SHZ_E_CANCELLED = -6
+SHZ_E_NODEV = -7
+
+BC_PERIODIC, BC_OUTFLOW, BC_REFLECT = 0, 1, 2
+RECON = {"minmod": 0, "mc": 1, "vanleer": 2, "koren": 3, "ppm": 4}
+RIEMANN = {"hllc": 0, "hll": 1}
+PROBLEM = {"sod": 0, "kh": 1, "tgv": 2, "sedov": 3, "advect": 4, "blast": 5, "gauss": 6}
+STOPPED = {0: "steps", 1: "time", 2: "end", 3: "timeout"}
+
+
+class shz_config(C.Structure):
+    _fields_ = [
+        ("n", C.c_int32 * 3),
+        ("dx", C.c_double),
+        ("gamma", C.c_double),
+        ("bc_lo", C.c_int32 * 3),
+        ("bc_hi", C.c_int32 * 3),
+        ("cfl", C.c_double),
+        ("rho_floor", C.c_double),
+        ("p_floor", C.c_double),
+        ("eta_dual", C.c_double),
+        ("shock_thresh", C.c_double),
+        ("riemann", C.c_int32),
+        ("recon", C.c_int32),
+        ("isentropic", C.c_int32),
+        ("signal_dims", C.c_int32),
+        ("t_end", C.c_double),
+        ("dt_max", C.c_double),
+        ("device", C.c_int32),
+    ]
+
+
+class shz_run_opts(C.Structure):
+    _fields_ = [("steps", C.c_int64), ("until", C.c_double), ("timeout_ms", C.c_double)]
+
+
+class shz_run_result(C.Structure):
+    _fields_ = [
+        ("t", C.c_double),
+        ("dt", C.c_double),
+        ("steps", C.c_int64),
+        ("taken", C.c_int64),
+        ("seconds", C.c_double),
+        ("stopped", C.c_int32),
+        ("last_dt", C.c_double),
+    ]
+
+
+class shz_diag(C.Structure):
+    _fields_ = [
+        ("t", C.c_double),
+        ("dt", C.c_double),
+        ("steps", C.c_int64),
+        ("mass", C.c_double),
+        ("momentum", C.c_double * 3),
+        ("e_kin", C.c_double),
+        ("e_int", C.c_double),
+        ("e_tot", C.c_double),
+        ("max_mach", C.c_double),
+        ("floored", C.c_double),
+    ]
+
+
+class shz_problem(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("axis", C.c_int32), ("seed", C.c_uint64), ("a", C.c_double * 8)]
+
+
+class shz_profile_result(C.Structure):
+    _fields_ = [("steps", C.c_int32), ("total_ms", C.c_double), ("sweep_ms", C.c_double), ("launches", C.c_int64)]
+
+
+# (name, restype, argtypes): every entry point declared in include/shaderous_b200.h
+SIGNATURES = [
+    ("shz_config_default", C.c_int, [C.POINTER(shz_config), C.c_int32, C.c_int32, C.c_int32, C.c_double]),
+    ("shz_create", C.c_int, [C.POINTER(shz_config), C.POINTER(C.c_void_p)]),
+    ("shz_destroy", None, [C.c_void_p]),
+    ("shz_last_error", C.c_char_p, [C.c_void_p]),
+    ("shz_reset_problem", C.c_int, [C.c_void_p, C.POINTER(shz_problem)]),
+    ("shz_problem_prims", C.c_int, [C.POINTER(shz_config), C.POINTER(shz_problem), C.c_int32, C.c_int32, C.c_void_p]),
+    ("shz_set_state", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t]),
+    ("shz_get_state", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t]),
+    ("shz_step", C.c_int, [C.c_void_p, C.c_int32]),
+    ("shz_run", C.c_int, [C.c_void_p, C.POINTER(shz_run_opts), C.POINTER(shz_run_result)]),
+    ("shz_diagnostics", C.c_int, [C.c_void_p, C.POINTER(shz_diag)]),
+    ("shz_clock", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
+    ("shz_set_clock", C.c_int, [C.c_void_p, C.c_double, C.c_int64]),
+    ("shz_set_t_end", C.c_int, [C.c_void_p, C.c_double]),
+    ("shz_sync", C.c_int, [C.c_void_p]),
+    ("shz_state_device", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
+    ("shz_profile", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(shz_profile_result)]),
+    ("shz_kernel_launches", C.c_int64, [C.c_void_p]),
+    ("shz_version", C.c_char_p, []),
+]
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Load the in-tree library (raises OSError if it is not built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise OSError(f"{LIB_PATH} is not built: run `python -m shaderous_b200.build`")
+        lib = C.CDLL(str(LIB_PATH))
+        for name, res, args in SIGNATURES:
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+NAN = math.nan

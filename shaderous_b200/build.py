@@ -1,0 +1,81 @@
+"""Build the in-tree shared libraries.
+
+- ``shaderous_b200/libshaderous_b200.so``: the CUDA kernels (sm_100a) and the C ABI of
+  ``include/shaderous_b200.h``, compiled with nvcc.
+- ``oracle/liboracle.so``: the float64 CPU oracle (test infrastructure only), compiled with g++.
+
+Run ``python -m shaderous_b200.build`` or call :func:`build_all`.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent.parent
+PKG = ROOT / "shaderous_b200"
+CSRC = PKG / "csrc"
+LIB = PKG / "libshaderous_b200.so"
+ORACLE_DIR = ROOT / "oracle"
+ORACLE_LIB = ORACLE_DIR / "liboracle.so"
+
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def _sources() -> list[Path]:
+    return sorted(list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cpp")))
+
+
+def _headers() -> list[Path]:
+    return sorted(list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + list((ROOT / "include").glob("*.h")))
+
+
+def _stale(target: Path, deps: list[Path]) -> bool:
+    if not target.exists():
+        return True
+    t = target.stat().st_mtime
+    return any(d.stat().st_mtime > t for d in deps)
+
+
+def build_library(force: bool = False, verbose: bool = False) -> Path:
+    srcs = _sources()
+    if not force and not _stale(LIB, srcs + _headers() + [Path(__file__)]):
+        return LIB
+    obj_dir = PKG / "_build"
+    obj_dir.mkdir(exist_ok=True)
+    objs = []
+    for src in srcs:
+        obj = obj_dir / (src.stem + ".o")
+        cmd = [NVCC, "-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC,-fopenmp,-O3",
+               "-I", str(ROOT / "include"), "-c", str(src), "-o", str(obj)]
+        if src.suffix == ".cu":
+            cmd[1:1] = ["-Xptxas", "-v"] if verbose else []
+        else:
+            cmd[1:1] = ["-x", "cu"]
+        subprocess.run(cmd, check=True)
+        objs.append(str(obj))
+    tmp = LIB.with_suffix(".so.tmp")
+    subprocess.run([NVCC, "-shared", *ARCH, "-o", str(tmp), *objs, "-Xcompiler", "-fopenmp", "-lgomp"], check=True)
+    os.replace(tmp, LIB)
+    return LIB
+
+
+def build_oracle(force: bool = False) -> Path:
+    src = ORACLE_DIR / "ref_hydro.cpp"
+    if not force and not _stale(ORACLE_LIB, [src, Path(__file__)]):
+        return ORACLE_LIB
+    tmp = ORACLE_LIB.with_suffix(".so.tmp")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-fopenmp", "-fPIC", "-shared", "-o", str(tmp), str(src)], check=True)
+    os.replace(tmp, ORACLE_LIB)
+    return ORACLE_LIB
+
+
+def build_all(force: bool = False, verbose: bool = False) -> None:
+    build_oracle(force)
+    build_library(force, verbose)
+
+
+if __name__ == "__main__":
+    build_all(force="--force" in sys.argv, verbose="-v" in sys.argv)

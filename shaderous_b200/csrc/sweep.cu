@@ -1,0 +1,707 @@
+// The uniform-grid hydro step as one fused kernel per step, plus its clock, rate and
+// diagnostics kernels.
+//
+// One step of the reference (src/sim.ts:3187-3328 encodeSteps) is four passes: rates
+// (hydro/rates.wgsl), the dt reduction and clock (gpu/reduce.wgsl, hydro/clock.wgsl), the
+// Hancock predictor (hydro/predict.wgsl -> predictor.wgsl) and the update
+// (hydro/update.wgsl -> tile.wgsl, flux.wgsl, riemann/hllc.wgsl, advance.wgsl, dual_energy.wgsl).
+// Here a step is clock_kernel (one thread: dt from the last sweep's rate maximum, the float64
+// clock advanced) and sweep_kernel, which reads each cell's conserved state once and in one
+// pass recovers primitives, forms limited edge increments, takes the Hancock half step, solves
+// each face's Riemann problem once, applies the conservative update with the dual-energy
+// switch, writes the new state, and folds the new state's signal rate into the next step's
+// maximum (warp shuffles, then one atomicMax per CTA on the float's bits).
+//
+// Decomposition: a CTA owns a TX x TY column of cells and marches it along z through TZ planes
+// (2.5D). Its threads are the (TX+2) x (TY+2) cells of the column plus one ring of halo cells;
+// each thread keeps the primitives of its own column for the planes the predictor reads along
+// z in registers, so z-neighbours and z-faces never touch shared memory. Per plane, the
+// primitives of the column plus the halo of the stencil go to shared memory for the x/y
+// neighbours; the face states toward the upper x and y faces go to shared memory so that the
+// next thread can solve its lower face; each face flux is computed once and used by both
+// cells, so both sides see bit-identical fluxes (the reference's flux-determinism check,
+// src/validation/tests.ts:961).
+//
+// The arithmetic follows the reference's CPU scheme, src/reference/hydro.ts (RefHydro), in
+// float32: a cell beyond a boundary takes the half-step state and flags of the cell it maps to
+// (mirrored for a reflecting wall) with edge increments recomputed at the ghost position
+// (hydro.ts:329-358). Collapsed axes (n = 1) carry no faces: in the reference their two faces
+// carry equal fluxes that cancel.
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+
+#include "hydro_math.cuh"
+#include "sweep.h"
+
+namespace shz {
+
+template <int DIM, int RECON>
+struct Geo {
+  static constexpr int H = (RECON == R_PPM) ? 3 : 2;   // halo of the primitives' region
+  static constexpr int ZH = (RECON == R_PPM) ? 2 : 1;  // planes each way the predictor reads along z
+  static constexpr int ZW = 2 * ZH + 1;                // planes held per thread
+  static constexpr int TX = (DIM == 1) ? 126 : 16;
+  static constexpr int TY = (DIM == 1) ? 1 : 16;
+  static constexpr int TZ = (DIM == 3) ? 64 : 1;
+  static constexpr int PX = TX + 2;
+  static constexpr int PY = (DIM >= 2) ? TY + 2 : 1;
+  static constexpr int NT = PX * PY;
+  static constexpr int PN = PX * PY;
+  static constexpr int WX = TX + 2 * H;
+  static constexpr int WY = (DIM >= 2) ? TY + 2 * H : 1;
+  static constexpr int WN = WX * WY;
+  static constexpr int NBUF = (DIM == 3) ? ZH + 1 : 1;
+  static constexpr int NF = (DIM >= 2) ? 2 : 1;  // in-plane face directions
+  static constexpr size_t SMEM_FLOATS = (size_t)NBUF * 7 * WN + (size_t)NF * 7 * PN + (size_t)NF * 8 * PN + 32;
+  static constexpr size_t SMEM_BYTES = SMEM_FLOATS * sizeof(float);
+};
+
+// Primitives of one plane of the CTA's region (column plus stencil halo) into shared memory,
+// through the boundary mapping.
+template <int DIM, int RECON>
+__device__ __forceinline__ void load_w_plane(const KParams& P, const float4* __restrict__ u1, const float4* __restrict__ u2,
+                                             int x0, int y0, int plane, float* __restrict__ sWb) {
+  using G = Geo<DIM, RECON>;
+  float fz = 1.f;
+  const int gz = (DIM == 3) ? bc_map(plane, P.n[2], P.bc_lo[2], P.bc_hi[2], fz) : 0;
+  const size_t zoff = (size_t)gz * P.n[1] * P.n[0];
+  for (int idx = threadIdx.x; idx < G::WN; idx += G::NT) {
+    const int lx = idx % G::WX, ly = idx / G::WX;
+    float fx, fy = 1.f;
+    const int gx = bc_map(x0 - G::H + lx, P.n[0], P.bc_lo[0], P.bc_hi[0], fx);
+    const int gy = (DIM >= 2) ? bc_map(y0 - G::H + ly, P.n[1], P.bc_lo[1], P.bc_hi[1], fy) : 0;
+    const size_t o = zoff + (size_t)gy * P.n[0] + gx;
+    const float4 a = __ldg(u1 + o), b = __ldg(u2 + o);
+    float w[7];
+    prim_from_cons(a, b, P, fx, fy, fz, w);
+#pragma unroll
+    for (int c = 0; c < 7; c++) sWb[c * G::WN + idx] = w[c];
+  }
+}
+
+template <int DIM, int RECON>
+__device__ __forceinline__ void read_w(const float* __restrict__ sWb, int wx, int wy, float* w) {
+  using G = Geo<DIM, RECON>;
+#pragma unroll
+  for (int c = 0; c < 7; c++) w[c] = sWb[c * G::WN + wy * G::WX + wx];
+}
+
+// The per-cell result of the predictor (hydro.ts:272-322 predictRaw): the half-step state q,
+// the shock flag and the first-order flag.
+struct Pred {
+  float q[6];
+  float flag;
+  bool fo;
+};
+
+// hydro.ts:294-321: slopes -> shock flag -> Hancock half step -> positivity fallback, given the
+// edge increments su/sd per active axis and the convergence and pressure jump the neighbours give.
+template <int DIM>
+__device__ __forceinline__ void hancock(const float* c, float conv, float jump, const float (*su)[6], const float (*sd)[6],
+                                        float h, const KParams& P, Pred& out) {
+  float big = 0.f, fall = 0.f, dv = 0.f;
+  float adv[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  float gradp[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+  for (int a = 0; a < DIM; a++) {
+    big = fmaxf(big, fmaxf(fabsf(su[a][4]), fabsf(sd[a][4])));
+    fall = fminf(fall, fminf(0.5f * su[a][0], -0.5f * sd[a][0]));
+    const float va = c[1 + a];
+#pragma unroll
+    for (int v = 0; v < 6; v++) adv[v] += va * (0.5f * (su[a][v] + sd[a][v]));
+    dv += 0.5f * (su[a][1 + a] + sd[a][1 + a]);
+    gradp[a] = 0.5f * (su[a][4] + sd[a][4]);
+  }
+  out.flag = (conv < 0.f && jump > P.shock_thresh) ? 1.f : 0.f;
+  const float rho = c[0], cs = c[6];
+  const float inv_rho = 1.f / rho;
+  float qh[6];
+  qh[0] = rho - h * (adv[0] + rho * dv);
+#pragma unroll
+  for (int d = 0; d < 3; d++) qh[1 + d] = c[1 + d] - h * (adv[1 + d] + gradp[d] * inv_rho);
+  qh[4] = c[4] - h * (adv[4] + rho * cs * cs * dv);
+  qh[5] = c[5] - h * adv[5];
+  const float rmin = qh[0] + fall;
+  const float pmin = qh[4] - 0.5f * big;
+  out.fo = !(rmin > 0.f && pmin > 0.f);
+#pragma unroll
+  for (int v = 0; v < 6; v++) out.q[v] = out.fo ? c[v] : qh[v];
+}
+
+// Face state q + 0.5 sgn inc (q alone when first order), with the cell's shock flag
+// (hydro.ts:362 side's f(n)).
+__device__ __forceinline__ void face_state(const Pred& pr, const float* inc, float sgn, float* f) {
+#pragma unroll
+  for (int v = 0; v < 6; v++) f[v] = pr.fo ? pr.q[v] : pr.q[v] + 0.5f * sgn * inc[v];
+  f[6] = pr.flag;
+}
+
+// The update of one cell (hydro.ts:422-446): conservative update, dual-energy switch and floors.
+// acc = (dm, dmx, dmy, dmz, de, dei, ds, dvn) summed with the reference's signs; ph = the
+// cell's half-step pressure.
+__device__ __forceinline__ void update_cell(const float4 a, const float4 b, const float* acc, float ph, float dtdx,
+                                            const KParams& P, float4& na, float4& nb) {
+  const float rho = fmaxf(a.x + dtdx * acc[0], P.rho_floor);
+  const float mx = a.y + dtdx * acc[1], my = a.z + dtdx * acc[2], mz = a.w + dtdx * acc[3];
+  float E = b.x + dtdx * acc[4];
+  float eint = b.y + dtdx * (acc[5] + fmaxf(ph, P.p_floor) * acc[7]);
+  const float ke = (0.5f * (mx * mx + my * my + mz * mz)) / rho;
+  const float eth = E - ke;
+  const float emin = P.e_floor;
+  if (eth > P.eta_dual * E && eth >= emin) {
+    eint = eth;
+  } else {
+    if (!(eint >= emin)) eint = emin;
+    E = ke + eint;
+  }
+  na = make_float4(rho, mx, my, mz);
+  nb = make_float4(E, eint, b.z + dtdx * acc[6], b.w);
+}
+
+__device__ __forceinline__ float warp_max(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Block maximum of a non-negative rate into *out (as the float's bits: non-negative floats
+// order as unsigned integers; a NaN orders above every finite rate, which the clock reports).
+// fmaxf drops NaN operands, so a NaN rate is carried as +inf bits through the shuffles.
+template <int NT>
+__device__ __forceinline__ void block_max_to(float v, float* sRed, unsigned* out) {
+  v = warp_max(v);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) sRed[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    constexpr int NW = (NT + 31) / 32;
+    float m = lane < NW ? sRed[lane] : 0.f;
+    m = warp_max(m);
+    if (lane == 0) atomicMax(out, __float_as_uint(m));
+  }
+}
+
+__device__ __forceinline__ float rate_guard(float r) { return (r == r) ? r : __int_as_float(0x7f800000); }
+
+template <int DIM, int RECON, bool ISEN>
+__global__ void __launch_bounds__(Geo<DIM, RECON>::NT, 1)
+    sweep_kernel(const KParams P, const float4* __restrict__ u1, const float4* __restrict__ u2, float4* __restrict__ o1,
+                 float4* __restrict__ o2, const DevClock* __restrict__ clk, unsigned* __restrict__ rate_out) {
+  using G = Geo<DIM, RECON>;
+  constexpr int H = G::H, ZH = G::ZH, ZW = G::ZW, PX = G::PX, PN = G::PN;
+  extern __shared__ __align__(16) float smem[];
+  float* sW = smem;
+  float* sFace = sW + G::NBUF * 7 * G::WN;
+  float* sFlux = sFace + G::NF * 7 * PN;
+  float* sRed = sFlux + G::NF * 8 * PN;
+
+  const int tid = threadIdx.x;
+  const int tx = tid % PX, ty = tid / PX;
+  const int x0 = blockIdx.x * G::TX, y0 = blockIdx.y * G::TY;
+  const int gx = x0 - 1 + tx, gy = (DIM >= 2) ? y0 - 1 + ty : 0;
+  const int wx = tx + H - 1, wy = (DIM >= 2) ? ty + H - 1 : 0;
+  const int nx = P.n[0], ny = P.n[1], nz = P.n[2];
+  // Roles: tile_t updates cell (gx, gy); row_t / col_t: the row / column lies in the tile.
+  const bool row_t = (DIM < 2) || (ty >= 1 && ty <= G::TY && gy < ny);
+  const bool col_t = tx >= 1 && tx <= G::TX && gx < nx;
+  const bool tile_t = row_t && col_t;
+  const bool xface_t = row_t && tx >= 1 && tx <= G::TX + 1 && gx <= nx;  // solves the x face below gx
+  const bool yface_t = (DIM >= 2) && col_t && ty >= 1 && ty <= G::TY + 1 && gy <= ny;
+
+  const double dt = clk->dt;
+  const float dtdx = (float)(dt / P.dx);
+  const float h = (float)((0.5 * dt) / P.dx);
+  float rate_max = 0.f;
+
+  // A step held at the stop time (dt = 0) leaves the state as it is (clock.wgsl:120-125).
+  if (clk->held) {
+    const int zb = (DIM == 3) ? blockIdx.z * G::TZ : 0;
+    const int ze = (DIM == 3) ? min(zb + G::TZ, nz) : 1;
+    for (int idx = tid; idx < G::TX * G::TY; idx += G::NT) {
+      const int cx = x0 + idx % G::TX, cy = (DIM >= 2) ? y0 + idx / G::TX : 0;
+      if (cx >= nx || cy >= ny) continue;
+      for (int z = zb; z < ze; z++) {
+        const size_t o = ((size_t)z * ny + cy) * nx + cx;
+        const float4 a = u1[o], b = u2[o];
+        o1[o] = a;
+        o2[o] = b;
+        rate_max = fmaxf(rate_max, rate_guard(signal_rate(a, b, P)));
+      }
+    }
+    block_max_to<G::NT>(rate_max, sRed, rate_out);
+    return;
+  }
+
+  // Ghost cells across an outflow or reflecting x/y boundary take their half-step state from
+  // the adjacent inner cell (hydro.ts:335-342); whether this CTA has any is CTA-uniform.
+  const bool xg_lo = x0 == 0 && P.bc_lo[0] != 0;
+  const bool xg_hi = x0 + G::TX >= nx && P.bc_hi[0] != 0;
+  const bool yg_lo = (DIM >= 2) && y0 == 0 && P.bc_lo[1] != 0;
+  const bool yg_hi = (DIM >= 2) && y0 + G::TY >= ny && P.bc_hi[1] != 0;
+  const bool xyg = xg_lo || xg_hi || yg_lo || yg_hi;
+  int g_src = -1, g_axis = 0;
+  bool g_flip = false;
+  if (xg_lo && gx == -1 && row_t) { g_src = tid + 1; g_axis = 0; g_flip = P.bc_lo[0] == 2; }
+  if (xg_hi && gx == nx && row_t) { g_src = tid - 1; g_axis = 0; g_flip = P.bc_hi[0] == 2; }
+  if (DIM >= 2 && yg_lo && gy == -1 && col_t) { g_src = tid + PX; g_axis = 1; g_flip = P.bc_lo[1] == 2; }
+  if (DIM >= 2 && yg_hi && gy == ny && col_t) { g_src = tid - PX; g_axis = 1; g_flip = P.bc_hi[1] == 2; }
+
+  const int z0 = (DIM == 3) ? blockIdx.z * G::TZ : 0;
+  const int z1 = (DIM == 3) ? min(z0 + G::TZ, nz) : 1;
+  auto buf = [&](int plane) -> float* {
+    return sW + (((plane % G::NBUF) + G::NBUF) % G::NBUF) * 7 * G::WN;
+  };
+
+  float zw[ZW][7];        // own column's primitives, planes j-ZH .. j+ZH
+  float zhi_prev[7];      // face state below the upper z face of plane j-1
+  float q_prev[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  float flag_prev = 0.f;
+  bool fo_prev = false;
+  float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  float ph_prev = 0.f;
+  float gsu[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // edges of the lower z ghost (outflow / reflect)
+#pragma unroll
+  for (int v = 0; v < 7; v++) zhi_prev[v] = 0.f;
+
+  if constexpr (DIM == 3) {
+    for (int pl = z0 - 1 - ZH; pl <= z0 - 2 + ZH; pl++) {
+      load_w_plane<DIM, RECON>(P, u1, u2, x0, y0, pl, buf(pl));
+      __syncthreads();
+#pragma unroll
+      for (int s = 0; s < ZW - 1; s++)
+#pragma unroll
+        for (int v = 0; v < 7; v++) zw[s][v] = zw[s + 1][v];
+      read_w<DIM, RECON>(buf(pl), wx, wy, zw[ZW - 1]);
+    }
+  }
+
+  const int jb = (DIM == 3) ? z0 - 1 : 0;
+  const int je = (DIM == 3) ? z1 : 0;
+  for (int j = jb; j <= je; j++) {
+    // 1. primitives of plane j + ZH (the plane itself when there is no march)
+    const int lp = (DIM == 3) ? j + ZH : 0;
+    load_w_plane<DIM, RECON>(P, u1, u2, x0, y0, lp, buf(lp));
+    __syncthreads();
+    float c[7];
+    if constexpr (DIM == 3) {
+#pragma unroll
+      for (int s = 0; s < ZW - 1; s++)
+#pragma unroll
+        for (int v = 0; v < 7; v++) zw[s][v] = zw[s + 1][v];
+      read_w<DIM, RECON>(buf(lp), wx, wy, zw[ZW - 1]);
+#pragma unroll
+      for (int v = 0; v < 7; v++) c[v] = zw[ZH][v];
+    } else {
+      read_w<DIM, RECON>(buf(0), wx, wy, c);
+    }
+
+    if constexpr (DIM == 3) {
+      // The lower z ghost plane (outflow / reflect): only its edges toward the domain, at the
+      // ghost position; its half-step state is plane 0's, taken below.
+      if (j == -1 && P.bc_lo[2] != 0) {
+        float sd_unused[6];
+        axis_edges<RECON, ISEN>(zw[ZH >= 2 ? ZH - 2 : 0], zw[ZH - 1], zw[ZH], zw[ZH + 1], zw[ZH >= 2 ? ZH + 2 : ZW - 1],
+                                P.inv_gamma, gsu, sd_unused);
+        continue;
+      }
+      // The upper z ghost plane: plane nz-1's half-step state with edges at the ghost position.
+      if (j == nz && P.bc_hi[2] != 0) {
+        float su_unused[6], gsd[6];
+        axis_edges<RECON, ISEN>(zw[ZH >= 2 ? ZH - 2 : 0], zw[ZH - 1], zw[ZH], zw[ZH + 1], zw[ZH >= 2 ? ZH + 2 : ZW - 1],
+                                P.inv_gamma, su_unused, gsd);
+        if (tile_t) {
+          Pred g;
+#pragma unroll
+          for (int v = 0; v < 6; v++) g.q[v] = q_prev[v];
+          if (P.bc_hi[2] == 2) g.q[3] = -g.q[3];
+          g.flag = flag_prev;
+          g.fo = fo_prev;
+          float zlo[7], Fz[8];
+          face_state(g, gsd, -1.f, zlo);
+          riemann<2>(zhi_prev, zlo, P, Fz);
+#pragma unroll
+          for (int v = 0; v < 8; v++) acc[v] -= Fz[v];
+          const size_t o = ((size_t)(j - 1) * ny + gy) * nx + gx;
+          float4 na, nb;
+          update_cell(__ldg(u1 + o), __ldg(u2 + o), acc, ph_prev, dtdx, P, na, nb);
+          o1[o] = na;
+          o2[o] = nb;
+          rate_max = fmaxf(rate_max, rate_guard(signal_rate(na, nb, P)));
+        }
+        continue;
+      }
+    }
+
+    // 2. predictor at plane j: edges per active axis, shock flag, Hancock half step.
+    float su[DIM][6], sd[DIM][6];
+    float conv = 0.f, jump = 0.f;
+    {
+      const float* sWj = buf((DIM == 3) ? j : 0);
+      float m[7], p[7], m2[7], p2[7];
+      read_w<DIM, RECON>(sWj, wx - 1, wy, m);
+      read_w<DIM, RECON>(sWj, wx + 1, wy, p);
+      if constexpr (RECON == R_PPM) {
+        read_w<DIM, RECON>(sWj, wx - 2, wy, m2);
+        read_w<DIM, RECON>(sWj, wx + 2, wy, p2);
+      }
+      axis_edges<RECON, ISEN>(m2, m, c, p, p2, P.inv_gamma, su[0], sd[0]);
+      conv += p[1] - m[1];
+      jump = fmaxf(jump, fabsf(p[4] - m[4]) / fminf(p[4], m[4]));
+      if constexpr (DIM >= 2) {
+        read_w<DIM, RECON>(sWj, wx, wy - 1, m);
+        read_w<DIM, RECON>(sWj, wx, wy + 1, p);
+        if constexpr (RECON == R_PPM) {
+          read_w<DIM, RECON>(sWj, wx, wy - 2, m2);
+          read_w<DIM, RECON>(sWj, wx, wy + 2, p2);
+        }
+        axis_edges<RECON, ISEN>(m2, m, c, p, p2, P.inv_gamma, su[1], sd[1]);
+        conv += p[2] - m[2];
+        jump = fmaxf(jump, fabsf(p[4] - m[4]) / fminf(p[4], m[4]));
+      }
+      if constexpr (DIM == 3) {
+        axis_edges<RECON, ISEN>(zw[ZH >= 2 ? ZH - 2 : 0], zw[ZH - 1], c, zw[ZH + 1], zw[ZH >= 2 ? ZH + 2 : ZW - 1],
+                                P.inv_gamma, su[2], sd[2]);
+        conv += zw[ZH + 1][3] - zw[ZH - 1][3];
+        jump = fmaxf(jump, fabsf(zw[ZH + 1][4] - zw[ZH - 1][4]) / fminf(zw[ZH + 1][4], zw[ZH - 1][4]));
+      }
+    }
+    Pred pr;
+    hancock<DIM>(c, conv, jump, su, sd, h, P, pr);
+
+    const bool tile_plane = j >= z0 && j < z1;
+    // 3. ghosts across outflow / reflecting x/y boundaries take the inner cell's half step.
+    if (xyg && tile_plane) {
+#pragma unroll
+      for (int v = 0; v < 6; v++) sFlux[v * PN + tid] = pr.q[v];
+      sFlux[6 * PN + tid] = pr.flag;
+      sFlux[7 * PN + tid] = pr.fo ? 1.f : 0.f;
+      __syncthreads();
+      if (g_src >= 0) {
+#pragma unroll
+        for (int v = 0; v < 6; v++) pr.q[v] = sFlux[v * PN + g_src];
+        if (g_flip) pr.q[1 + g_axis] = -pr.q[1 + g_axis];
+        pr.flag = sFlux[6 * PN + g_src];
+        pr.fo = sFlux[7 * PN + g_src] != 0.f;
+      }
+    }
+    if constexpr (DIM == 3) {
+      // plane 0 stands in for the lower z ghost: its face state toward plane 0
+      if (j == 0 && P.bc_lo[2] != 0) {
+        Pred g = pr;
+        if (P.bc_lo[2] == 2) g.q[3] = -g.q[3];
+        face_state(g, gsu, 1.f, zhi_prev);
+      }
+    }
+
+    // 4. face states toward the upper x and y faces, for the thread beyond each.
+    if (tile_plane) {
+      float f[7];
+      face_state(pr, su[0], 1.f, f);
+#pragma unroll
+      for (int v = 0; v < 7; v++) sFace[v * PN + tid] = f[v];
+      if constexpr (DIM >= 2) {
+        face_state(pr, su[1], 1.f, f);
+#pragma unroll
+        for (int v = 0; v < 7; v++) sFace[(7 + v) * PN + tid] = f[v];
+      }
+    }
+    __syncthreads();
+
+    // 5. fluxes: the lower x and y faces into shared memory, the lower z face in registers.
+    if (tile_plane) {
+      if (xface_t) {
+        float L[7], R[7], F[8];
+#pragma unroll
+        for (int v = 0; v < 7; v++) L[v] = sFace[v * PN + tid - 1];
+        face_state(pr, sd[0], -1.f, R);
+        riemann<0>(L, R, P, F);
+#pragma unroll
+        for (int v = 0; v < 8; v++) sFlux[v * PN + tid] = F[v];
+      }
+      if constexpr (DIM >= 2) {
+        if (yface_t) {
+          float L[7], R[7], F[8];
+#pragma unroll
+          for (int v = 0; v < 7; v++) L[v] = sFace[(7 + v) * PN + tid - PX];
+          face_state(pr, sd[1], -1.f, R);
+          riemann<1>(L, R, P, F);
+#pragma unroll
+          for (int v = 0; v < 8; v++) sFlux[(8 + v) * PN + tid] = F[v];
+        }
+      }
+    }
+    float Fz[8];
+    if constexpr (DIM == 3) {
+      if (tile_t && j >= z0) {
+        float R[7];
+        face_state(pr, sd[2], -1.f, R);
+        riemann<2>(zhi_prev, R, P, Fz);
+      }
+    }
+    __syncthreads();
+
+    // 6. updates: plane j-1 now has its upper z flux; plane j gets its in-plane fluxes.
+    if (tile_t) {
+      if constexpr (DIM == 3) {
+        if (j - 1 >= z0) {
+#pragma unroll
+          for (int v = 0; v < 8; v++) acc[v] -= Fz[v];
+          const size_t o = ((size_t)(j - 1) * ny + gy) * nx + gx;
+          float4 na, nb;
+          update_cell(__ldg(u1 + o), __ldg(u2 + o), acc, ph_prev, dtdx, P, na, nb);
+          o1[o] = na;
+          o2[o] = nb;
+          rate_max = fmaxf(rate_max, rate_guard(signal_rate(na, nb, P)));
+        }
+      }
+      if (tile_plane) {
+#pragma unroll
+        for (int v = 0; v < 8; v++) {
+          float a = sFlux[v * PN + tid];
+          a -= sFlux[v * PN + tid + 1];
+          if constexpr (DIM >= 2) {
+            a += sFlux[(8 + v) * PN + tid];
+            a -= sFlux[(8 + v) * PN + tid + PX];
+          }
+          if constexpr (DIM == 3) a += Fz[v];
+          acc[v] = a;
+        }
+        ph_prev = pr.q[4];
+        if constexpr (DIM < 3) {
+          const size_t o = (size_t)gy * nx + gx;
+          float4 na, nb;
+          update_cell(__ldg(u1 + o), __ldg(u2 + o), acc, ph_prev, dtdx, P, na, nb);
+          o1[o] = na;
+          o2[o] = nb;
+          rate_max = fmaxf(rate_max, rate_guard(signal_rate(na, nb, P)));
+        }
+      }
+    }
+    if constexpr (DIM == 3) {
+      face_state(pr, su[2], 1.f, zhi_prev);
+#pragma unroll
+      for (int v = 0; v < 6; v++) q_prev[v] = pr.q[v];
+      flag_prev = pr.flag;
+      fo_prev = pr.fo;
+    }
+  }
+  block_max_to<G::NT>(rate_max, sRed, rate_out);
+}
+
+// The signal-rate maximum of a state (the reference's rates pass, hydro/rates.wgsl, and its
+// reduction, gpu/reduce.wgsl): used for the first step after the state is set.
+__global__ void rate_kernel(const KParams P, const float4* __restrict__ u1, const float4* __restrict__ u2, size_t ncell,
+                            unsigned* __restrict__ out) {
+  __shared__ float sRed[32];
+  float m = 0.f;
+  for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < ncell; o += (size_t)gridDim.x * blockDim.x)
+    m = fmaxf(m, rate_guard(signal_rate(__ldg(u1 + o), __ldg(u2 + o), P)));
+  block_max_to<256>(m, sRed, out);
+}
+
+// One thread: dt from the rate maximum (clock.wgsl:38-147, in the reference's CPU form
+// hydro.ts:382 dt = min(cfl dx / rate, t_end - t)), the clock advanced by the step in float64.
+// A rate that is NaN or infinite marks the clock bad and holds it.
+__global__ void clock_kernel(DevClock* clk, unsigned* rates, int slot) {
+  const float rate = __uint_as_float(rates[slot]);
+  rates[slot ^ 1] = 0u;
+  const double t = clk->t;
+  double dt = clk->cfl_dx / fmax((double)rate, 1e-30);
+  if (!(rate == rate) || isinf(rate)) clk->bad = 1;
+  dt = fmin(dt, clk->dt_max);
+  const double te = clk->t_end;
+  if (te < HUGE_VAL) {
+    const double rem = te - t;
+    if (rem <= 1e-12 * fabs(te)) dt = 0.0;
+    else dt = fmin(dt, rem);
+  }
+  if (clk->bad) dt = 0.0;
+  clk->dt = dt;
+  clk->held = dt > 0.0 ? 0 : 1;
+  if (dt > 0.0) {
+    clk->t = t + dt;
+    clk->steps += 1;
+    clk->last_dt = dt;
+  }
+}
+
+__global__ void zero_kernel(unsigned* p) { *p = 0u; }
+
+// Compensated (Neumaier) float64 accumulation.
+struct Acc {
+  double s, c;
+  __device__ void add(double x) {
+    const double t = s + x;
+    c += fabs(s) >= fabs(x) ? (s - t) + x : (x - t) + s;
+    s = t;
+  }
+  __device__ double value() const { return s + c; }
+};
+
+// The conservation totals (hydro/diagnostics.wgsl channels 0-8, src/sim.ts:1808), per block in
+// compensated float64: mass, momentum (3), kinetic, internal (E - KE), total energy, floored
+// cells; the Mach maximum separately. Writes NDIAG doubles per block.
+constexpr int NDIAG = 9;
+__global__ void diag_partial_kernel(const KParams P, const float4* __restrict__ u1, const float4* __restrict__ u2,
+                                    size_t ncell, double* __restrict__ part) {
+  Acc acc[8];
+#pragma unroll
+  for (int i = 0; i < 8; i++) acc[i] = Acc{0.0, 0.0};
+  double mach = 0.0;
+  const double dv = P.dv;
+  for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < ncell; o += (size_t)gridDim.x * blockDim.x) {
+    const float4 a = __ldg(u1 + o), b = __ldg(u2 + o);
+    const double rho = fmax((double)a.x, (double)P.rho_floor);
+    const double vx = a.y / rho, vy = a.z / rho, vz = a.w / rho;
+    const double v2 = vx * vx + vy * vy + vz * vz;
+    const double p = fmax((double)P.gm1 * b.y, (double)P.p_floor);
+    const double cs = sqrt((double)P.gamma * p / rho);
+    acc[0].add(rho * dv);
+    acc[1].add((double)a.y * dv);
+    acc[2].add((double)a.z * dv);
+    acc[3].add((double)a.w * dv);
+    acc[4].add(0.5 * rho * v2 * dv);
+    acc[5].add(((double)b.x - 0.5 * rho * v2) * dv);
+    acc[6].add((double)b.x * dv);
+    acc[7].add((a.x <= P.rho_floor * 1.0001f || p <= P.p_floor * 1.0001) ? 1.0 : 0.0);
+    mach = fmax(mach, sqrt(v2) / cs);
+  }
+  // block reduction in a fixed order: each warp's lanes, then the warps
+  __shared__ double sh[32][NDIAG];
+  double v[NDIAG];
+#pragma unroll
+  for (int i = 0; i < 8; i++) v[i] = acc[i].value();
+  v[8] = mach;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1)
+#pragma unroll
+    for (int i = 0; i < NDIAG; i++) {
+      const double o = __shfl_down_sync(0xffffffffu, v[i], off);
+      v[i] = (i == 8) ? fmax(v[i], o) : v[i] + o;
+    }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0)
+    for (int i = 0; i < NDIAG; i++) sh[warp][i] = v[i];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int nw = blockDim.x >> 5;
+    for (int i = 0; i < NDIAG; i++) {
+      Acc s{0.0, 0.0};
+      double mx = 0.0;
+      for (int w = 0; w < nw; w++) {
+        if (i == 8) mx = fmax(mx, sh[w][i]);
+        else s.add(sh[w][i]);
+      }
+      part[(size_t)blockIdx.x * NDIAG + i] = (i == 8) ? mx : s.value();
+    }
+  }
+}
+
+__global__ void diag_final_kernel(const double* __restrict__ part, int nblocks, double* __restrict__ out) {
+  const int i = threadIdx.x;
+  if (i >= NDIAG) return;
+  Acc s{0.0, 0.0};
+  double mx = 0.0;
+  for (int b = 0; b < nblocks; b++) {
+    const double x = part[(size_t)b * NDIAG + i];
+    if (i == 8) mx = fmax(mx, x);
+    else s.add(x);
+  }
+  out[i] = (i == 8) ? mx : s.value();
+}
+
+// ---------------------------------------------------------------------------------------------
+// Host launchers.
+
+template <int DIM, int RECON, bool ISEN>
+static cudaError_t launch_sweep_t(const KParams& P, const float4* u1, const float4* u2, float4* o1, float4* o2,
+                                  const DevClock* clk, unsigned* rate_out, cudaStream_t s) {
+  using G = Geo<DIM, RECON>;
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(sweep_kernel<DIM, RECON, ISEN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)G::SMEM_BYTES);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  dim3 grid((P.n[0] + G::TX - 1) / G::TX, DIM >= 2 ? (P.n[1] + G::TY - 1) / G::TY : 1,
+            DIM == 3 ? (P.n[2] + G::TZ - 1) / G::TZ : 1);
+  sweep_kernel<DIM, RECON, ISEN><<<grid, G::NT, G::SMEM_BYTES, s>>>(P, u1, u2, o1, o2, clk, rate_out);
+  return cudaGetLastError();
+}
+
+template <int DIM, int RECON>
+static cudaError_t launch_sweep_r(const KParams& P, bool isen, const float4* u1, const float4* u2, float4* o1, float4* o2,
+                                  const DevClock* clk, unsigned* rate_out, cudaStream_t s) {
+  if constexpr (RECON == R_PPM) {
+    return launch_sweep_t<DIM, RECON, false>(P, u1, u2, o1, o2, clk, rate_out, s);
+  } else {
+    return isen ? launch_sweep_t<DIM, RECON, true>(P, u1, u2, o1, o2, clk, rate_out, s)
+                : launch_sweep_t<DIM, RECON, false>(P, u1, u2, o1, o2, clk, rate_out, s);
+  }
+}
+
+template <int DIM>
+static cudaError_t launch_sweep_d(const KParams& P, int recon, bool isen, const float4* u1, const float4* u2, float4* o1,
+                                  float4* o2, const DevClock* clk, unsigned* rate_out, cudaStream_t s) {
+  switch (recon) {
+    case R_MINMOD: return launch_sweep_r<DIM, R_MINMOD>(P, isen, u1, u2, o1, o2, clk, rate_out, s);
+    case R_MC: return launch_sweep_r<DIM, R_MC>(P, isen, u1, u2, o1, o2, clk, rate_out, s);
+    case R_VANLEER: return launch_sweep_r<DIM, R_VANLEER>(P, isen, u1, u2, o1, o2, clk, rate_out, s);
+    case R_KOREN: return launch_sweep_r<DIM, R_KOREN>(P, isen, u1, u2, o1, o2, clk, rate_out, s);
+    case R_PPM: return launch_sweep_r<DIM, R_PPM>(P, isen, u1, u2, o1, o2, clk, rate_out, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_sweep(const KParams& P, int ndim, int recon, bool isen, const float4* u1, const float4* u2, float4* o1,
+                         float4* o2, const DevClock* clk, unsigned* rate_out, cudaStream_t s) {
+  switch (ndim) {
+    case 1: return launch_sweep_d<1>(P, recon, isen, u1, u2, o1, o2, clk, rate_out, s);
+    case 2: return launch_sweep_d<2>(P, recon, isen, u1, u2, o1, o2, clk, rate_out, s);
+    case 3: return launch_sweep_d<3>(P, recon, isen, u1, u2, o1, o2, clk, rate_out, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+size_t sweep_smem_bytes(int ndim, int recon) {
+  const bool ppm = recon == R_PPM;
+  switch (ndim) {
+    case 1: return ppm ? Geo<1, R_PPM>::SMEM_BYTES : Geo<1, R_MINMOD>::SMEM_BYTES;
+    case 2: return ppm ? Geo<2, R_PPM>::SMEM_BYTES : Geo<2, R_MINMOD>::SMEM_BYTES;
+    default: return ppm ? Geo<3, R_PPM>::SMEM_BYTES : Geo<3, R_MINMOD>::SMEM_BYTES;
+  }
+}
+
+int sweep_min_cells(int recon) { return recon == R_PPM ? 3 : 2; }
+
+cudaError_t launch_rate(const KParams& P, const float4* u1, const float4* u2, size_t ncell, unsigned* out, cudaStream_t s) {
+  zero_kernel<<<1, 1, 0, s>>>(out);
+  int blocks = (int)((ncell + 255) / 256);
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  if (blocks < 1) blocks = 1;
+  rate_kernel<<<blocks, 256, 0, s>>>(P, u1, u2, ncell, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_clock(DevClock* clk, unsigned* rates, int slot, cudaStream_t s) {
+  clock_kernel<<<1, 1, 0, s>>>(clk, rates, slot);
+  return cudaGetLastError();
+}
+
+int diag_blocks(size_t ncell) {
+  size_t b = (ncell + 255) / 256;
+  if (b > 148 * 4) b = 148 * 4;
+  return b < 1 ? 1 : (int)b;
+}
+
+cudaError_t launch_diag(const KParams& P, const float4* u1, const float4* u2, size_t ncell, double* part, double* out,
+                        cudaStream_t s) {
+  const int blocks = diag_blocks(ncell);
+  diag_partial_kernel<<<blocks, 256, 0, s>>>(P, u1, u2, ncell, part);
+  diag_final_kernel<<<1, 32, 0, s>>>(part, blocks, out);
+  return cudaGetLastError();
+}
+
+}  // namespace shz
