@@ -48,7 +48,7 @@ def build_library(force: bool = False, verbose: bool = False) -> Path:
     objs = []
     for src in srcs:
         obj = obj_dir / (src.stem + ".o")
-        cmd = [NVCC, "-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC,-fopenmp,-O3",
+        cmd = [NVCC, "-O3", "-std=c++17", *ARCH, "-lineinfo", "--use_fast_math", "-Xcompiler", "-fPIC,-fopenmp,-O3",
                "-I", str(ROOT / "include"), "-c", str(src), "-o", str(obj)]
         if src.suffix == ".cu":
             cmd[1:1] = ["-Xptxas", "-v"] if verbose else []
