@@ -204,6 +204,38 @@ int64_t shz_kernel_launches(const shz_sim* sim);
 /* Library version string. */
 const char* shz_version(void);
 
+/*
+ * Conservation totals of a state the caller owns, computed without allocating anything.
+ * No counterpart in the reference.
+ *
+ * For callers that cannot let a library allocate device memory: a host that keeps all of its
+ * GPU memory in its own pool or fixed arena and accounts for every byte (a serving process
+ * admitting work against a fixed HBM budget), or a binding handed device buffers by another
+ * runtime with no allocator of its own to call. It makes no cudaMalloc, cudaFree or other
+ * allocating call; its scratch is a file-scope device array of SHZ_TOTALS_MAX_BLOCKS rows of
+ * SHZ_DIAG_VALUES doubles (576 KiB) that every GPU loading the library holds until exit.
+ *
+ * cfg:    grid size n[3], dx, gamma, rho_floor, p_floor and device are read; the rest is ignored.
+ *         States of more than SHZ_TOTALS_MAX_BLOCKS * SHZ_TOTALS_CELLS_PER_BLOCK cells
+ *         (134,217,728 = 512^3) are refused with SHZ_E_CONFIG.
+ * u1, u2: device pointers to the state, two float4 arrays in the layout above.
+ * out:    device pointer to SHZ_DIAG_VALUES doubles: mass, momentum x/y/z, e_kin, e_int, e_tot,
+ *         floored cells, max Mach (the fields of shz_diag, same meaning).
+ * stream: cudaStream_t to enqueue on (NULL for the default stream); the call returns once the
+ *         work is enqueued, and `out` is ready when the stream reaches it.
+ *
+ * The first call on a device looks up the array's device address (cudaGetSymbolAddress) with
+ * that device current; make that first call before any stream capture. All calls share the one
+ * array: calls whose work overlaps on the GPU race on it, so serialise them (one stream, or
+ * events between streams). Each call overwrites every row it reads, so nothing left by an
+ * earlier call matters. On failure, shz_totals_noalloc_error() gives the message.
+ */
+#define SHZ_DIAG_VALUES 9
+#define SHZ_TOTALS_MAX_BLOCKS 8192
+#define SHZ_TOTALS_CELLS_PER_BLOCK 16384
+int shz_totals_noalloc(const shz_config* cfg, const void* u1, const void* u2, double* out, void* stream);
+const char* shz_totals_noalloc_error(void);
+
 #ifdef __cplusplus
 }
 #endif

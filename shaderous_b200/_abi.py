@@ -110,7 +110,13 @@ SIGNATURES = [
     ("shz_profile", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(shz_profile_result)]),
     ("shz_kernel_launches", C.c_int64, [C.c_void_p]),
     ("shz_version", C.c_char_p, []),
+    ("shz_totals_noalloc", C.c_int, [C.POINTER(shz_config), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("shz_totals_noalloc_error", C.c_char_p, []),
 ]
+
+SHZ_DIAG_VALUES = 9
+SHZ_TOTALS_MAX_BLOCKS = 8192
+SHZ_TOTALS_CELLS_PER_BLOCK = 16384
 
 _lib = None
 
