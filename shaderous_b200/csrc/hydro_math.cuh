@@ -155,6 +155,9 @@ __device__ __forceinline__ void axis_edges(const float* m2, const float* m, cons
 // hydro.ts:360-375 side, rotated so that index 1 is normal to the face; then
 // hydro.ts:102-159 riemannFlux. L and R are (rho, vx, vy, vz, p, s, shock flag). The flux comes
 // back in the lab frame: (m, mx, my, mz, e, ei, s, vn).
+// The three regions (left-supersonic, right-supersonic, star) and the star side are chosen by
+// selects rather than branches, so that a warp whose faces fall in different regions runs one
+// path; the values computed for the regions not chosen are discarded.
 template <int AXIS>
 __device__ __forceinline__ void riemann(const float* L, const float* R, const KParams& P, float* F) {
   constexpr int A0 = 1 + AXIS, A1 = 1 + (AXIS + 1) % 3, A2 = 1 + (AXIS + 2) % 3;
@@ -175,54 +178,52 @@ __device__ __forceinline__ void riemann(const float* L, const float* R, const KP
   const float fpl0 = ml0 * lu + lp, fpl1 = ml1 * lu, fpl2 = ml2 * lu;
   const float fpr0 = mr0 * ru + rp, fpr1 = mr1 * ru, fpr2 = mr2 * ru;
   const float fel = (el + lp) * lu, fer = (er + rp) * ru;
-  float m, p0, p1, p2, e, vn;
-  if (sl >= 0.f) {
-    m = ml0; p0 = fpl0; p1 = fpl1; p2 = fpl2; e = fel; vn = lu;
-  } else if (sr <= 0.f) {
-    m = mr0; p0 = fpr0; p1 = fpr1; p2 = fpr2; e = fer; vn = ru;
-  } else {
-    const float ql = lr * (sl - lu);
-    const float qr = rr * (sr - ru);
-    const float sm = (rp - lp + lu * ql - ru * qr) / (ql - qr);
-    const float inv = 1.f / (sr - sl);
-    const float slsr = sl * sr;
-    const float hm = (sr * ml0 - sl * mr0 + slsr * (rr - lr)) * inv;
-    const float hp0 = (sr * fpl0 - sl * fpr0 + slsr * (mr0 - ml0)) * inv;
-    const float hp1 = (sr * fpl1 - sl * fpr1 + slsr * (mr1 - ml1)) * inv;
-    const float hp2 = (sr * fpl2 - sl * fpr2 + slsr * (mr2 - ml2)) * inv;
-    const float he = (sr * fel - sl * fer + slsr * (er - el)) * inv;
-    float cm, c0, c1, c2, ce;
-    if (sm >= 0.f) {
-      const float f = ql / (sl - sm);
-      const float es = f * (el / lr + (sm - lu) * (sm + lp / ql));
-      cm = ml0 + sl * (f - lr);
-      c0 = fpl0 + sl * (f * sm - ml0);
-      c1 = fpl1 + sl * (f * lv - ml1);
-      c2 = fpl2 + sl * (f * lw - ml2);
-      ce = fel + sl * (es - el);
-    } else {
-      const float f = qr / (sr - sm);
-      const float es = f * (er / rr + (sm - ru) * (sm + rp / qr));
-      cm = mr0 + sr * (f - rr);
-      c0 = fpr0 + sr * (f * sm - mr0);
-      c1 = fpr1 + sr * (f * rv - mr1);
-      c2 = fpr2 + sr * (f * rw - mr2);
-      ce = fer + sr * (es - er);
-    }
-    m = cm + (hm - cm) * w_hll;
-    p0 = c0 + (hp0 - c0) * w_hll;
-    p1 = c1 + (hp1 - c1) * w_hll;
-    p2 = c2 + (hp2 - c2) * w_hll;
-    e = ce + (he - ce) * w_hll;
-    vn = sm;
-  }
+
+  // HLL state flux and the contact speed
+  const float ql = lr * (sl - lu);
+  const float qr = rr * (sr - ru);
+  const float sm = (rp - lp + lu * ql - ru * qr) / (ql - qr);
+  const float inv = 1.f / (sr - sl);
+  const float slsr = sl * sr;
+  const float hm = (sr * ml0 - sl * mr0 + slsr * (rr - lr)) * inv;
+  const float hp0 = (sr * fpl0 - sl * fpr0 + slsr * (mr0 - ml0)) * inv;
+  const float hp1 = (sr * fpl1 - sl * fpr1 + slsr * (mr1 - ml1)) * inv;
+  const float hp2 = (sr * fpl2 - sl * fpr2 + slsr * (mr2 - ml2)) * inv;
+  const float he = (sr * fel - sl * fer + slsr * (er - el)) * inv;
+  // HLLC star state on the side of the contact the face lies on
+  const bool left = sm >= 0.f;
+  const float sK = left ? sl : sr, qK = left ? ql : qr, rK = left ? lr : rr, uK = left ? lu : ru;
+  const float vK = left ? lv : rv, wK = left ? lw : rw, pK = left ? lp : rp, eK = left ? el : er;
+  const float mK0 = left ? ml0 : mr0, mK1 = left ? ml1 : mr1, mK2 = left ? ml2 : mr2;
+  const float fK0 = left ? fpl0 : fpr0, fK1 = left ? fpl1 : fpr1, fK2 = left ? fpl2 : fpr2, feK = left ? fel : fer;
+  const float f = qK / (sK - sm);
+  const float es = f * (eK / rK + (sm - uK) * (sm + pK / qK));
+  const float cm = mK0 + sK * (f - rK);
+  const float c0 = fK0 + sK * (f * sm - mK0);
+  const float c1 = fK1 + sK * (f * vK - mK1);
+  const float c2 = fK2 + sK * (f * wK - mK2);
+  const float ce = feK + sK * (es - eK);
+  float m = cm + (hm - cm) * w_hll;
+  float p0 = c0 + (hp0 - c0) * w_hll;
+  float p1 = c1 + (hp1 - c1) * w_hll;
+  float p2 = c2 + (hp2 - c2) * w_hll;
+  float e = ce + (he - ce) * w_hll;
+  float vn = sm;
+  // supersonic faces take the upwind side's flux
+  const bool supl = sl >= 0.f, supr = sr <= 0.f;
+  m = supl ? ml0 : (supr ? mr0 : m);
+  p0 = supl ? fpl0 : (supr ? fpr0 : p0);
+  p1 = supl ? fpl1 : (supr ? fpr1 : p1);
+  p2 = supl ? fpl2 : (supr ? fpr2 : p2);
+  e = supl ? fel : (supr ? fer : e);
+  vn = supl ? lu : (supr ? ru : vn);
   const bool up = m >= 0.f;
   F[0] = m;
   F[A0] = p0;
   F[A1] = p1;
   F[A2] = p2;
   F[4] = e;
-  F[5] = m * (up ? lei / lr : rei / rr);
+  F[5] = m * ((up ? lei : rei) / (up ? lr : rr));
   F[6] = m * (up ? L[5] : R[5]);
   F[7] = vn;
 }
@@ -243,6 +244,23 @@ __device__ __forceinline__ void prim_from_cons(const float4 a, const float4 b, c
   w[5] = b.z * inv;
   w[6] = sqrtf(P.gamma * p * inv);
 }
+
+// The six primitives the stencil reads of a neighbour (rho, vx, vy, vz, p, s): the sound
+// speed is needed only at the centre cell and is formed there (with_cs).
+__device__ __forceinline__ void prim6_from_cons(const float4 a, const float4 b, const KParams& P, float fx, float fy,
+                                                float fz, float* w) {
+  const float rho = fmaxf(a.x, P.rho_floor);
+  const float inv = 1.f / rho;
+  float p = P.gm1 * b.y;
+  if (!(p >= P.p_floor)) p = P.p_floor;
+  w[0] = rho;
+  w[1] = a.y * inv * fx;
+  w[2] = a.z * inv * fy;
+  w[3] = a.w * inv * fz;
+  w[4] = p;
+  w[5] = b.z * inv;
+}
+__device__ __forceinline__ void with_cs(float* w, const KParams& P) { w[6] = sqrtf(P.gamma * w[4] / w[0]); }
 
 // The signal rate of a cell (hydro.ts:254): |vx| + |vy| + |vz| + signal * cs.
 __device__ __forceinline__ float signal_rate(const float4 a, const float4 b, const KParams& P) {

@@ -40,7 +40,6 @@ template <int DIM, int RECON>
 struct Geo {
   static constexpr int H = (RECON == R_PPM) ? 3 : 2;   // halo of the primitives' region
   static constexpr int ZH = (RECON == R_PPM) ? 2 : 1;  // planes each way the predictor reads along z
-  static constexpr int ZW = 2 * ZH + 1;                // planes held per thread
   static constexpr int TX = (DIM == 1) ? 126 : 16;
   static constexpr int TY = (DIM == 1) ? 1 : 16;
   static constexpr int TZ = (DIM == 3) ? 64 : 1;
@@ -51,9 +50,14 @@ struct Geo {
   static constexpr int WX = TX + 2 * H;
   static constexpr int WY = (DIM >= 2) ? TY + 2 * H : 1;
   static constexpr int WN = WX * WY;
-  static constexpr int NBUF = (DIM == 3) ? ZH + 1 : 1;
-  static constexpr int NF = (DIM >= 2) ? 2 : 1;  // in-plane face directions
-  static constexpr size_t SMEM_FLOATS = (size_t)NBUF * 7 * WN + (size_t)NF * 7 * PN + (size_t)NF * 8 * PN + 32;
+  static constexpr int WC = 6;                               // primitives kept per cell (no sound speed)
+  static constexpr int NBUF = (DIM == 3) ? 2 * ZH + 1 : 1;   // ring of planes: the predictor's z stencil
+  static constexpr int NF = (DIM >= 2) ? 2 : 1;              // in-plane face directions
+  // Registers per thread such that two CTAs are resident per SM. Warps are spread over the SM's
+  // four sub-partitions, each with a 16K-register file: two 11-warp CTAs put 6 warps on one,
+  // and 6 x 32 x 80 <= 16384.
+  static constexpr int MAXREG = (DIM == 1) ? 64 : 80;
+  static constexpr size_t SMEM_FLOATS = (size_t)NBUF * WC * WN + (size_t)NF * 7 * PN + (size_t)NF * 8 * PN + 32;
   static constexpr size_t SMEM_BYTES = SMEM_FLOATS * sizeof(float);
 };
 
@@ -73,18 +77,19 @@ __device__ __forceinline__ void load_w_plane(const KParams& P, const float4* __r
     const int gy = (DIM >= 2) ? bc_map(y0 - G::H + ly, P.n[1], P.bc_lo[1], P.bc_hi[1], fy) : 0;
     const size_t o = zoff + (size_t)gy * P.n[0] + gx;
     const float4 a = __ldg(u1 + o), b = __ldg(u2 + o);
-    float w[7];
-    prim_from_cons(a, b, P, fx, fy, fz, w);
+    float w[6];
+    prim6_from_cons(a, b, P, fx, fy, fz, w);
 #pragma unroll
-    for (int c = 0; c < 7; c++) sWb[c * G::WN + idx] = w[c];
+    for (int c = 0; c < 6; c++) sWb[c * G::WN + idx] = w[c];
   }
 }
 
+// The six stored primitives of region cell (wx, wy) of a plane.
 template <int DIM, int RECON>
 __device__ __forceinline__ void read_w(const float* __restrict__ sWb, int wx, int wy, float* w) {
   using G = Geo<DIM, RECON>;
 #pragma unroll
-  for (int c = 0; c < 7; c++) w[c] = sWb[c * G::WN + wy * G::WX + wx];
+  for (int c = 0; c < 6; c++) w[c] = sWb[c * G::WN + wy * G::WX + wx];
 }
 
 // The per-cell result of the predictor (hydro.ts:272-322 predictRaw): the half-step state q,
@@ -129,11 +134,12 @@ __device__ __forceinline__ void hancock(const float* c, float conv, float jump, 
   for (int v = 0; v < 6; v++) out.q[v] = out.fo ? c[v] : qh[v];
 }
 
-// Face state q + 0.5 sgn inc (q alone when first order), with the cell's shock flag
-// (hydro.ts:362 side's f(n)).
+// Face state q + 0.5 sgn inc (q alone when first order: the increments are zeroed), with the
+// cell's shock flag (hydro.ts:362 side's f(n)).
 __device__ __forceinline__ void face_state(const Pred& pr, const float* inc, float sgn, float* f) {
+  const float k = pr.fo ? 0.f : 0.5f * sgn;
 #pragma unroll
-  for (int v = 0; v < 6; v++) f[v] = pr.fo ? pr.q[v] : pr.q[v] + 0.5f * sgn * inc[v];
+  for (int v = 0; v < 6; v++) f[v] = pr.q[v] + k * inc[v];
   f[6] = pr.flag;
 }
 
@@ -166,8 +172,8 @@ __device__ __forceinline__ float warp_max(float v) {
 }
 
 // Block maximum of a non-negative rate into *out (as the float's bits: non-negative floats
-// order as unsigned integers; a NaN orders above every finite rate, which the clock reports).
-// fmaxf drops NaN operands, so a NaN rate is carried as +inf bits through the shuffles.
+// order as unsigned integers). fmaxf drops NaN operands, so rate_guard carries a NaN rate as
+// +inf, which orders above every finite rate and which the clock reports.
 template <int NT>
 __device__ __forceinline__ void block_max_to(float v, float* sRed, unsigned* out) {
   v = warp_max(v);
@@ -185,14 +191,14 @@ __device__ __forceinline__ void block_max_to(float v, float* sRed, unsigned* out
 __device__ __forceinline__ float rate_guard(float r) { return (r == r) ? r : __int_as_float(0x7f800000); }
 
 template <int DIM, int RECON, bool ISEN>
-__global__ void __launch_bounds__(Geo<DIM, RECON>::NT, 1)
+__global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, RECON>::MAXREG))
     sweep_kernel(const KParams P, const float4* __restrict__ u1, const float4* __restrict__ u2, float4* __restrict__ o1,
                  float4* __restrict__ o2, const DevClock* __restrict__ clk, unsigned* __restrict__ rate_out) {
   using G = Geo<DIM, RECON>;
-  constexpr int H = G::H, ZH = G::ZH, ZW = G::ZW, PX = G::PX, PN = G::PN;
+  constexpr int H = G::H, ZH = G::ZH, PX = G::PX, PN = G::PN, WN = G::WN, WC = G::WC;
   extern __shared__ __align__(16) float smem[];
   float* sW = smem;
-  float* sFace = sW + G::NBUF * 7 * G::WN;
+  float* sFace = sW + G::NBUF * WC * WN;
   float* sFlux = sFace + G::NF * 7 * PN;
   float* sRed = sFlux + G::NF * 8 * PN;
 
@@ -201,6 +207,7 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT, 1)
   const int x0 = blockIdx.x * G::TX, y0 = blockIdx.y * G::TY;
   const int gx = x0 - 1 + tx, gy = (DIM >= 2) ? y0 - 1 + ty : 0;
   const int wx = tx + H - 1, wy = (DIM >= 2) ? ty + H - 1 : 0;
+  const int wo = wy * G::WX + wx;  // own cell within a plane of the region
   const int nx = P.n[0], ny = P.n[1], nz = P.n[2];
   // Roles: tile_t updates cell (gx, gy); row_t / col_t: the row / column lies in the tile.
   const bool row_t = (DIM < 2) || (ty >= 1 && ty <= G::TY && gy < ny);
@@ -249,11 +256,11 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT, 1)
 
   const int z0 = (DIM == 3) ? blockIdx.z * G::TZ : 0;
   const int z1 = (DIM == 3) ? min(z0 + G::TZ, nz) : 1;
-  auto buf = [&](int plane) -> float* {
-    return sW + (((plane % G::NBUF) + G::NBUF) % G::NBUF) * 7 * G::WN;
+  // plane -> its slot of the ring (planes may be negative near the lower boundary)
+  auto ring = [&](int plane) -> float* {
+    return sW + (((plane % G::NBUF) + G::NBUF) % G::NBUF) * WC * WN;
   };
 
-  float zw[ZW][7];        // own column's primitives, planes j-ZH .. j+ZH
   float zhi_prev[7];      // face state below the upper z face of plane j-1
   float q_prev[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   float flag_prev = 0.f;
@@ -265,15 +272,8 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT, 1)
   for (int v = 0; v < 7; v++) zhi_prev[v] = 0.f;
 
   if constexpr (DIM == 3) {
-    for (int pl = z0 - 1 - ZH; pl <= z0 - 2 + ZH; pl++) {
-      load_w_plane<DIM, RECON>(P, u1, u2, x0, y0, pl, buf(pl));
-      __syncthreads();
-#pragma unroll
-      for (int s = 0; s < ZW - 1; s++)
-#pragma unroll
-        for (int v = 0; v < 7; v++) zw[s][v] = zw[s + 1][v];
-      read_w<DIM, RECON>(buf(pl), wx, wy, zw[ZW - 1]);
-    }
+    // the planes below the first that the predictor reads along z
+    for (int pl = z0 - 1 - ZH; pl <= z0 - 2 + ZH; pl++) load_w_plane<DIM, RECON>(P, u1, u2, x0, y0, pl, ring(pl));
   }
 
   const int jb = (DIM == 3) ? z0 - 1 : 0;
@@ -281,36 +281,30 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT, 1)
   for (int j = jb; j <= je; j++) {
     // 1. primitives of plane j + ZH (the plane itself when there is no march)
     const int lp = (DIM == 3) ? j + ZH : 0;
-    load_w_plane<DIM, RECON>(P, u1, u2, x0, y0, lp, buf(lp));
+    load_w_plane<DIM, RECON>(P, u1, u2, x0, y0, lp, ring(lp));
     __syncthreads();
-    float c[7];
-    if constexpr (DIM == 3) {
-#pragma unroll
-      for (int s = 0; s < ZW - 1; s++)
-#pragma unroll
-        for (int v = 0; v < 7; v++) zw[s][v] = zw[s + 1][v];
-      read_w<DIM, RECON>(buf(lp), wx, wy, zw[ZW - 1]);
-#pragma unroll
-      for (int v = 0; v < 7; v++) c[v] = zw[ZH][v];
-    } else {
-      read_w<DIM, RECON>(buf(0), wx, wy, c);
-    }
+    const float* sWj = ring((DIM == 3) ? j : 0);
 
     if constexpr (DIM == 3) {
-      // The lower z ghost plane (outflow / reflect): only its edges toward the domain, at the
-      // ghost position; its half-step state is plane 0's, taken below.
-      if (j == -1 && P.bc_lo[2] != 0) {
-        float sd_unused[6];
-        axis_edges<RECON, ISEN>(zw[ZH >= 2 ? ZH - 2 : 0], zw[ZH - 1], zw[ZH], zw[ZH + 1], zw[ZH >= 2 ? ZH + 2 : ZW - 1],
-                                P.inv_gamma, gsu, sd_unused);
-        continue;
-      }
-      // The upper z ghost plane: plane nz-1's half-step state with edges at the ghost position.
-      if (j == nz && P.bc_hi[2] != 0) {
-        float su_unused[6], gsd[6];
-        axis_edges<RECON, ISEN>(zw[ZH >= 2 ? ZH - 2 : 0], zw[ZH - 1], zw[ZH], zw[ZH + 1], zw[ZH >= 2 ? ZH + 2 : ZW - 1],
-                                P.inv_gamma, su_unused, gsd);
-        if (tile_t) {
+      // The z ghost planes (outflow / reflect) need only their edges toward the domain, at the
+      // ghost position; their half-step state is that of the adjacent inner plane.
+      const bool zg_lo = j == -1 && P.bc_lo[2] != 0;
+      const bool zg_hi = j == nz && P.bc_hi[2] != 0;
+      if (zg_lo || zg_hi) {
+        float c[7], m[7], p[7], m2[7], p2[7], su[6], sd[6];
+        read_w<DIM, RECON>(sWj, wx, wy, c);
+        with_cs(c, P);
+        read_w<DIM, RECON>(ring(j - 1) + 0, wx, wy, m);
+        read_w<DIM, RECON>(ring(j + 1) + 0, wx, wy, p);
+        if constexpr (RECON == R_PPM) {
+          read_w<DIM, RECON>(ring(j - 2), wx, wy, m2);
+          read_w<DIM, RECON>(ring(j + 2), wx, wy, p2);
+        }
+        axis_edges<RECON, ISEN>(m2, m, c, p, p2, P.inv_gamma, su, sd);
+        if (zg_lo) {
+#pragma unroll
+          for (int v = 0; v < 6; v++) gsu[v] = su[v];
+        } else if (tile_t) {
           Pred g;
 #pragma unroll
           for (int v = 0; v < 6; v++) g.q[v] = q_prev[v];
@@ -318,7 +312,7 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT, 1)
           g.flag = flag_prev;
           g.fo = fo_prev;
           float zlo[7], Fz[8];
-          face_state(g, gsd, -1.f, zlo);
+          face_state(g, sd, -1.f, zlo);
           riemann<2>(zhi_prev, zlo, P, Fz);
 #pragma unroll
           for (int v = 0; v < 8; v++) acc[v] -= Fz[v];
@@ -334,10 +328,12 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT, 1)
     }
 
     // 2. predictor at plane j: edges per active axis, shock flag, Hancock half step.
+    float c[7];
+    read_w<DIM, RECON>(sWj, wx, wy, c);
+    with_cs(c, P);
     float su[DIM][6], sd[DIM][6];
     float conv = 0.f, jump = 0.f;
     {
-      const float* sWj = buf((DIM == 3) ? j : 0);
       float m[7], p[7], m2[7], p2[7];
       read_w<DIM, RECON>(sWj, wx - 1, wy, m);
       read_w<DIM, RECON>(sWj, wx + 1, wy, p);
@@ -360,12 +356,18 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT, 1)
         jump = fmaxf(jump, fabsf(p[4] - m[4]) / fminf(p[4], m[4]));
       }
       if constexpr (DIM == 3) {
-        axis_edges<RECON, ISEN>(zw[ZH >= 2 ? ZH - 2 : 0], zw[ZH - 1], c, zw[ZH + 1], zw[ZH >= 2 ? ZH + 2 : ZW - 1],
-                                P.inv_gamma, su[2], sd[2]);
-        conv += zw[ZH + 1][3] - zw[ZH - 1][3];
-        jump = fmaxf(jump, fabsf(zw[ZH + 1][4] - zw[ZH - 1][4]) / fminf(zw[ZH + 1][4], zw[ZH - 1][4]));
+        read_w<DIM, RECON>(ring(j - 1), wx, wy, m);
+        read_w<DIM, RECON>(ring(j + 1), wx, wy, p);
+        if constexpr (RECON == R_PPM) {
+          read_w<DIM, RECON>(ring(j - 2), wx, wy, m2);
+          read_w<DIM, RECON>(ring(j + 2), wx, wy, p2);
+        }
+        axis_edges<RECON, ISEN>(m2, m, c, p, p2, P.inv_gamma, su[2], sd[2]);
+        conv += p[3] - m[3];
+        jump = fmaxf(jump, fabsf(p[4] - m[4]) / fminf(p[4], m[4]));
       }
     }
+    (void)wo;
     Pred pr;
     hancock<DIM>(c, conv, jump, su, sd, h, P, pr);
 
@@ -622,6 +624,10 @@ static cudaError_t launch_sweep_t(const KParams& P, const float4* u1, const floa
   if (!configured) {
     cudaError_t e = cudaFuncSetAttribute(sweep_kernel<DIM, RECON, ISEN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)G::SMEM_BYTES);
+    if (e != cudaSuccess) return e;
+    // all of the unified L1/shared storage as shared memory, so that two CTAs fit per SM
+    e = cudaFuncSetAttribute(sweep_kernel<DIM, RECON, ISEN>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             (int)cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess) return e;
     configured = true;
   }
