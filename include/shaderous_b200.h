@@ -198,6 +198,40 @@ typedef struct shz_profile_result {
 } shz_profile_result;
 int shz_profile(shz_sim* sim, int32_t n, shz_profile_result* out);
 
+/*
+ * The adaptive grid's block tree (host), deciding slot for slot as the reference's BlockTree
+ * (src/amr/tree.ts:106-824), and its flat tables for bit-exact checks. Blocks hold 16^ndim cells
+ * (BS, tree.ts:14); the block table has 32 ints per slot (BT_STRIDE, layout tree.ts:42-60), the
+ * regrid table 12 (RG_STRIDE, tree.ts:62-66).
+ */
+#define SHZ_AMR_BS 16
+#define SHZ_AMR_BT_STRIDE 32
+#define SHZ_AMR_RG_STRIDE 12
+typedef struct shz_tree shz_tree;
+/* new BlockTree(ndim, nr, maxLevel, cap, bcLo, bcHi, edgeBalance) (tree.ts:139). */
+int shz_tree_create(int32_t ndim, int32_t nr, int32_t max_level, int32_t cap, const int32_t bc_lo[3],
+                    const int32_t bc_hi[3], int32_t edge_balance, shz_tree** out);
+void shz_tree_destroy(shz_tree* t);
+const char* shz_tree_error(void);
+/* adapt((b) => indicator[b.slot], hi, lo) (tree.ts:489). regrid: cap * 12 ints or NULL;
+ * changed: 0 if the tree did not change (adapt returned null). */
+int shz_tree_adapt(shz_tree* t, const double* indicator_by_slot, double hi, double lo, int32_t* regrid, int32_t* changed);
+/* The steps the last adapt took, flattened [what, level, c0..c(ndim-1)] per step (tree.ts:574). */
+int shz_tree_last_steps(const shz_tree* t, int32_t* out, int32_t max_ints, int32_t* n_ints);
+/* replayAdapt(steps) (tree.ts:579): the same flattened form. */
+int shz_tree_replay(shz_tree* t, const int32_t* steps, int32_t n_ints, int32_t* regrid, int32_t* changed);
+/* refine(get(level, c)) (tree.ts:366): *n_split = blocks split (0 if refused). */
+int shz_tree_refine(shz_tree* t, int32_t level, const int32_t c[3], int32_t* n_split);
+/* neighbor(get(level, c), f) (tree.ts:283): kind 0 same, 1 coarse, 2 boundary; slot or type. */
+int shz_tree_neighbor(const shz_tree* t, int32_t level, const int32_t c[3], int32_t f, int32_t* kind, int32_t* slot_or_type);
+int shz_tree_table(const shz_tree* t, int32_t* out);                  /* cap * 32 ints */
+/* lists() (tree.ts:695): every block coarsest first, the leaves, blocks per level. */
+int shz_tree_lists(const shz_tree* t, int32_t* all, int32_t* leaves, int32_t* per_level, int32_t* n_all, int32_t* n_leaves);
+int64_t shz_tree_index_grid_size(const shz_tree* t);
+int shz_tree_index_grid(const shz_tree* t, uint32_t* out);             /* leaf slot per finest block cell */
+/* count, free slots, leaves, deepest level, highest slot used */
+int shz_tree_stats(const shz_tree* t, int32_t* blocks, int32_t* free_slots, int32_t* leaves, int32_t* deepest, int32_t* high_slot);
+
 /* Launches of the library's own kernels on this handle since creation. */
 int64_t shz_kernel_launches(const shz_sim* sim);
 

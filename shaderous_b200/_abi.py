@@ -110,6 +110,23 @@ SIGNATURES = [
     ("shz_profile", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(shz_profile_result)]),
     ("shz_kernel_launches", C.c_int64, [C.c_void_p]),
     ("shz_version", C.c_char_p, []),
+    ("shz_tree_create", C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_int32),
+                                  C.POINTER(C.c_int32), C.c_int32, C.POINTER(C.c_void_p)]),
+    ("shz_tree_destroy", None, [C.c_void_p]),
+    ("shz_tree_error", C.c_char_p, []),
+    ("shz_tree_adapt", C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_void_p, C.POINTER(C.c_int32)]),
+    ("shz_tree_last_steps", C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]),
+    ("shz_tree_replay", C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.POINTER(C.c_int32)]),
+    ("shz_tree_refine", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    ("shz_tree_neighbor", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.c_int32, C.POINTER(C.c_int32),
+                                    C.POINTER(C.c_int32)]),
+    ("shz_tree_table", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("shz_tree_lists", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_int32),
+                                 C.POINTER(C.c_int32)]),
+    ("shz_tree_index_grid_size", C.c_int64, [C.c_void_p]),
+    ("shz_tree_index_grid", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("shz_tree_stats", C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                 C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     ("shz_totals_noalloc", C.c_int, [C.POINTER(shz_config), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("shz_totals_noalloc_error", C.c_char_p, []),
 ]

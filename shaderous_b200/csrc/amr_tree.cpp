@@ -1,0 +1,529 @@
+// Host block tree: the decisions of the reference's src/amr/tree.ts, slot for slot.
+// Citations are to that file. The reference keeps its tables up to date incrementally between
+// re-meshes; the tables here are rebuilt whole on each read, which gives the same arrays (the
+// reference's own test "keeps its block table and index grid up to date across re-meshes"
+// asserts that equality).
+#include "amr_tree.h"
+
+#include <algorithm>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+
+namespace shz {
+namespace amr {
+
+// tree.ts:139-184 constructor: the free stack holds cap-1 .. 0 with slot 0 on top, so slots are
+// taken lowest first and a freed slot goes back on top.
+BlockTree::BlockTree(int ndim_, int nr_, int max_level_, int cap_, const int lo[3], const int hi[3], bool edge,
+                     const int* lim_)
+    : ndim(ndim_), nr(nr_), max_level(max_level_), cap(cap_), level_limit(max_level_), nchild(1 << ndim_),
+      nface(2 * ndim_), edge_balance(edge) {
+  for (int a = 0; a < 3; a++) {
+    bc_lo[a] = lo[a];
+    bc_hi[a] = hi[a];
+    lim[a] = lim_ ? lim_[a] : nr;
+  }
+  if (edge) {
+    for (int a = 0; a < ndim; a++)
+      for (int b = a + 1; b < ndim; b++)
+        for (int sa : {-1, 1})
+          for (int sb : {-1, 1}) {
+            std::array<int, 3> d = {0, 0, 0};
+            d[a] = sa;
+            d[b] = sb;
+            diagonals_.push_back(d);
+          }
+  }
+  span_ = (int64_t)nr << max_level;
+  slots_.assign(cap, nullptr);
+  for (int s = cap - 1; s >= 0; s--) free_.push_back(s);
+  const int nz = ndim == 3 ? lim[2] : 1;
+  const int nroot = lim[0] * (ndim >= 2 ? lim[1] : 1) * nz;
+  if (nroot > cap)
+    throw std::runtime_error("block budget " + std::to_string(cap) + " is smaller than the " + std::to_string(nroot) +
+                             " root blocks");
+  for (int k = 0; k < nz; k++)
+    for (int j = 0; j < (ndim >= 2 ? lim[1] : 1); j++)
+      for (int i = 0; i < lim[0]; i++) {
+        const int c[3] = {i, j, k};
+        create(0, c, nullptr);
+      }
+}
+
+int64_t BlockTree::key(int level, int c0, int c1, int c2) const {
+  return (((int64_t)level * span_ + c2) * span_ + c1) * span_ + c0;
+}
+
+Block* BlockTree::create(int level, const int c[3], Block* parent) {
+  const int slot = free_.back();
+  free_.pop_back();
+  if (slot > high_slot) high_slot = slot;
+  arena_.push_back(Block{slot, level, {c[0], c[1], c[2]}, parent, {}});
+  Block* b = &arena_.back();
+  slots_[slot] = b;
+  blocks_[key(level, c[0], c[1], c[2])] = b;
+  return b;
+}
+
+void BlockTree::remove(Block* b) {
+  blocks_.erase(key(b->level, b->c[0], b->c[1], b->c[2]));
+  slots_[b->slot] = nullptr;
+  free_.push_back(b->slot);
+}
+
+bool BlockTree::live(const Block* b) const {
+  auto it = blocks_.find(key(b->level, b->c[0], b->c[1], b->c[2]));
+  return it != blocks_.end() && it->second == b;
+}
+
+std::vector<Block*> BlockTree::all() const {
+  std::vector<std::vector<Block*>> by(max_level + 1);
+  for (Block* b : slots_)
+    if (b) by[b->level].push_back(b);
+  std::vector<Block*> out;
+  for (auto& v : by) out.insert(out.end(), v.begin(), v.end());
+  return out;
+}
+
+std::vector<Block*> BlockTree::leaves() const {
+  std::vector<Block*> out;
+  for (Block* b : all())
+    if (b->leaf()) out.push_back(b);
+  return out;
+}
+
+Block* BlockTree::get(int level, const int c[3]) const {
+  auto it = blocks_.find(key(level, c[0], c[1], ndim == 3 ? c[2] : 0));
+  return it == blocks_.end() ? nullptr : it->second;
+}
+
+// tree.ts:283-304 neighbor.
+Neighbor BlockTree::neighbor(const Block* b, int f) const {
+  const int axis = f >> 1;
+  int c[3] = {b->c[0], b->c[1], b->c[2]};
+  const int step = (f & 1) ? 1 : -1;
+  const int n = lim[axis] << b->level;
+  int v = c[axis] + step;
+  if (v < 0 || v >= n) {
+    const int type = (f & 1) ? bc_hi[axis] : bc_lo[axis];
+    if (type != 0) return {NbKind::Bc, nullptr, type};
+    v = (v + n) % n;
+  }
+  c[axis] = v;
+  auto it = blocks_.find(key(b->level, c[0], c[1], c[2]));
+  if (it != blocks_.end()) return {NbKind::Same, it->second, 0};
+  if (b->level > 0) {
+    auto co = blocks_.find(key(b->level - 1, c[0] >> 1, c[1] >> 1, c[2] >> 1));
+    if (co != blocks_.end()) return {NbKind::Coarse, co->second, 0};
+  }
+  throw std::runtime_error("2:1 balance broken at level " + std::to_string(b->level) + " face " + std::to_string(f));
+}
+
+// tree.ts:311-329 atOffset.
+Block* BlockTree::at_offset(const Block* b, const int d[3]) const {
+  int c[3] = {b->c[0], b->c[1], b->c[2]};
+  for (int a = 0; a < 3; a++) {
+    if (!d[a]) continue;
+    const int n = lim[a] << b->level;
+    int v = c[a] + d[a];
+    if (v < 0 || v >= n) {
+      if ((d[a] > 0 ? bc_hi[a] : bc_lo[a]) != 0) return nullptr;
+      v = (v + n) % n;
+    }
+    c[a] = v;
+  }
+  for (int l = b->level; l >= 0; l--) {
+    const int s = b->level - l;
+    auto it = blocks_.find(key(l, c[0] >> s, c[1] >> s, c[2] >> s));
+    if (it != blocks_.end()) return it->second;
+  }
+  return nullptr;
+}
+
+// tree.ts:332-343 coarserAround.
+std::vector<Block*> BlockTree::coarser_around(const Block* b) const {
+  std::vector<Block*> out;
+  for (int f = 0; f < nface; f++) {
+    Neighbor nb = neighbor(b, f);
+    if (nb.kind == NbKind::Coarse) out.push_back(nb.block);
+  }
+  for (const auto& d : diagonals_) {
+    Block* q = at_offset(b, d.data());
+    if (q && q->level < b->level) out.push_back(q);
+  }
+  return out;
+}
+
+// tree.ts:346-352 refineCost.
+int BlockTree::refine_cost(const Block* b, std::unordered_set<const Block*>& seen) const {
+  if (seen.count(b) || !b->leaf()) return 0;
+  seen.insert(b);
+  int cost = nchild;
+  for (Block* q : coarser_around(b)) cost += refine_cost(q, seen);
+  return cost;
+}
+
+int BlockTree::cost_to_refine(const std::vector<Block*>& list) const {
+  std::unordered_set<const Block*> seen;
+  int cost = 0;
+  for (Block* b : list) cost += refine_cost(b, seen);
+  return cost;
+}
+
+// tree.ts:366-386 refine: split a leaf, first splitting coarser neighbours so balance holds.
+std::vector<Block*> BlockTree::refine(Block* b, const std::unordered_set<Block*>* forbidden) {
+  std::vector<Block*> done;
+  if (!b->leaf() || b->level >= level_limit) return done;
+  std::unordered_set<const Block*> need;
+  if (refine_cost(b, need) > (int)free_.size()) return done;
+  if (forbidden)
+    for (const Block* q : need)
+      if (forbidden->count(const_cast<Block*>(q))) return done;
+  std::function<void(Block*)> split = [&](Block* q) {
+    if (!q->leaf()) return;
+    const std::vector<Block*> around = coarser_around(q);
+    for (Block* nb : around) split(nb);
+    if (!q->leaf()) return;
+    q->children.reserve(nchild);
+    for (int o = 0; o < nchild; o++) {
+      const int c[3] = {2 * q->c[0] + (o & 1), 2 * q->c[1] + ((o >> 1) & 1), ndim == 3 ? 2 * q->c[2] + ((o >> 2) & 1) : 0};
+      q->children.push_back(create(q->level + 1, c, q));
+    }
+    done.push_back(q);
+  };
+  split(b);
+  return done;
+}
+
+// tree.ts:389-402 canCoarsen.
+bool BlockTree::can_coarsen(const Block* p) const {
+  if (p->leaf()) return false;
+  for (const Block* ch : p->children)
+    if (!ch->leaf()) return false;
+  for (const Block* ch : p->children) {
+    for (int f = 0; f < nface; f++) {
+      Neighbor nb = neighbor(ch, f);
+      if (nb.kind == NbKind::Same && !nb.block->leaf()) return false;
+    }
+    for (const auto& d : diagonals_) {
+      const Block* q = at_offset(ch, d.data());
+      if (q && q->level == ch->level && !q->leaf()) return false;
+    }
+  }
+  return true;
+}
+
+// tree.ts:404-409 coarsen.
+void BlockTree::coarsen(Block* p) {
+  for (Block* ch : p->children) remove(ch);
+  p->children.clear();
+}
+
+// tree.ts:420-430 evictable: parents with only leaf children, scored by their most strongly
+// flagged child; the lowest tier first, then the least flagged (a stable sort, as Array.sort).
+std::vector<BlockTree::Evictable> BlockTree::evictable(const std::vector<Block*>& lv,
+                                                       const std::unordered_map<const Block*, double>& ind,
+                                                       const std::function<double(const Block*)>& tier) const {
+  std::vector<Block*> parents;
+  std::unordered_set<const Block*> seen;
+  for (Block* b : lv)
+    if (b->parent && seen.insert(b->parent).second) parents.push_back(b->parent);
+  std::vector<Evictable> out;
+  for (Block* p : parents) {
+    if (p->leaf()) continue;
+    bool any = false;
+    for (Block* ch : p->children) any |= !ch->leaf();
+    if (any) continue;
+    double score = -std::numeric_limits<double>::infinity();
+    for (Block* ch : p->children) {
+      auto it = ind.find(ch);
+      score = std::max(score, it == ind.end() ? 0.0 : it->second);
+    }
+    out.push_back({p, score, tier ? tier(p) : NO_TIER});
+  }
+  std::stable_sort(out.begin(), out.end(), [](const Evictable& a, const Evictable& b) {
+    if (a.tier == b.tier) return a.score < b.score;
+    return a.tier > b.tier;
+  });
+  return out;
+}
+
+// tree.ts:433-442 near.
+bool BlockTree::near(const Block* a, const Block* q) const {
+  const int64_t sa = (int64_t)1 << (max_level - a->level);
+  const int64_t sq = (int64_t)1 << (max_level - q->level);
+  for (int i = 0; i < ndim; i++) {
+    const int64_t lo = a->c[i] * sa;
+    const int64_t qlo = (q->c[i] - 1) * sq;
+    if (lo + sa <= qlo || qlo + 3 * sq <= lo) return false;
+  }
+  return true;
+}
+
+// tree.ts:449-467 makeRoom.
+bool BlockTree::make_room(Block* b, double level, const std::vector<Evictable>& ev,
+                          const std::unordered_set<const Block*>& touched, double tier, std::vector<Block*>& out) {
+  out.clear();
+  if (!b->leaf() || b->level >= level_limit) return false;
+  std::unordered_set<const Block*> need;
+  int shortage = refine_cost(b, need) - (int)free_.size();
+  if (shortage <= 0) return false;
+  for (const Evictable& e : ev) {
+    Block* p = e.p;
+    if (e.tier < tier || (e.tier == tier && e.score >= EVICT_MARGIN * level)) break;
+    if (touched.count(p) || !live(p) || p->leaf()) continue;
+    bool bad = false;
+    for (Block* ch : p->children) bad |= !ch->leaf() || touched.count(ch) > 0;
+    if (bad) continue;
+    if (need.count(p)) continue;
+    bool close = false;
+    for (const Block* q : need)
+      if (near(p, q)) { close = true; break; }
+    if (close || !can_coarsen(p)) continue;
+    out.push_back(p);
+    shortage -= nchild;
+    if (shortage <= 0) return true;
+  }
+  out.clear();
+  return false;
+}
+
+namespace {
+// tree.ts:598-636 adaptRun: the bookkeeping of a re-mesh.
+struct Run {
+  BlockTree& t;
+  std::unordered_set<const Block*>& touched;
+  std::unordered_map<int, RegridOp> ops;
+  std::vector<std::vector<int>> steps;
+  std::unordered_set<Block*> evicted;
+
+  void merge(Block* p) {
+    RegridOp op;
+    op.kind = RG_RESTRICT;
+    op.src = p->slot;
+    for (Block* ch : p->children) op.children.push_back(ch->slot);
+    if (t.ndim == 1) {
+      const std::vector<int> c = op.children;
+      op.children.insert(op.children.end(), c.begin(), c.end());
+    }
+    t.coarsen(p);
+    touched.insert(p);
+    ops[p->slot] = op;
+  }
+  bool step(int what, Block* b) {
+    std::vector<int> s = {what, b->level};
+    for (int a = 0; a < t.ndim; a++) s.push_back(b->c[a]);
+    steps.push_back(s);
+    if (what == ADAPT_REFINE) {
+      const std::vector<Block*> split = t.refine(b, &evicted);
+      for (Block* q : split) {
+        touched.insert(q);
+        for (int o = 0; o < (int)q->children.size(); o++) {
+          touched.insert(q->children[o]);
+          RegridOp op;
+          op.kind = RG_PROLONG;
+          op.src = q->slot;
+          op.octant = o;
+          ops[q->children[o]->slot] = op;
+        }
+      }
+      return !split.empty();
+    }
+    merge(b);
+    if (what == ADAPT_EVICT) evicted.insert(b);
+    return true;
+  }
+  std::vector<RegridOp> table() {
+    std::vector<RegridOp> out;
+    if (ops.empty()) return out;
+    out.assign(t.cap, RegridOp());
+    for (Block* leaf : t.leaves()) {
+      auto it = ops.find(leaf->slot);
+      if (it != ops.end()) {
+        out[leaf->slot] = it->second;
+      } else {
+        RegridOp op;
+        op.kind = RG_COPY;
+        op.src = leaf->slot;
+        out[leaf->slot] = op;
+      }
+    }
+    return out;
+  }
+};
+}  // namespace
+
+// tree.ts:489-544 adapt.
+std::vector<RegridOp> BlockTree::adapt(const std::function<double(const Block*)>& indicator, double hi, double lo,
+                                       const std::function<double(const Block*)>& tier) {
+  const std::vector<Block*> before = leaves();
+  std::unordered_map<const Block*, double> ind, tiers;
+  for (Block* b : before) {
+    const double t = tier ? tier(b) : NO_TIER;
+    tiers[b] = t;
+    const double raw = indicator(b);
+    ind[b] = (t < NO_TIER && raw >= 0) ? std::max(raw, ZONE_INDICATOR) : raw;
+  }
+  std::unordered_set<const Block*> touched;
+  Run run{*this, touched, {}, {}, {}};
+
+  std::vector<Block*> wanted;
+  for (Block* b : before)
+    if (ind[b] > hi && b->level < level_limit) wanted.push_back(b);
+  std::stable_sort(wanted.begin(), wanted.end(), [&](Block* a, Block* b) {
+    const double ta = tiers[a], tb = tiers[b];
+    if (ta == tb) return ind[a] > ind[b];
+    return ta < tb;
+  });
+  bool have_ev = false;
+  std::vector<Evictable> ev;
+  std::vector<Block*> room;
+  for (Block* b : wanted) {
+    if (!b->leaf() || !live(b)) continue;
+    if (!run.step(ADAPT_REFINE, b)) {
+      if (!have_ev) {
+        ev = evictable(before, ind, tier);
+        have_ev = true;
+      }
+      if (make_room(b, ind[b], ev, touched, tiers[b], room)) {
+        for (Block* p : room) run.step(ADAPT_EVICT, p);
+        run.step(ADAPT_REFINE, b);
+      }
+    }
+  }
+
+  auto ind_of = [&](const Block* b) {
+    auto it = ind.find(b);
+    return it == ind.end() ? 0.0 : it->second;
+  };
+  auto hot = [&](const Block* b) {
+    if (ind_of(b) > lo) return true;
+    auto tt = tiers.find(b);
+    if (tt != tiers.end() && tt->second < NO_TIER) return true;
+    if (ind_of(b) < 0) return false;
+    for (int f = 0; f < nface; f++) {
+      Neighbor nb = neighbor(b, f);
+      if (nb.kind != NbKind::Bc && ind_of(nb.block) > hi) return true;
+    }
+    return false;
+  };
+  std::vector<Block*> parents;
+  std::unordered_set<const Block*> seen;
+  for (Block* b : before)
+    if (b->parent && seen.insert(b->parent).second) parents.push_back(b->parent);
+  for (Block* p : parents) {
+    if (touched.count(p) || !live(p) || p->leaf()) continue;
+    bool skip = false;
+    for (Block* ch : p->children) skip |= touched.count(ch) > 0 || !ch->leaf();
+    if (skip) continue;
+    bool any_hot = false;
+    for (Block* ch : p->children)
+      if (hot(ch)) { any_hot = true; break; }
+    if (any_hot || !can_coarsen(p)) continue;
+    run.step(ADAPT_MERGE, p);
+  }
+  last_steps = run.steps;
+  return run.table();
+}
+
+// tree.ts:579-589 replayAdapt.
+std::vector<RegridOp> BlockTree::replay_adapt(const std::vector<std::vector<int>>& steps) {
+  std::unordered_set<const Block*> touched;
+  Run run{*this, touched, {}, {}, {}};
+  for (const auto& s : steps) {
+    int c[3] = {0, 0, 0};
+    for (int a = 0; a < ndim; a++) c[a] = s[2 + a];
+    Block* b = get(s[1], c);
+    if (!b) throw std::runtime_error("a re-mesh to replay acts on a block the mesh does not have");
+    run.step(s[0], b);
+  }
+  last_steps = run.steps;
+  return run.table();
+}
+
+// tree.ts:654-679 writeRow, for every slot.
+void BlockTree::table(int32_t* t) const {
+  for (int slot = 0; slot < cap; slot++) {
+    int32_t* o = t + (size_t)slot * BT_STRIDE;
+    for (int i = 0; i < BT_STRIDE; i++) o[i] = -1;
+    o[4] = 0;
+    const Block* b = slots_[slot];
+    if (!b) continue;
+    o[0] = b->level;
+    o[1] = b->c[0];
+    o[2] = b->c[1];
+    o[3] = b->c[2];
+    o[4] = FLAG_ACTIVE | (b->leaf() ? FLAG_LEAF : 0);
+    o[5] = b->parent ? b->parent->slot : -1;
+    for (int f = 0; f < 6; f++) {
+      if (f >= nface) {
+        o[6 + f] = b->slot;
+        continue;
+      }
+      Neighbor nb = neighbor(b, f);
+      if (nb.kind == NbKind::Same) {
+        o[6 + f] = nb.block->slot;
+      } else if (nb.kind == NbKind::Coarse) {
+        o[6 + f] = NB_COARSE;
+        o[20 + f] = nb.block->slot;
+      } else {
+        o[6 + f] = -1 - nb.type;
+      }
+    }
+    for (size_t i = 0; i < b->children.size(); i++) o[12 + i] = b->children[i]->slot;
+    if (!b->leaf() && ndim == 1)
+      for (size_t i = 0; i < b->children.size(); i++) o[14 + i] = b->children[i]->slot;
+  }
+}
+
+// tree.ts:681-693 regridTable.
+void BlockTree::regrid_table(const std::vector<RegridOp>& ops, int cap, int32_t* t) {
+  std::memset(t, 0, sizeof(int32_t) * (size_t)cap * RG_STRIDE);
+  for (int slot = 0; slot < (int)ops.size() && slot < cap; slot++) {
+    const RegridOp& op = ops[slot];
+    if (op.kind == RG_NONE) continue;
+    int32_t* o = t + (size_t)slot * RG_STRIDE;
+    o[0] = op.kind;
+    o[1] = op.src;
+    o[2] = op.octant;
+    for (size_t i = 0; i < op.children.size() && i < 8; i++) o[4 + i] = op.children[i];
+  }
+}
+
+// tree.ts:695-715 lists.
+void BlockTree::lists(std::vector<int32_t>& a, std::vector<int32_t>& lv, std::vector<int32_t>& per_level) const {
+  a.clear();
+  lv.clear();
+  per_level.assign(max_level + 1, 0);
+  for (const Block* b : all()) {
+    a.push_back(b->slot);
+    per_level[b->level]++;
+    if (b->leaf()) lv.push_back(b->slot);
+  }
+}
+
+int64_t BlockTree::index_grid_size() const {
+  const int64_t m = (int64_t)nr << max_level;
+  return ndim == 1 ? m : (ndim == 2 ? m * m : m * m * m);
+}
+
+// tree.ts:721-816 indexGrid (the whole grid; every cell lies in exactly one leaf).
+void BlockTree::index_grid(uint32_t* g) const {
+  const int64_t m = (int64_t)nr << max_level;
+  for (const Block* b : slots_) {
+    if (!b || !b->leaf()) continue;
+    const int64_t span = (int64_t)1 << (max_level - b->level);
+    if (ndim == 1) {
+      for (int64_t x = b->c[0] * span; x < (b->c[0] + 1) * span; x++) g[x] = b->slot;
+      continue;
+    }
+    const int64_t z0 = ndim == 3 ? b->c[2] * span : 0;
+    for (int64_t k = z0; k < z0 + (ndim == 3 ? span : 1); k++)
+      for (int64_t j = b->c[1] * span; j < (b->c[1] + 1) * span; j++)
+        for (int64_t x = b->c[0] * span; x < (b->c[0] + 1) * span; x++) g[(k * m + j) * m + x] = b->slot;
+  }
+}
+
+}  // namespace amr
+}  // namespace shz
