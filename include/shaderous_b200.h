@@ -232,6 +232,55 @@ int shz_tree_index_grid(const shz_tree* t, uint32_t* out);             /* leaf s
 /* count, free slots, leaves, deepest level, highest slot used */
 int shz_tree_stats(const shz_tree* t, int32_t* blocks, int32_t* free_slots, int32_t* leaves, int32_t* deepest, int32_t* high_slot);
 
+/*
+ * A run on the adaptive block grid: replaces AmrSim (src/amr/amr_sim.ts:178) behind the same
+ * Simulation interface. The domain is a cube of side `box` (centred on 0) covered by nr^ndim
+ * root blocks of 16^ndim cells, refined up to max_level levels in a budget of `cap` block slots.
+ * A step is assemble -> clock -> predict -> update (src/amr/amr_sim.ts:2709-2946), captured as
+ * one CUDA graph; every regrid_every steps (REGRID_EVERY = 8, amr_sim.ts:73) the Löhner
+ * indicator (amr/flag.wgsl) drives BlockTree.adapt and the new leaves are filled
+ * (amr/regrid.wgsl). Limiters minmod, mc, vanleer and koren (PPM needs a third ghost layer).
+ */
+typedef struct shz_amr_config {
+  shz_config hydro;     /* physics and boundaries; n[] and dx are ignored */
+  int32_t ndim;         /* 2 or 3 */
+  int32_t nr;           /* root blocks per side */
+  int32_t max_level;    /* deepest level (0..7) */
+  int32_t cap;          /* block slots (leaves and parents) */
+  double box;           /* side of the domain; level-0 cell size box / (16 nr) */
+  double refine_hi;     /* refine leaves whose indicator exceeds this */
+  double refine_lo;     /* merge siblings whose indicators are all below this */
+  int32_t regrid_every; /* steps between refinement checks (0: never) */
+} shz_amr_config;
+typedef struct shz_amr shz_amr;
+
+int shz_amr_create(const shz_amr_config* cfg, shz_amr** out);
+void shz_amr_destroy(shz_amr* a);
+const char* shz_amr_error(const shz_amr* a);
+/* Initial conditions of a built-in problem on the adaptive grid: the mesh is built by up to
+ * max_level passes of adapt() over the sampled state (amr_sim.ts:1924-2100), each leaf sampled at
+ * its own cell centres; blocks that a problem's discontinuity crosses count as flagged. */
+int shz_amr_reset_problem(shz_amr* a, const shz_problem* prob);
+int shz_amr_step(shz_amr* a, int32_t n);
+int shz_amr_run(shz_amr* a, const shz_run_opts* opts, shz_run_result* res);
+int shz_amr_diagnostics(shz_amr* a, shz_diag* out);
+int shz_amr_clock(shz_amr* a, double* t, double* dt, int64_t* steps);
+/* Run the refinement check now (flag, adapt, regrid); *changed = 1 if the mesh changed. */
+int shz_amr_regrid(shz_amr* a, int32_t* changed);
+/* The leaves, coarsest first (lists().leaves): slots, levels and block coordinates (3 per leaf). */
+int shz_amr_leaves(shz_amr* a, int32_t* n_leaves, int32_t* slots, int32_t* levels, int32_t* coords);
+/* The block table on the device (cap * 32 ints), read back: the same as the tree's. */
+int shz_amr_table(shz_amr* a, int32_t* out);
+/* State of the leaves in lists().leaves order: 16^ndim cells each, x fastest, float4 u1 and u2. */
+int shz_amr_get_leaves_state(shz_amr* a, float* u1, float* u2);
+/* The last refinement indicators per slot (cap floats). */
+int shz_amr_flags(shz_amr* a, float* out);
+/* The device's ghost classification of block `slot`: (kind, source slot, l0, l1, l2) for each of
+ * the 20^ndim texels of its primitive region, x fastest (amr/grid.wgsl ghost_src). */
+int shz_amr_ghost_map(shz_amr* a, int32_t slot, int32_t* out);
+int shz_amr_profile(shz_amr* a, int32_t n, shz_profile_result* out);
+int64_t shz_amr_kernel_launches(const shz_amr* a);
+
 /* Launches of the library's own kernels on this handle since creation. */
 int64_t shz_kernel_launches(const shz_sim* sim);
 

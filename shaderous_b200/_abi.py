@@ -85,6 +85,20 @@ class shz_problem(C.Structure):
     _fields_ = [("kind", C.c_int32), ("axis", C.c_int32), ("seed", C.c_uint64), ("a", C.c_double * 8)]
 
 
+class shz_amr_config(C.Structure):
+    _fields_ = [
+        ("hydro", shz_config),
+        ("ndim", C.c_int32),
+        ("nr", C.c_int32),
+        ("max_level", C.c_int32),
+        ("cap", C.c_int32),
+        ("box", C.c_double),
+        ("refine_hi", C.c_double),
+        ("refine_lo", C.c_double),
+        ("regrid_every", C.c_int32),
+    ]
+
+
 class shz_profile_result(C.Structure):
     _fields_ = [("steps", C.c_int32), ("total_ms", C.c_double), ("sweep_ms", C.c_double), ("launches", C.c_int64)]
 
@@ -127,6 +141,22 @@ SIGNATURES = [
     ("shz_tree_index_grid", C.c_int, [C.c_void_p, C.c_void_p]),
     ("shz_tree_stats", C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                  C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    ("shz_amr_create", C.c_int, [C.POINTER(shz_amr_config), C.POINTER(C.c_void_p)]),
+    ("shz_amr_destroy", None, [C.c_void_p]),
+    ("shz_amr_error", C.c_char_p, [C.c_void_p]),
+    ("shz_amr_reset_problem", C.c_int, [C.c_void_p, C.POINTER(shz_problem)]),
+    ("shz_amr_step", C.c_int, [C.c_void_p, C.c_int32]),
+    ("shz_amr_run", C.c_int, [C.c_void_p, C.POINTER(shz_run_opts), C.POINTER(shz_run_result)]),
+    ("shz_amr_diagnostics", C.c_int, [C.c_void_p, C.POINTER(shz_diag)]),
+    ("shz_amr_clock", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
+    ("shz_amr_regrid", C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
+    ("shz_amr_leaves", C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("shz_amr_table", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("shz_amr_get_leaves_state", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("shz_amr_flags", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("shz_amr_ghost_map", C.c_int, [C.c_void_p, C.c_int32, C.c_void_p]),
+    ("shz_amr_profile", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(shz_profile_result)]),
+    ("shz_amr_kernel_launches", C.c_int64, [C.c_void_p]),
     ("shz_totals_noalloc", C.c_int, [C.POINTER(shz_config), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("shz_totals_noalloc_error", C.c_char_p, []),
 ]

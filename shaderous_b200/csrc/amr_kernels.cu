@@ -1,0 +1,850 @@
+// The passes of one step on the adaptive block grid, as persistent work-list kernels.
+//
+// A block holds 16^ndim cells. Three atlases live in HBM, slot-major, with x fastest:
+//   - the conserved state: two parities of 16^ndim cells x (u1, u2) float4;
+//   - the primitives with two ghost layers: 20^ndim cells x (w1 = rho, v; w2 = p, s, cs, 0);
+//   - the half-step states over the block and one ghost layer: 18^ndim cells x
+//     (p1 = rho, v; p2 = p, s, shock flag, first-order flag).
+// One step is four kernels, captured in a CUDA graph by the host:
+//   1. amr_assemble over every block (leaves and parents): primitives with ghost fill.
+//   2. clock_kernel: dt.
+//   3. amr_predict over the leaves: half steps.
+//   4. amr_update over the leaves: fluxes, fine-flux matching and the update.
+// This follows the reference's AmrSim.encodeSteps (src/amr/amr_sim.ts:2709-2946), and its rules
+// for the ghost fill (amr/grid.wgsl:186-222 ghost_src; amr/cons.wgsl:19-125 restriction and
+// prolongation; amr/assemble.wgsl:47-75 from_coarse), the predictor at the source
+// (amr/predict.wgsl:184-221) and the matching of coarse faces to the mean of the fine fluxes
+// (amr/update.wgsl:207-295). Every kernel walks a device list of block slots with a fixed grid of
+// CTAs, one block at a time per CTA.
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "amr_kernels.h"
+#include "hydro_cell.cuh"
+#include "hydro_math.cuh"
+
+namespace shz {
+namespace amrk {
+
+constexpr int BS = 16, NG = 2, PAD = BS + 2 * NG, PP = BS + 2, BTS = 32, RGS = 12;
+constexpr int NT = 256;  // threads per CTA
+
+template <int DIM>
+struct BG {
+  static constexpr int CB = DIM == 3 ? BS * BS * BS : BS * BS;       // cells per block
+  static constexpr int WN = DIM == 3 ? PAD * PAD * PAD : PAD * PAD;  // primitive texels per slot
+  static constexpr int PN = DIM == 3 ? PP * PP * PP : PP * PP;       // half-step texels per slot
+};
+
+__device__ __forceinline__ int bt_at(const int* __restrict__ bt, int slot, int i) { return __ldg(bt + slot * BTS + i); }
+__device__ __forceinline__ bool leaf_of(const int* __restrict__ bt, int slot) { return (bt_at(bt, slot, 4) & 2) != 0; }
+
+template <int DIM>
+__device__ __forceinline__ int cell_ix(const int* l) {
+  return DIM == 3 ? (l[2] * BS + l[1]) * BS + l[0] : l[1] * BS + l[0];
+}
+template <int DIM>
+__device__ __forceinline__ int wtex(const int* l) {
+  return DIM == 3 ? ((l[2] + NG) * PAD + (l[1] + NG)) * PAD + (l[0] + NG) : (l[1] + NG) * PAD + (l[0] + NG);
+}
+template <int DIM>
+__device__ __forceinline__ int ptex(const int* l) {
+  return DIM == 3 ? ((l[2] + 1) * PP + (l[1] + 1)) * PP + (l[0] + 1) : (l[1] + 1) * PP + (l[0] + 1);
+}
+
+// Where the value of a (possibly ghost) cell of a block comes from (amr/grid.wgsl:186-222):
+// kind 0 a cell at the same level (the block's own, a neighbour's, or its image across a
+// boundary of the domain, with velocity signs), kind 1 beyond a face whose neighbour is one
+// level coarser (slot = that coarser leaf), kind 2 an edge or corner ghost.
+struct Src {
+  int kind, slot;
+  int l[3];
+  float flip[3];
+};
+
+template <int DIM>
+__device__ __forceinline__ Src ghost_src(const int* __restrict__ bt, int slot, const int* l) {
+  Src s;
+  s.kind = 0;
+  s.slot = slot;
+  s.l[0] = l[0]; s.l[1] = l[1]; s.l[2] = l[2];
+  s.flip[0] = s.flip[1] = s.flip[2] = 1.f;
+  int out = 0, axis = 0;
+#pragma unroll
+  for (int a = 0; a < DIM; a++)
+    if (l[a] < 0 || l[a] >= BS) { out++; axis = a; }
+  if (out == 0) return s;
+  if (out > 1) { s.kind = 2; return s; }
+  const int upper = l[axis] >= BS ? 1 : 0;
+  const int nb = bt_at(bt, slot, 6 + 2 * axis + upper);
+  if (nb >= 0) {
+    s.slot = nb;
+    s.l[axis] = l[axis] + (upper ? -BS : BS);
+  } else if (nb == -1) {
+    s.kind = 1;
+    s.slot = bt_at(bt, slot, 20 + 2 * axis + upper);
+  } else {
+    // a face of the domain of kind -1 - nb (hydro/boundary.wgsl:47-52): mirror image beyond a
+    // wall, the edge cell beyond an outflow face
+    const int k = -1 - nb;
+    if (k == 2) {
+      s.l[axis] = upper ? 2 * BS - 1 - l[axis] : -1 - l[axis];
+      s.flip[axis] = -1.f;
+    } else {
+      s.l[axis] = upper ? BS - 1 : 0;
+    }
+  }
+  return s;
+}
+
+// An edge or corner ghost takes the value of the face ghost beside it: the cell clamped into the
+// block along every out-of-range axis but the first. (Nothing in the scheme reads these except
+// the shock flag of a rim ghost next to a coarser block.)
+template <int DIM>
+__device__ __forceinline__ Src ghost_src_any(const int* __restrict__ bt, int slot, const int* l) {
+  Src s = ghost_src<DIM>(bt, slot, l);
+  if (s.kind != 2) return s;
+  int m[3] = {l[0], l[1], l[2]};
+  bool first = true;
+#pragma unroll
+  for (int a = 0; a < DIM; a++)
+    if (m[a] < 0 || m[a] >= BS) {
+      if (first) first = false;
+      else m[a] = min(max(m[a], 0), BS - 1);
+    }
+  return ghost_src<DIM>(bt, slot, m);
+}
+
+struct Cons {
+  float4 a, b;
+};
+
+// The conserved state of cell l of a same-level block (amr/cons.wgsl:19-43 u_at): a leaf's own
+// cell, or the mean of the 2^ndim cells of the leaf child under it.
+template <int DIM>
+__device__ __forceinline__ Cons u_at(const int* __restrict__ bt, const float4* __restrict__ u1, const float4* __restrict__ u2,
+                                     int slot, const int* lin) {
+  // (the index is inside the block by construction; clamped so that no table can send a read
+  // outside the atlas)
+  const int l[3] = {min(max(lin[0], 0), BS - 1), min(max(lin[1], 0), BS - 1), DIM == 3 ? min(max(lin[2], 0), BS - 1) : 0};
+  if (leaf_of(bt, slot)) {
+    const size_t o = (size_t)slot * BG<DIM>::CB + cell_ix<DIM>(l);
+    return Cons{__ldg(u1 + o), __ldg(u2 + o)};
+  }
+  int h[3] = {l[0] >= BS / 2, l[1] >= BS / 2, DIM == 3 ? (l[2] >= BS / 2) : 0};
+  const int ch = bt_at(bt, slot, 12 + (h[0] | (h[1] << 1) | (h[2] << 2)));
+  if (ch < 0 || !leaf_of(bt, ch)) return Cons{make_float4(1.f, 0.f, 0.f, 0.f), make_float4(1.f, 1.f, 0.f, 0.f)};
+  float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a;
+  const int nz = DIM == 3 ? 2 : 1;
+  for (int k = 0; k < nz; k++)
+    for (int j = 0; j < 2; j++)
+      for (int i = 0; i < 2; i++) {
+        int f[3] = {2 * (l[0] - (BS / 2) * h[0]) + i, 2 * (l[1] - (BS / 2) * h[1]) + j,
+                    DIM == 3 ? 2 * (l[2] - (BS / 2) * h[2]) + k : 0};
+        const size_t o = (size_t)ch * BG<DIM>::CB + cell_ix<DIM>(f);
+        const float4 x = __ldg(u1 + o), y = __ldg(u2 + o);
+        a.x += x.x; a.y += x.y; a.z += x.z; a.w += x.w;
+        b.x += y.x; b.y += y.y; b.z += y.z; b.w += y.w;
+      }
+  const float w = DIM == 3 ? 0.125f : 0.25f;
+  return Cons{make_float4(a.x * w, a.y * w, a.z * w, a.w * w), make_float4(b.x * w, b.y * w, b.z * w, b.w * w)};
+}
+
+// amr/cons.wgsl u_near: the conserved state of a kind-0 cell near a coarse block, with the
+// boundary's velocity signs.
+template <int DIM>
+__device__ __forceinline__ bool u_near(const int* __restrict__ bt, const float4* __restrict__ u1, const float4* __restrict__ u2,
+                                       int slot, const int* l, Cons& u) {
+  const Src s = ghost_src<DIM>(bt, slot, l);
+  if (s.kind != 0) return false;
+  u = u_at<DIM>(bt, u1, u2, s.slot, s.l);
+  u.a.y *= s.flip[0];
+  u.a.z *= s.flip[1];
+  u.a.w *= s.flip[2];
+  return true;
+}
+
+// The prolongation's single slope per component (the limiter's limit4: MC for Koren and MC,
+// else the limiter itself; amr/cons.wgsl:53-66 slope_between with the product-rule momentum).
+template <int R>
+__device__ __forceinline__ float lim4(float a, float b) {
+  return limit<R == R_KOREN ? R_MC : R>(a, b, 0.f);
+}
+template <int R>
+__device__ __forceinline__ Cons slope_between(const Cons& c, const Cons& m, const Cons& p, float rho_floor) {
+  Cons s;
+  s.a.x = lim4<R>(c.a.x - m.a.x, p.a.x - c.a.x);
+  const float ic = 1.f / fmaxf(c.a.x, rho_floor), im = 1.f / fmaxf(m.a.x, rho_floor), ip = 1.f / fmaxf(p.a.x, rho_floor);
+  const float vc[3] = {c.a.y * ic, c.a.z * ic, c.a.w * ic};
+  const float vm[3] = {m.a.y * im, m.a.z * im, m.a.w * im};
+  const float vp[3] = {p.a.y * ip, p.a.z * ip, p.a.w * ip};
+  float sm[3];
+#pragma unroll
+  for (int i = 0; i < 3; i++) sm[i] = vc[i] * s.a.x + c.a.x * lim4<R>(vc[i] - vm[i], vp[i] - vc[i]);
+  s.a.y = sm[0]; s.a.z = sm[1]; s.a.w = sm[2];
+  s.b.x = lim4<R>(c.b.x - m.b.x, p.b.x - c.b.x);
+  s.b.y = lim4<R>(c.b.y - m.b.y, p.b.y - c.b.y);
+  s.b.z = lim4<R>(c.b.z - m.b.z, p.b.z - c.b.z);
+  s.b.w = lim4<R>(c.b.w - m.b.w, p.b.w - c.b.w);
+  return s;
+}
+
+struct Slopes {
+  Cons s[3];
+  float f;
+};
+
+// amr/cons.wgsl:78-125 prolong_slopes / prolong_child: limited slopes scaled back by one common
+// factor so that the children's density, energy and internal energy stay positive.
+template <int DIM, int R>
+__device__ __forceinline__ Slopes prolong_slopes(const Cons& uc, const Cons* m, const bool* mok, const Cons* p,
+                                                 const bool* pok, float rho_floor) {
+  Slopes sl;
+  float drop[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    sl.s[a] = Cons{make_float4(0.f, 0.f, 0.f, 0.f), make_float4(0.f, 0.f, 0.f, 0.f)};
+    if (a < DIM && mok[a] && pok[a]) sl.s[a] = slope_between<R>(uc, m[a], p[a], rho_floor);
+    drop[0] += fabsf(sl.s[a].a.x);
+    drop[1] += fabsf(sl.s[a].b.x);
+    drop[2] += fabsf(sl.s[a].b.y);
+  }
+  const float room[3] = {0.5f * fmaxf(uc.a.x, 0.f), 0.5f * fmaxf(uc.b.x, 0.f), 0.5f * fmaxf(uc.b.y, 0.f)};
+  float f = 1.f;
+#pragma unroll
+  for (int i = 0; i < 3; i++) f = fminf(f, fminf(1.f, room[i] / fmaxf(0.25f * drop[i], 1e-37f)));
+  sl.f = f;
+  return sl;
+}
+__device__ __forceinline__ Cons prolong_child(const Cons& uc, const Slopes& s, const int* par) {
+  const float o0 = s.f * (par[0] - 0.5f) * 0.5f, o1 = s.f * (par[1] - 0.5f) * 0.5f, o2 = s.f * (par[2] - 0.5f) * 0.5f;
+  Cons u;
+  u.a.x = uc.a.x + o0 * s.s[0].a.x + o1 * s.s[1].a.x + o2 * s.s[2].a.x;
+  u.a.y = uc.a.y + o0 * s.s[0].a.y + o1 * s.s[1].a.y + o2 * s.s[2].a.y;
+  u.a.z = uc.a.z + o0 * s.s[0].a.z + o1 * s.s[1].a.z + o2 * s.s[2].a.z;
+  u.a.w = uc.a.w + o0 * s.s[0].a.w + o1 * s.s[1].a.w + o2 * s.s[2].a.w;
+  u.b.x = uc.b.x + o0 * s.s[0].b.x + o1 * s.s[1].b.x + o2 * s.s[2].b.x;
+  u.b.y = uc.b.y + o0 * s.s[0].b.y + o1 * s.s[1].b.y + o2 * s.s[2].b.y;
+  u.b.z = uc.b.z + o0 * s.s[0].b.z + o1 * s.s[1].b.z + o2 * s.s[2].b.z;
+  u.b.w = uc.b.w + o0 * s.s[0].b.w + o1 * s.s[1].b.w + o2 * s.s[2].b.w;
+  return u;
+}
+
+// amr/assemble.wgsl:47-75 from_coarse: a ghost beyond a face whose neighbour is one level
+// coarser, prolonged from the coarse leaf `cs` with slopes from that leaf's neighbours.
+template <int DIM, int R>
+__device__ __forceinline__ Cons from_coarse(const int* __restrict__ bt, const float4* __restrict__ u1,
+                                            const float4* __restrict__ u2, int nr, int slot, const int* l, int cs,
+                                            float rho_floor) {
+  const int nc = nr * BS << bt_at(bt, cs, 0);
+  int gf[3], lc[3], par[3];
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    gf[a] = a < DIM ? bt_at(bt, slot, 1 + a) * BS + l[a] : 0;
+    int gc = gf[a] >> 1;
+    gc = ((gc % nc) + nc) % nc;
+    lc[a] = a < DIM ? gc - bt_at(bt, cs, 1 + a) * BS : 0;
+    par[a] = a < DIM ? (gf[a] & 1) : 0;
+  }
+  Cons uc, m[3], p[3];
+  bool mok[3] = {false, false, false}, pok[3] = {false, false, false};
+  if (!u_near<DIM>(bt, u1, u2, cs, lc, uc)) uc = Cons{make_float4(1.f, 0.f, 0.f, 0.f), make_float4(1.f, 1.f, 0.f, 0.f)};
+#pragma unroll
+  for (int a = 0; a < DIM; a++) {
+    int at[3] = {lc[0], lc[1], lc[2]};
+    at[a] -= 1;
+    mok[a] = u_near<DIM>(bt, u1, u2, cs, at, m[a]);
+    at[a] += 2;
+    pok[a] = u_near<DIM>(bt, u1, u2, cs, at, p[a]);
+  }
+  const Slopes sl = prolong_slopes<DIM, R>(uc, m, mok, p, pok, rho_floor);
+  return prolong_child(uc, sl, par);
+}
+
+__device__ __forceinline__ float warp_max_f(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ float block_max(float v, float* sRed) {
+  v = warp_max_f(v);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) sRed[warp] = v;
+  __syncthreads();
+  float m = lane < NT / 32 ? sRed[lane] : 0.f;
+  return warp_max_f(m);
+}
+__device__ __forceinline__ float rate_guard_f(float r) { return (r == r) ? r : __int_as_float(0x7f800000); }
+
+// 1. Primitives of every block in the list with two ghost layers; the rate / dx maximum over the
+// leaves' own cells (assemble.wgsl:78-154; PER_DX in clock.wgsl).
+template <int DIM, int R>
+__global__ void __launch_bounds__(NT) amr_assemble(const KParams P, const int* __restrict__ bt, int nr, double dx0,
+                                                   const int* __restrict__ list, int n, const float4* __restrict__ u1,
+                                                   const float4* __restrict__ u2, float4* __restrict__ w1,
+                                                   float4* __restrict__ w2, unsigned* __restrict__ rate_out) {
+  __shared__ float sRed[NT / 32];
+  float rmax = 0.f;
+  for (int i = blockIdx.x; i < n; i += gridDim.x) {
+    const int slot = __ldg(list + i);
+    const bool leaf = leaf_of(bt, slot);
+    const float inv_dx = (float)(ldexp(1.0, bt_at(bt, slot, 0)) / dx0);
+    for (int t = threadIdx.x; t < BG<DIM>::WN; t += NT) {
+      int l[3] = {t % PAD - NG, (t / PAD) % PAD - NG, DIM == 3 ? t / (PAD * PAD) - NG : 0};
+      const Src s = ghost_src_any<DIM>(bt, slot, l);
+      Cons u;
+      if (s.kind == 0) {
+        u = u_at<DIM>(bt, u1, u2, s.slot, s.l);
+        u.a.y *= s.flip[0];
+        u.a.z *= s.flip[1];
+        u.a.w *= s.flip[2];
+      } else {
+        u = from_coarse<DIM, R>(bt, u1, u2, nr, slot, s.l, s.slot, P.rho_floor);
+      }
+      float w[7];
+      prim_from_cons(u.a, u.b, P, 1.f, 1.f, 1.f, w);
+      const size_t o = (size_t)slot * BG<DIM>::WN + t;
+      w1[o] = make_float4(w[0], w[1], w[2], w[3]);
+      w2[o] = make_float4(w[4], w[5], w[6], 0.f);
+      bool inside = leaf;
+#pragma unroll
+      for (int a = 0; a < DIM; a++) inside = inside && l[a] >= 0 && l[a] < BS;
+      if (inside) rmax = fmaxf(rmax, rate_guard_f(fabsf(w[1]) + fabsf(w[2]) + fabsf(w[3]) + P.signal * w[6]) * inv_dx);
+    }
+  }
+  const float m = block_max(rmax, sRed);
+  if (threadIdx.x == 0) atomicMax(rate_out, __float_as_uint(m));
+}
+
+template <int DIM>
+__device__ __forceinline__ void load_w(const float4* __restrict__ w1, const float4* __restrict__ w2, int slot, const int* l,
+                                       float* w) {
+  const size_t o = (size_t)slot * BG<DIM>::WN + wtex<DIM>(l);
+  const float4 a = __ldg(w1 + o), b = __ldg(w2 + o);
+  w[0] = a.x; w[1] = a.y; w[2] = a.z; w[3] = a.w;
+  w[4] = b.x; w[5] = b.y; w[6] = b.z;
+}
+
+// 2. Half steps of every leaf over its cells and first ghost layer (predict.wgsl:184-221): a
+// same-level or boundary ghost is predicted at its source and mirrored; a ghost beside a coarser
+// block in place, its transverse slopes dropped at the rim of the face.
+template <int DIM, int R, bool ISEN>
+__global__ void __launch_bounds__(NT) amr_predict(const KParams P, const int* __restrict__ bt, double dx0,
+                                                  const int* __restrict__ list, int n, const float4* __restrict__ w1,
+                                                  const float4* __restrict__ w2, float4* __restrict__ p1,
+                                                  float4* __restrict__ p2, const DevClock* __restrict__ clk) {
+  const double dt = clk->dt;
+  for (int i = blockIdx.x; i < n; i += gridDim.x) {
+    const int slot = __ldg(list + i);
+    const float h = (float)((0.5 * dt) * ldexp(1.0, bt_at(bt, slot, 0)) / dx0);
+    for (int t = threadIdx.x; t < BG<DIM>::PN; t += NT) {
+      int l[3] = {t % PP - 1, (t / PP) % PP - 1, DIM == 3 ? t / (PP * PP) - 1 : 0};
+      const Src s = ghost_src<DIM>(bt, slot, l);
+      if (s.kind == 2) continue;
+      const bool at_source = s.kind == 0;
+      const int src = at_source ? s.slot : slot;
+      int c0[3] = {at_source ? s.l[0] : l[0], at_source ? s.l[1] : l[1], at_source ? s.l[2] : l[2]};
+      float mask[3] = {1.f, 1.f, 1.f};
+      if (!at_source)
+#pragma unroll
+        for (int a = 0; a < DIM; a++) mask[a] = (l[a] == 0 || l[a] == BS - 1) ? 0.f : 1.f;
+      float c[7];
+      load_w<DIM>(w1, w2, src, c0, c);
+      float su[DIM][6], sd[DIM][6];
+      float conv = 0.f, jump = 0.f;
+#pragma unroll
+      for (int a = 0; a < DIM; a++) {
+        float m[7], p[7];
+        int lm[3] = {c0[0], c0[1], c0[2]}, lp[3] = {c0[0], c0[1], c0[2]};
+        lm[a] -= 1;
+        lp[a] += 1;
+        load_w<DIM>(w1, w2, src, lm, m);
+        load_w<DIM>(w1, w2, src, lp, p);
+        axis_edges<R, ISEN>(m, m, c, p, p, P.inv_gamma, su[a], sd[a]);
+        conv += p[1 + a] - m[1 + a];
+        jump = fmaxf(jump, fabsf(p[4] - m[4]) / fminf(p[4], m[4]));
+      }
+      Pred pr;
+      hancock_masked<DIM>(c, conv, jump, su, sd, mask, h, P, pr);
+      if (at_source) {
+        pr.q[1] *= s.flip[0];
+        pr.q[2] *= s.flip[1];
+        pr.q[3] *= s.flip[2];
+      }
+      const size_t o = (size_t)slot * BG<DIM>::PN + t;
+      p1[o] = make_float4(pr.q[0], pr.q[1], pr.q[2], pr.q[3]);
+      p2[o] = make_float4(pr.q[4], pr.q[5], pr.flag, pr.fo ? 1.f : 0.f);
+    }
+  }
+}
+
+// The flux through the face between cells a and a + e_AXIS of block `slot`
+// (flux.wgsl flux_between): face states from the half steps and the edge increments the
+// primitives give along the axis.
+template <int DIM, int R, bool ISEN, int AXIS>
+__device__ __forceinline__ void face_flux(const KParams& P, const float4* __restrict__ w1, const float4* __restrict__ w2,
+                                          const float4* __restrict__ p1, const float4* __restrict__ p2, int slot,
+                                          const int* a, float* F) {
+  int am[3] = {a[0], a[1], a[2]}, b[3] = {a[0], a[1], a[2]}, bp[3] = {a[0], a[1], a[2]};
+  am[AXIS] -= 1;
+  b[AXIS] += 1;
+  bp[AXIS] += 2;
+  float wm[7], wa[7], wb[7], wbp[7];
+  load_w<DIM>(w1, w2, slot, am, wm);
+  load_w<DIM>(w1, w2, slot, a, wa);
+  load_w<DIM>(w1, w2, slot, b, wb);
+  load_w<DIM>(w1, w2, slot, bp, wbp);
+  float su[6], sd[6], tu[6], td[6];
+  axis_edges<R, ISEN>(wm, wm, wa, wb, wb, P.inv_gamma, su, sd);   // cell a: toward its upper face
+  axis_edges<R, ISEN>(wa, wa, wb, wbp, wbp, P.inv_gamma, tu, td);  // cell b: from its lower face
+  Pred pa, pb;
+  {
+    const size_t o = (size_t)slot * BG<DIM>::PN + ptex<DIM>(a);
+    const float4 x = __ldg(p1 + o), y = __ldg(p2 + o);
+    pa.q[0] = x.x; pa.q[1] = x.y; pa.q[2] = x.z; pa.q[3] = x.w; pa.q[4] = y.x; pa.q[5] = y.y;
+    pa.flag = y.z;
+    pa.fo = y.w != 0.f;
+  }
+  {
+    const size_t o = (size_t)slot * BG<DIM>::PN + ptex<DIM>(b);
+    const float4 x = __ldg(p1 + o), y = __ldg(p2 + o);
+    pb.q[0] = x.x; pb.q[1] = x.y; pb.q[2] = x.z; pb.q[3] = x.w; pb.q[4] = y.x; pb.q[5] = y.y;
+    pb.flag = y.z;
+    pb.fo = y.w != 0.f;
+  }
+  float L[7], Rr[7];
+  face_state(pa, su, 1.f, L);
+  face_state(pb, td, -1.f, Rr);
+  riemann<AXIS>(L, Rr, P, F);
+}
+
+// The fine-flux matching of a face at the edge of a block (amr/update.wgsl:207-295): where the
+// same-level neighbour beyond it is refined, the face's flux is the mean of the fluxes through
+// the 2^(ndim-1) fine faces it covers, computed as the fine leaf computes them.
+template <int DIM, int R, bool ISEN, int AXIS>
+__device__ __forceinline__ void match_face(const KParams& P, const int* __restrict__ bt, const float4* __restrict__ w1,
+                                           const float4* __restrict__ w2, const float4* __restrict__ p1,
+                                           const float4* __restrict__ p2, int slot, const int* l, bool hi, float* F) {
+  const int np = bt_at(bt, slot, 6 + 2 * AXIS + (hi ? 1 : 0));
+  if (np < 0 || leaf_of(bt, np)) return;
+  const bool upper = !hi;
+  int h[3] = {l[0] >= BS / 2, l[1] >= BS / 2, DIM == 3 ? (l[2] >= BS / 2) : 0};
+  int bits[3] = {h[0], h[1], h[2]};
+  bits[AXIS] = upper ? 1 : 0;
+  if (DIM == 2) bits[2] = 0;
+  const int ch = bt_at(bt, np, 12 + (bits[0] | (bits[1] << 1) | (bits[2] << 2)));
+  if (ch < 0) return;
+  int a0[3] = {2 * (l[0] - (BS / 2) * h[0]), 2 * (l[1] - (BS / 2) * h[1]), DIM == 3 ? 2 * (l[2] - (BS / 2) * h[2]) : 0};
+  a0[AXIS] = upper ? BS - 1 : -1;
+  constexpr int T1 = (AXIS + 1) % 3, T2 = (AXIS + 2) % 3;
+  const int n1 = (DIM == 2 && T1 == 2) ? 1 : 2;
+  const int n2 = (DIM == 2 && T2 == 2) ? 1 : 2;
+  float sum[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  for (int j = 0; j < n2; j++)
+    for (int i = 0; i < n1; i++) {
+      int a[3] = {a0[0], a0[1], a0[2]};
+      a[T1] += i;
+      a[T2] += j;
+      float f[8];
+      face_flux<DIM, R, ISEN, AXIS>(P, w1, w2, p1, p2, ch, a, f);
+#pragma unroll
+      for (int v = 0; v < 8; v++) sum[v] += f[v];
+    }
+  const float w = 1.f / (float)(n1 * n2);
+#pragma unroll
+  for (int v = 0; v < 8; v++) F[v] = sum[v] * w;
+}
+
+// 3. Fluxes and the update of every leaf (update.wgsl:327-560). A CTA takes a block plane by
+// plane along z; each thread owns a column and solves its lower x and y faces (the last row
+// also the block's upper face) into shared memory, and its z faces in registers, so every face
+// is solved once.
+template <int DIM, int R, bool ISEN>
+__global__ void __launch_bounds__(NT) amr_update(const KParams P, const int* __restrict__ bt, double dx0,
+                                                 const int* __restrict__ list, int n, const float4* __restrict__ u1,
+                                                 const float4* __restrict__ u2, const float4* __restrict__ w1,
+                                                 const float4* __restrict__ w2, const float4* __restrict__ p1,
+                                                 const float4* __restrict__ p2, float4* __restrict__ o1,
+                                                 float4* __restrict__ o2, const DevClock* __restrict__ clk) {
+  __shared__ float sFx[8][BS * (BS + 1)];
+  __shared__ float sFy[8][BS * (BS + 1)];
+  const double dt = clk->dt;
+  const bool held = clk->held != 0;
+  const int tx = threadIdx.x % BS, ty = threadIdx.x / BS;
+  for (int i = blockIdx.x; i < n; i += gridDim.x) {
+    const int slot = __ldg(list + i);
+    const float dtdx = (float)(dt * ldexp(1.0, bt_at(bt, slot, 0)) / dx0);
+    float Fzlo[8];
+    const int nk = DIM == 3 ? BS : 1;
+    for (int k = 0; k < nk; k++) {
+      int l[3] = {tx, ty, k};
+      float F[8];
+      // x faces
+      {
+        int a[3] = {tx - 1, ty, k};
+        face_flux<DIM, R, ISEN, 0>(P, w1, w2, p1, p2, slot, a, F);
+        if (tx == 0) match_face<DIM, R, ISEN, 0>(P, bt, w1, w2, p1, p2, slot, l, false, F);
+#pragma unroll
+        for (int v = 0; v < 8; v++) sFx[v][ty * (BS + 1) + tx] = F[v];
+        if (tx == BS - 1) {
+          face_flux<DIM, R, ISEN, 0>(P, w1, w2, p1, p2, slot, l, F);
+          match_face<DIM, R, ISEN, 0>(P, bt, w1, w2, p1, p2, slot, l, true, F);
+#pragma unroll
+          for (int v = 0; v < 8; v++) sFx[v][ty * (BS + 1) + BS] = F[v];
+        }
+      }
+      // y faces
+      {
+        int a[3] = {tx, ty - 1, k};
+        face_flux<DIM, R, ISEN, 1>(P, w1, w2, p1, p2, slot, a, F);
+        if (ty == 0) match_face<DIM, R, ISEN, 1>(P, bt, w1, w2, p1, p2, slot, l, false, F);
+#pragma unroll
+        for (int v = 0; v < 8; v++) sFy[v][ty * BS + tx] = F[v];
+        if (ty == BS - 1) {
+          face_flux<DIM, R, ISEN, 1>(P, w1, w2, p1, p2, slot, l, F);
+          match_face<DIM, R, ISEN, 1>(P, bt, w1, w2, p1, p2, slot, l, true, F);
+#pragma unroll
+          for (int v = 0; v < 8; v++) sFy[v][BS * BS + tx] = F[v];
+        }
+      }
+      float Fzhi[8];
+      if constexpr (DIM == 3) {
+        if (k == 0) {
+          int a[3] = {tx, ty, -1};
+          face_flux<DIM, R, ISEN, 2>(P, w1, w2, p1, p2, slot, a, Fzlo);
+          match_face<DIM, R, ISEN, 2>(P, bt, w1, w2, p1, p2, slot, l, false, Fzlo);
+        }
+        face_flux<DIM, R, ISEN, 2>(P, w1, w2, p1, p2, slot, l, Fzhi);
+        if (k == BS - 1) match_face<DIM, R, ISEN, 2>(P, bt, w1, w2, p1, p2, slot, l, true, Fzhi);
+      }
+      __syncthreads();
+      float acc[8];
+#pragma unroll
+      for (int v = 0; v < 8; v++) {
+        float x = sFx[v][ty * (BS + 1) + tx];
+        x -= sFx[v][ty * (BS + 1) + tx + 1];
+        x += sFy[v][ty * BS + tx];
+        x -= sFy[v][(ty + 1) * BS + tx];
+        if constexpr (DIM == 3) {
+          x += Fzlo[v];
+          x -= Fzhi[v];
+        }
+        acc[v] = x;
+      }
+      const size_t oc = (size_t)slot * BG<DIM>::CB + cell_ix<DIM>(l);
+      const size_t op = (size_t)slot * BG<DIM>::PN + ptex<DIM>(l);
+      const float4 a = __ldg(u1 + oc), b = __ldg(u2 + oc);
+      if (held) {
+        o1[oc] = a;
+        o2[oc] = b;
+      } else {
+        float4 na, nb;
+        update_cell(a, b, acc, __ldg(p2 + op).x, dtdx, P, na, nb);
+        o1[oc] = na;
+        o2[oc] = nb;
+      }
+      if constexpr (DIM == 3) {
+#pragma unroll
+        for (int v = 0; v < 8; v++) Fzlo[v] = Fzhi[v];
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// Löhner's refinement indicator per leaf (amr/flag.wgsl:66-155): the largest over the block's
+// cells of the normalised second differences of density and pressure (EPS = 0.01), at least
+// GAS_MIN.
+template <int DIM>
+__global__ void __launch_bounds__(NT) amr_flag(const int* __restrict__ list, int n, const float4* __restrict__ w1,
+                                               const float4* __restrict__ w2, float* __restrict__ flags) {
+  __shared__ float sRed[NT / 32];
+  const float EPS = 0.01f;
+  for (int i = blockIdx.x; i < n; i += gridDim.x) {
+    const int slot = __ldg(list + i);
+    float m = 0.f;
+    for (int t = threadIdx.x; t < BG<DIM>::CB; t += NT) {
+      int l[3] = {t % BS, (t / BS) % BS, DIM == 3 ? t / (BS * BS) : 0};
+      const size_t o = (size_t)slot * BG<DIM>::WN + wtex<DIM>(l);
+      const float r0 = __ldg(w1 + o).x, p0 = __ldg(w2 + o).x;
+      float nr = 0.f, dr = 0.f, np = 0.f, dp = 0.f;
+#pragma unroll
+      for (int a = 0; a < DIM; a++) {
+        int lp[3] = {l[0], l[1], l[2]}, lm[3] = {l[0], l[1], l[2]};
+        lp[a] += 1;
+        lm[a] -= 1;
+        const size_t op = (size_t)slot * BG<DIM>::WN + wtex<DIM>(lp), om = (size_t)slot * BG<DIM>::WN + wtex<DIM>(lm);
+        const float rp = __ldg(w1 + op).x, rm = __ldg(w1 + om).x, pp = __ldg(w2 + op).x, pm = __ldg(w2 + om).x;
+        const float sr = rp - 2.f * r0 + rm, sp = pp - 2.f * p0 + pm;
+        const float er = fabsf(rp - r0) + fabsf(r0 - rm) + EPS * (fabsf(rp) + 2.f * fabsf(r0) + fabsf(rm));
+        const float ep = fabsf(pp - p0) + fabsf(p0 - pm) + EPS * (fabsf(pp) + 2.f * fabsf(p0) + fabsf(pm));
+        nr += sr * sr;
+        dr += er * er;
+        np += sp * sp;
+        dp += ep * ep;
+      }
+      const float ind = fmaxf(sqrtf(nr / fmaxf(dr, 1e-30f)), sqrtf(np / fmaxf(dp, 1e-30f)));
+      m = fmaxf(m, ind);
+    }
+    m = block_max(m, sRed);
+    if (threadIdx.x == 0) flags[slot] = fmaxf(m, 1e-30f);
+  }
+}
+
+// Filling the leaves of a new tree from the old one (amr/regrid.wgsl:41-139): copy, restrict
+// the eight old children, or prolong from the old leaf with the kinetic energy kept
+// consistent (each child's own kinetic energy plus its interpolated internal energy, less one
+// shared offset that keeps the mean total energy the coarse cell's).
+template <int DIM, int R>
+__global__ void __launch_bounds__(NT) amr_regrid(const KParams P, const int* __restrict__ rg, const int* __restrict__ list,
+                                                 int n, const float4* __restrict__ u1, const float4* __restrict__ u2,
+                                                 const float4* __restrict__ w1, const float4* __restrict__ w2,
+                                                 float4* __restrict__ o1, float4* __restrict__ o2) {
+  for (int i = blockIdx.x; i < n; i += gridDim.x) {
+    const int slot = __ldg(list + i);
+    const int kind = __ldg(rg + slot * RGS), src = __ldg(rg + slot * RGS + 1), oct = __ldg(rg + slot * RGS + 2);
+    for (int t = threadIdx.x; t < BG<DIM>::CB; t += NT) {
+      int l[3] = {t % BS, (t / BS) % BS, DIM == 3 ? t / (BS * BS) : 0};
+      Cons u;
+      if (kind == 2) {
+        int lc[3] = {(l[0] >> 1) + (BS / 2) * (oct & 1), (l[1] >> 1) + (BS / 2) * ((oct >> 1) & 1),
+                     DIM == 3 ? (l[2] >> 1) + (BS / 2) * ((oct >> 2) & 1) : 0};
+        const size_t oc = (size_t)src * BG<DIM>::CB + cell_ix<DIM>(lc);
+        const Cons uc{__ldg(u1 + oc), __ldg(u2 + oc)};
+        Cons m[3], p[3];
+        bool ok[3] = {true, true, true};
+#pragma unroll
+        for (int a = 0; a < DIM; a++) {
+          for (int sgn = -1; sgn <= 1; sgn += 2) {
+            int at[3] = {lc[0], lc[1], lc[2]};
+            at[a] += sgn;
+            const size_t ow = (size_t)src * BG<DIM>::WN + wtex<DIM>(at);
+            const float4 x = __ldg(w1 + ow), y = __ldg(w2 + ow);
+            const float eint = y.x * P.inv_gm1;
+            Cons c;
+            c.a = make_float4(x.x, x.x * x.y, x.x * x.z, x.x * x.w);
+            c.b = make_float4(eint + 0.5f * x.x * (x.y * x.y + x.z * x.z + x.w * x.w), eint, x.x * y.y, 0.f);
+            (sgn < 0 ? m[a] : p[a]) = c;
+          }
+        }
+        const Slopes sl = prolong_slopes<DIM, R>(uc, m, ok, p, ok, P.rho_floor);
+        int par[3] = {l[0] & 1, l[1] & 1, DIM == 3 ? (l[2] & 1) : 0};
+        u = prolong_child(uc, sl, par);
+        float ke = 0.f;
+        for (int kz = 0; kz < (DIM == 3 ? 2 : 1); kz++)
+          for (int jy = 0; jy < 2; jy++)
+            for (int ix = 0; ix < 2; ix++) {
+              int pc[3] = {ix, jy, kz};
+              const Cons c = prolong_child(uc, sl, pc);
+              ke += 0.5f * (c.a.y * c.a.y + c.a.z * c.a.z + c.a.w * c.a.w) / fmaxf(c.a.x, P.rho_floor);
+            }
+        ke *= DIM == 3 ? 0.125f : 0.25f;
+        u.b.x = 0.5f * (u.a.y * u.a.y + u.a.z * u.a.z + u.a.w * u.a.w) / fmaxf(u.a.x, P.rho_floor) + u.b.y +
+                (uc.b.x - uc.b.y - ke);
+      } else if (kind == 3) {
+        int h[3] = {l[0] >= BS / 2, l[1] >= BS / 2, DIM == 3 ? (l[2] >= BS / 2) : 0};
+        const int ch = __ldg(rg + slot * RGS + 4 + (h[0] | (h[1] << 1) | (h[2] << 2)));
+        float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a;
+        for (int kz = 0; kz < (DIM == 3 ? 2 : 1); kz++)
+          for (int jy = 0; jy < 2; jy++)
+            for (int ix = 0; ix < 2; ix++) {
+              int f[3] = {2 * (l[0] - (BS / 2) * h[0]) + ix, 2 * (l[1] - (BS / 2) * h[1]) + jy,
+                          DIM == 3 ? 2 * (l[2] - (BS / 2) * h[2]) + kz : 0};
+              const size_t o = (size_t)ch * BG<DIM>::CB + cell_ix<DIM>(f);
+              const float4 x = __ldg(u1 + o), y = __ldg(u2 + o);
+              a.x += x.x; a.y += x.y; a.z += x.z; a.w += x.w;
+              b.x += y.x; b.y += y.y; b.z += y.z; b.w += y.w;
+            }
+        const float w = DIM == 3 ? 0.125f : 0.25f;
+        u.a = make_float4(a.x * w, a.y * w, a.z * w, a.w * w);
+        u.b = make_float4(b.x * w, b.y * w, b.z * w, b.w * w);
+      } else {
+        const size_t o = (size_t)src * BG<DIM>::CB + t;
+        u = Cons{__ldg(u1 + o), __ldg(u2 + o)};
+      }
+      const size_t o = (size_t)slot * BG<DIM>::CB + t;
+      o1[o] = u.a;
+      o2[o] = u.b;
+    }
+  }
+}
+
+// Conservation totals over the leaves in compensated float64, one partial row per CTA.
+struct AccD {
+  double s, c;
+  __device__ void add(double x) {
+    const double t = s + x;
+    c += fabs(s) >= fabs(x) ? (s - t) + x : (x - t) + s;
+    s = t;
+  }
+};
+template <int DIM>
+__global__ void __launch_bounds__(NT) amr_diag(const KParams P, const int* __restrict__ bt, double dx0,
+                                               const int* __restrict__ list, int n, const float4* __restrict__ u1,
+                                               const float4* __restrict__ u2, double* __restrict__ part) {
+  AccD acc[8];
+  for (int i = 0; i < 8; i++) acc[i] = AccD{0.0, 0.0};
+  double mach = 0.0;
+  for (int i = blockIdx.x; i < n; i += gridDim.x) {
+    const int slot = __ldg(list + i);
+    const double dx = dx0 / ldexp(1.0, bt_at(bt, slot, 0));
+    const double dv = DIM == 3 ? dx * dx * dx : dx * dx;
+    for (int t = threadIdx.x; t < BG<DIM>::CB; t += NT) {
+      const size_t o = (size_t)slot * BG<DIM>::CB + t;
+      const float4 a = __ldg(u1 + o), b = __ldg(u2 + o);
+      const double rho = fmax((double)a.x, (double)P.rho_floor);
+      const double vx = a.y / rho, vy = a.z / rho, vz = a.w / rho, v2 = vx * vx + vy * vy + vz * vz;
+      const double p = fmax((double)P.gm1 * b.y, (double)P.p_floor);
+      acc[0].add(rho * dv);
+      acc[1].add((double)a.y * dv);
+      acc[2].add((double)a.z * dv);
+      acc[3].add((double)a.w * dv);
+      acc[4].add(0.5 * rho * v2 * dv);
+      acc[5].add(((double)b.x - 0.5 * rho * v2) * dv);
+      acc[6].add((double)b.x * dv);
+      acc[7].add((a.x <= P.rho_floor * 1.0001f || p <= P.p_floor * 1.0001) ? 1.0 : 0.0);
+      mach = fmax(mach, sqrt(v2) / sqrt((double)P.gamma * p / rho));
+    }
+  }
+  __shared__ double sh[NT][9];
+  for (int v = 0; v < 8; v++) sh[threadIdx.x][v] = acc[v].s + acc[v].c;
+  sh[threadIdx.x][8] = mach;
+  __syncthreads();
+  if (threadIdx.x < 9) {
+    const int v = threadIdx.x;
+    AccD s{0.0, 0.0};
+    double mx = 0.0;
+    for (int t = 0; t < NT; t++) {
+      if (v == 8) mx = fmax(mx, sh[t][8]);
+      else s.add(sh[t][v]);
+    }
+    part[(size_t)blockIdx.x * 9 + v] = v == 8 ? mx : s.s + s.c;
+  }
+}
+
+__global__ void amr_diag_final(const double* __restrict__ part, int nblocks, double* __restrict__ out) {
+  const int v = threadIdx.x;
+  if (v >= 9) return;
+  AccD s{0.0, 0.0};
+  double mx = 0.0;
+  for (int b = 0; b < nblocks; b++) {
+    if (v == 8) mx = fmax(mx, part[(size_t)b * 9 + 8]);
+    else s.add(part[(size_t)b * 9 + v]);
+  }
+  out[v] = v == 8 ? mx : s.s + s.c;
+}
+
+// The ghost classification of every texel of a block's primitive region, for checking the
+// device's ghost indexing against the tables: (kind, slot, l0, l1, l2) per texel.
+template <int DIM>
+__global__ void amr_ghost_map(const int* __restrict__ bt, int slot, int* __restrict__ out) {
+  for (int t = threadIdx.x + blockIdx.x * blockDim.x; t < BG<DIM>::WN; t += blockDim.x * gridDim.x) {
+    int l[3] = {t % PAD - NG, (t / PAD) % PAD - NG, DIM == 3 ? t / (PAD * PAD) - NG : 0};
+    const Src s = ghost_src<DIM>(bt, slot, l);
+    out[t * 5 + 0] = s.kind;
+    out[t * 5 + 1] = s.slot;
+    out[t * 5 + 2] = s.l[0];
+    out[t * 5 + 3] = s.l[1];
+    out[t * 5 + 4] = s.l[2];
+  }
+}
+
+}  // namespace amrk
+
+// ---------------------------------------------------------------------------------------------
+// Host launchers.
+
+namespace {
+int grid_for(int n, int per_sm) {
+  int g = 148 * per_sm;
+  if (n < g) g = n;
+  return g < 1 ? 1 : g;
+}
+}  // namespace
+
+#define SHZ_RECON_SWITCH(recon, ISEN, CALL)                                  \
+  switch (recon) {                                                           \
+    case R_MINMOD: { constexpr int R = R_MINMOD; CALL; break; }             \
+    case R_MC: { constexpr int R = R_MC; CALL; break; }                     \
+    case R_VANLEER: { constexpr int R = R_VANLEER; CALL; break; }           \
+    default: { constexpr int R = R_KOREN; CALL; break; }                    \
+  }
+
+cudaError_t amr_launch_assemble(const AmrLaunch& L, const int* list, int n, const float4* u1, const float4* u2,
+                                unsigned* rate_out, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  const int g = grid_for(n, 4);
+  if (L.ndim == 3) {
+    SHZ_RECON_SWITCH(L.recon, false, (amrk::amr_assemble<3, R><<<g, amrk::NT, 0, s>>>(L.P, L.bt, L.nr, L.dx0, list, n, u1, u2, L.w1, L.w2, rate_out)))
+  } else {
+    SHZ_RECON_SWITCH(L.recon, false, (amrk::amr_assemble<2, R><<<g, amrk::NT, 0, s>>>(L.P, L.bt, L.nr, L.dx0, list, n, u1, u2, L.w1, L.w2, rate_out)))
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t amr_launch_predict(const AmrLaunch& L, const int* list, int n, const DevClock* clk, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  const int g = grid_for(n, 4);
+  if (L.ndim == 3) {
+    if (L.isen) { SHZ_RECON_SWITCH(L.recon, true, (amrk::amr_predict<3, R, true><<<g, amrk::NT, 0, s>>>(L.P, L.bt, L.dx0, list, n, L.w1, L.w2, L.p1, L.p2, clk))) }
+    else { SHZ_RECON_SWITCH(L.recon, false, (amrk::amr_predict<3, R, false><<<g, amrk::NT, 0, s>>>(L.P, L.bt, L.dx0, list, n, L.w1, L.w2, L.p1, L.p2, clk))) }
+  } else {
+    if (L.isen) { SHZ_RECON_SWITCH(L.recon, true, (amrk::amr_predict<2, R, true><<<g, amrk::NT, 0, s>>>(L.P, L.bt, L.dx0, list, n, L.w1, L.w2, L.p1, L.p2, clk))) }
+    else { SHZ_RECON_SWITCH(L.recon, false, (amrk::amr_predict<2, R, false><<<g, amrk::NT, 0, s>>>(L.P, L.bt, L.dx0, list, n, L.w1, L.w2, L.p1, L.p2, clk))) }
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t amr_launch_update(const AmrLaunch& L, const int* list, int n, const float4* u1, const float4* u2, float4* o1,
+                              float4* o2, const DevClock* clk, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  const int g = grid_for(n, 4);
+  if (L.ndim == 3) {
+    if (L.isen) { SHZ_RECON_SWITCH(L.recon, true, (amrk::amr_update<3, R, true><<<g, amrk::NT, 0, s>>>(L.P, L.bt, L.dx0, list, n, u1, u2, L.w1, L.w2, L.p1, L.p2, o1, o2, clk))) }
+    else { SHZ_RECON_SWITCH(L.recon, false, (amrk::amr_update<3, R, false><<<g, amrk::NT, 0, s>>>(L.P, L.bt, L.dx0, list, n, u1, u2, L.w1, L.w2, L.p1, L.p2, o1, o2, clk))) }
+  } else {
+    if (L.isen) { SHZ_RECON_SWITCH(L.recon, true, (amrk::amr_update<2, R, true><<<g, amrk::NT, 0, s>>>(L.P, L.bt, L.dx0, list, n, u1, u2, L.w1, L.w2, L.p1, L.p2, o1, o2, clk))) }
+    else { SHZ_RECON_SWITCH(L.recon, false, (amrk::amr_update<2, R, false><<<g, amrk::NT, 0, s>>>(L.P, L.bt, L.dx0, list, n, u1, u2, L.w1, L.w2, L.p1, L.p2, o1, o2, clk))) }
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t amr_launch_flag(const AmrLaunch& L, const int* list, int n, float* flags, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  const int g = grid_for(n, 4);
+  if (L.ndim == 3) amrk::amr_flag<3><<<g, amrk::NT, 0, s>>>(list, n, L.w1, L.w2, flags);
+  else amrk::amr_flag<2><<<g, amrk::NT, 0, s>>>(list, n, L.w1, L.w2, flags);
+  return cudaGetLastError();
+}
+
+cudaError_t amr_launch_regrid(const AmrLaunch& L, const int* rg, const int* list, int n, const float4* u1, const float4* u2,
+                              float4* o1, float4* o2, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  const int g = grid_for(n, 4);
+  if (L.ndim == 3) {
+    SHZ_RECON_SWITCH(L.recon, false, (amrk::amr_regrid<3, R><<<g, amrk::NT, 0, s>>>(L.P, rg, list, n, u1, u2, L.w1, L.w2, o1, o2)))
+  } else {
+    SHZ_RECON_SWITCH(L.recon, false, (amrk::amr_regrid<2, R><<<g, amrk::NT, 0, s>>>(L.P, rg, list, n, u1, u2, L.w1, L.w2, o1, o2)))
+  }
+  return cudaGetLastError();
+}
+
+int amr_diag_blocks(int n) { return grid_for(n, 2); }
+
+cudaError_t amr_launch_diag(const AmrLaunch& L, const int* list, int n, const float4* u1, const float4* u2, double* part,
+                            double* out, cudaStream_t s) {
+  const int g = amr_diag_blocks(n);
+  if (L.ndim == 3) amrk::amr_diag<3><<<g, amrk::NT, 0, s>>>(L.P, L.bt, L.dx0, list, n, u1, u2, part);
+  else amrk::amr_diag<2><<<g, amrk::NT, 0, s>>>(L.P, L.bt, L.dx0, list, n, u1, u2, part);
+  amrk::amr_diag_final<<<1, 32, 0, s>>>(part, g, out);
+  return cudaGetLastError();
+}
+
+cudaError_t amr_launch_ghost_map(const AmrLaunch& L, int slot, int* out, cudaStream_t s) {
+  if (L.ndim == 3) amrk::amr_ghost_map<3><<<32, 256, 0, s>>>(L.bt, slot, out);
+  else amrk::amr_ghost_map<2><<<2, 256, 0, s>>>(L.bt, slot, out);
+  return cudaGetLastError();
+}
+
+}  // namespace shz

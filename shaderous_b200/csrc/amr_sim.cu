@@ -1,0 +1,653 @@
+// The adaptive-grid run (shz_amr_*): the host side of the reference's AmrSim
+// (src/amr/amr_sim.ts). It owns the block tree (amr_tree.cpp), the atlases in HBM, the block
+// table and slot lists on the device, and one stream. A step is one CUDA graph of four kernels
+// (assemble, clock, predict, update: amr_kernels.cu); every regrid_every steps the Löhner flags
+// are read back, BlockTree.adapt decides the new mesh on the host, the new tables go up and the
+// regrid kernel fills the new leaves (amr_sim.ts:2648 applyRegrid, :3033 encodeFlags, :3525 readFlags).
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/shaderous_b200.h"
+#include "amr_kernels.h"
+#include "amr_tree.h"
+#include "problems.h"
+#include "sweep.h"
+
+using shz::amr::BlockTree;
+using shz::amr::RegridOp;
+
+struct shz_amr {
+  shz_amr_config cfg;
+  shz::AmrLaunch L;
+  std::unique_ptr<BlockTree> tree;
+  int CB = 0, WN = 0, PN = 0;
+  float4* u1[2] = {nullptr, nullptr};
+  float4* u2[2] = {nullptr, nullptr};
+  float4 *w1 = nullptr, *w2 = nullptr, *p1 = nullptr, *p2 = nullptr;
+  int *d_bt = nullptr, *d_all = nullptr, *d_leaves = nullptr, *d_rg = nullptr;
+  float* d_flags = nullptr;
+  shz::DevClock* clk = nullptr;
+  unsigned* rates = nullptr;  // slots 0, 1: the steps'; 2: the refinement check's
+  double *diag_part = nullptr, *diag_out = nullptr;
+  int* d_ghost = nullptr;
+  std::vector<int32_t> h_bt, h_all, h_leaves, h_rg;
+  std::vector<float> h_flags;
+  int cur = 0, slot = 0;
+  long long since_check = 0;
+  cudaStream_t stream = nullptr;
+  cudaGraphExec_t graphs[4] = {nullptr, nullptr, nullptr, nullptr};
+  long long launches = 0;
+  std::string err;
+  int device = 0;
+};
+
+namespace {
+
+int fail(shz_amr* a, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (a) a->err = buf;
+  return code;
+}
+
+std::string g_create_err;
+
+#define AMR_CUDA(a, call)                                                                                 \
+  do {                                                                                                    \
+    cudaError_t e_ = (call);                                                                              \
+    if (e_ != cudaSuccess)                                                                                \
+      return fail(a, e_ == cudaErrorMemoryAllocation ? SHZ_E_OOM : SHZ_E_CUDA, "%s: %s", #call,          \
+                  cudaGetErrorString(e_));                                                                \
+  } while (0)
+
+struct Dev {
+  int prev = -1;
+  explicit Dev(int d) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != d) cudaSetDevice(d);
+  }
+  ~Dev() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+void drop_graphs(shz_amr* a) {
+  for (auto& g : a->graphs)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+}
+
+// The block table and the slot lists of the current tree, to the device.
+int upload_tables(shz_amr* a) {
+  const int cap = a->cfg.cap;
+  a->h_bt.resize((size_t)cap * shz::amr::BT_STRIDE);
+  a->tree->table(a->h_bt.data());
+  std::vector<int32_t> per;
+  a->tree->lists(a->h_all, a->h_leaves, per);
+  AMR_CUDA(a, cudaMemcpyAsync(a->d_bt, a->h_bt.data(), a->h_bt.size() * sizeof(int32_t), cudaMemcpyHostToDevice, a->stream));
+  AMR_CUDA(a, cudaMemcpyAsync(a->d_all, a->h_all.data(), a->h_all.size() * sizeof(int32_t), cudaMemcpyHostToDevice, a->stream));
+  AMR_CUDA(a, cudaMemcpyAsync(a->d_leaves, a->h_leaves.data(), a->h_leaves.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                              a->stream));
+  AMR_CUDA(a, cudaStreamSynchronize(a->stream));
+  drop_graphs(a);
+  return 0;
+}
+
+int write_clock(shz_amr* a, double t, long long steps) {
+  shz::DevClock h;
+  std::memset(&h, 0, sizeof h);
+  h.t = t;
+  h.t_end = a->cfg.hydro.t_end;
+  h.dt_max = a->cfg.hydro.dt_max;
+  h.cfl_dx = a->cfg.hydro.cfl;  // the rates are per unit of each block's own cell size
+  h.steps = steps;
+  AMR_CUDA(a, cudaMemcpyAsync(a->clk, &h, sizeof h, cudaMemcpyHostToDevice, a->stream));
+  AMR_CUDA(a, cudaMemsetAsync(a->rates, 0, 3 * sizeof(unsigned), a->stream));
+  AMR_CUDA(a, cudaStreamSynchronize(a->stream));
+  return 0;
+}
+
+int read_clock(shz_amr* a, shz::DevClock* h) {
+  AMR_CUDA(a, cudaMemcpyAsync(h, a->clk, sizeof *h, cudaMemcpyDeviceToHost, a->stream));
+  AMR_CUDA(a, cudaStreamSynchronize(a->stream));
+  return 0;
+}
+
+int n_all(const shz_amr* a) { return (int)a->h_all.size(); }
+int n_leaves(const shz_amr* a) { return (int)a->h_leaves.size(); }
+
+// One step's four kernels, enqueued.
+int enqueue_step(shz_amr* a) {
+  AMR_CUDA(a, shz::amr_launch_assemble(a->L, a->d_all, n_all(a), a->u1[a->cur], a->u2[a->cur], a->rates + a->slot, a->stream));
+  AMR_CUDA(a, shz::launch_clock(a->clk, a->rates, a->slot, a->stream));
+  AMR_CUDA(a, shz::amr_launch_predict(a->L, a->d_leaves, n_leaves(a), a->clk, a->stream));
+  AMR_CUDA(a, shz::amr_launch_update(a->L, a->d_leaves, n_leaves(a), a->u1[a->cur], a->u2[a->cur], a->u1[1 - a->cur],
+                                     a->u2[1 - a->cur], a->clk, a->stream));
+  return 0;
+}
+
+// One step, as the CUDA graph of its four kernels for this (state parity, rate slot); the graphs
+// are captured once per mesh and replayed.
+int step_once(shz_amr* a) {
+  cudaGraphExec_t& g = a->graphs[a->cur * 2 + a->slot];
+  if (!g) {
+    cudaGraph_t graph;
+    AMR_CUDA(a, cudaStreamBeginCapture(a->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = enqueue_step(a);
+    cudaError_t e = cudaStreamEndCapture(a->stream, &graph);
+    if (rc) return rc;
+    if (e != cudaSuccess) return fail(a, SHZ_E_CUDA, "capture of a step: %s", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&g, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return fail(a, SHZ_E_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
+  }
+  AMR_CUDA(a, cudaGraphLaunch(g, a->stream));
+  a->launches += 4;
+  a->cur ^= 1;
+  a->slot ^= 1;
+  return 0;
+}
+
+// The refinement indicators of the current state: a fresh assemble, then the Löhner pass.
+int compute_flags(shz_amr* a) {
+  AMR_CUDA(a, cudaMemsetAsync(a->rates + 2, 0, sizeof(unsigned), a->stream));
+  AMR_CUDA(a, shz::amr_launch_assemble(a->L, a->d_all, n_all(a), a->u1[a->cur], a->u2[a->cur], a->rates + 2, a->stream));
+  AMR_CUDA(a, cudaMemsetAsync(a->d_flags, 0, sizeof(float) * a->cfg.cap, a->stream));
+  AMR_CUDA(a, shz::amr_launch_flag(a->L, a->d_leaves, n_leaves(a), a->d_flags, a->stream));
+  a->launches += 2;
+  a->h_flags.resize(a->cfg.cap);
+  AMR_CUDA(a, cudaMemcpyAsync(a->h_flags.data(), a->d_flags, sizeof(float) * a->cfg.cap, cudaMemcpyDeviceToHost, a->stream));
+  AMR_CUDA(a, cudaStreamSynchronize(a->stream));
+  return 0;
+}
+
+// tree.adapt over the indicators; if the mesh changed, the new tables and the regrid pass.
+int check_and_regrid(shz_amr* a, const std::vector<double>* extra, int* changed) {
+  int rc = compute_flags(a);
+  if (rc) return rc;
+  std::vector<RegridOp> ops;
+  try {
+    ops = a->tree->adapt(
+        [&](const shz::amr::Block* b) {
+          double v = a->h_flags[b->slot];
+          if (extra) v = std::max(v, (*extra)[b->slot]);
+          return v;
+        },
+        a->cfg.refine_hi, a->cfg.refine_lo);
+  } catch (const std::exception& e) {
+    return fail(a, SHZ_E_CONFIG, "adapt: %s", e.what());
+  }
+  *changed = ops.empty() ? 0 : 1;
+  if (ops.empty()) return 0;
+  a->h_rg.resize((size_t)a->cfg.cap * shz::amr::RG_STRIDE);
+  BlockTree::regrid_table(ops, a->cfg.cap, a->h_rg.data());
+  AMR_CUDA(a, cudaMemcpyAsync(a->d_rg, a->h_rg.data(), a->h_rg.size() * sizeof(int32_t), cudaMemcpyHostToDevice, a->stream));
+  if ((rc = upload_tables(a))) return rc;
+  if (!extra) {
+    AMR_CUDA(a, shz::amr_launch_regrid(a->L, a->d_rg, a->d_leaves, n_leaves(a), a->u1[a->cur], a->u2[a->cur],
+                                       a->u1[1 - a->cur], a->u2[1 - a->cur], a->stream));
+    a->launches += 1;
+    a->cur ^= 1;
+  }
+  return 0;
+}
+
+// Level-0 cell size and the finest grid, for sampling problems.
+double dx0_of(const shz_amr_config& c) { return c.box / (c.nr * shz::amr::BS); }
+
+shz_config fine_config(const shz_amr_config& c) {
+  shz_config f = c.hydro;
+  const int nf = (c.nr * shz::amr::BS) << c.max_level;
+  f.n[0] = nf;
+  f.n[1] = c.ndim >= 2 ? nf : 1;
+  f.n[2] = c.ndim == 3 ? nf : 1;
+  f.dx = c.box / nf;
+  return f;
+}
+
+// Whether a problem's discontinuity crosses a block's box (the initial mesh refines there even
+// where no cell centre of a coarse block sees it).
+bool crosses(const shz::ProblemCtx& q, const double lo[3], const double hi[3], int nd) {
+  const shz_problem& p = q.p;
+  auto sphere = [&](double r) {
+    double d2 = 0, far2 = 0;
+    for (int a = 0; a < nd; a++) {
+      const double c = std::min(std::max(0.0, lo[a]), hi[a]);
+      d2 += c * c;
+      const double f = std::max(std::fabs(lo[a]), std::fabs(hi[a]));
+      far2 += f * f;
+    }
+    return d2 <= r * r && far2 >= r * r;
+  };
+  switch (p.kind) {
+    case SHZ_PROB_SOD: return lo[p.axis] <= 0 && hi[p.axis] >= 0;
+    case SHZ_PROB_SEDOV: return sphere(q.sedov_r);
+    case SHZ_PROB_BLAST: return sphere(p.a[4]);
+    case SHZ_PROB_KH: {
+      const double e = 0.25 * q.L[1];
+      return (lo[1] <= e && hi[1] >= e) || (lo[1] <= -e && hi[1] >= -e);
+    }
+    default: return false;
+  }
+}
+
+// Sample the problem into every leaf, and upload (u[cur]).
+int sample_leaves(shz_amr* a, const shz::ProblemCtx& q) {
+  const int BS = shz::amr::BS, nd = a->cfg.ndim, CB = a->CB;
+  const double dx0 = dx0_of(a->cfg), half = a->cfg.box / 2;
+  const int batch = 256;
+  float4 *h1 = nullptr, *h2 = nullptr;
+  AMR_CUDA(a, cudaMallocHost(&h1, (size_t)batch * CB * sizeof(float4)));
+  if (cudaMallocHost(&h2, (size_t)batch * CB * sizeof(float4)) != cudaSuccess) {
+    cudaFreeHost(h1);
+    return fail(a, SHZ_E_OOM, "pinned staging");
+  }
+  int rc = 0;
+  const int nl = n_leaves(a);
+  for (int b0 = 0; b0 < nl && rc == 0; b0 += batch) {
+    const int b1 = std::min(nl, b0 + batch);
+#pragma omp parallel for schedule(dynamic)
+    for (int bi = b0; bi < b1; bi++) {
+      const int slot = a->h_leaves[bi];
+      const int32_t* row = a->h_bt.data() + (size_t)slot * shz::amr::BT_STRIDE;
+      const int lev = row[0];
+      const double dx = dx0 / (double)(1 << lev);
+      const uint64_t span = (uint64_t)(a->cfg.nr * BS) << lev;
+      for (int t = 0; t < CB; t++) {
+        const int i = t % BS, j = (t / BS) % BS, k = nd == 3 ? t / (BS * BS) : 0;
+        const int gi = row[1] * BS + i, gj = row[2] * BS + j, gk = nd == 3 ? row[3] * BS + k : 0;
+        const double x = (gi + 0.5) * dx - half, y = (gj + 0.5) * dx - half, z = nd == 3 ? (gk + 0.5) * dx - half : 0.0;
+        const uint64_t cell = ((((uint64_t)lev << 56) ^ ((uint64_t)gk * span + gj)) * span) + gi;
+        double w[6];
+        shz::sample_problem(q, x, y, z, cell, w);
+        const double rho = w[0], eint = w[4] / (a->cfg.hydro.gamma - 1);
+        const double ke = 0.5 * rho * (w[1] * w[1] + w[2] * w[2] + w[3] * w[3]);
+        const size_t o = (size_t)(bi - b0) * CB + t;
+        h1[o] = make_float4((float)rho, (float)(rho * w[1]), (float)(rho * w[2]), (float)(rho * w[3]));
+        h2[o] = make_float4((float)(eint + ke), (float)eint, (float)(rho * w[5]), 0.f);
+      }
+    }
+    for (int bi = b0; bi < b1 && rc == 0; bi++) {
+      const size_t dst = (size_t)a->h_leaves[bi] * CB, src = (size_t)(bi - b0) * CB;
+      if (cudaMemcpyAsync(a->u1[a->cur] + dst, h1 + src, CB * sizeof(float4), cudaMemcpyHostToDevice, a->stream) != cudaSuccess ||
+          cudaMemcpyAsync(a->u2[a->cur] + dst, h2 + src, CB * sizeof(float4), cudaMemcpyHostToDevice, a->stream) != cudaSuccess)
+        rc = fail(a, SHZ_E_CUDA, "leaf upload");
+    }
+    if (cudaStreamSynchronize(a->stream) != cudaSuccess) rc = fail(a, SHZ_E_CUDA, "leaf upload sync");
+  }
+  cudaFreeHost(h1);
+  cudaFreeHost(h2);
+  return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* shz_amr_error(const shz_amr* a) { return a ? a->err.c_str() : g_create_err.c_str(); }
+
+int shz_amr_create(const shz_amr_config* cfg, shz_amr** out) {
+  if (!cfg || !out) return SHZ_E_CONFIG;
+  *out = nullptr;
+  const shz_amr_config& c = *cfg;
+  auto refuse = [&](const char* why) {
+    g_create_err = std::string("refused AMR configuration: ") + why;
+    return SHZ_E_CONFIG;
+  };
+  if (c.ndim != 2 && c.ndim != 3) return refuse("ndim must be 2 or 3");
+  if (c.nr < 1 || c.max_level < 0 || c.max_level > shz::amr::MAX_LEVELS) return refuse("nr >= 1 and max_level 0..7");
+  if (c.hydro.recon == SHZ_RECON_PPM) return refuse("PPM reaches three cells; the blocks keep two ghost layers");
+  if (c.hydro.recon < 0 || c.hydro.recon > SHZ_RECON_KOREN) return refuse("recon must be minmod, mc, vanleer or koren");
+  if (!(c.box > 0) || !(c.hydro.gamma > 1) || !(c.hydro.cfl > 0)) return refuse("box > 0, gamma > 1, cfl > 0");
+  for (int ax = 0; ax < 3; ax++)
+    if (c.hydro.bc_lo[ax] < 0 || c.hydro.bc_lo[ax] > 2 || c.hydro.bc_hi[ax] < 0 || c.hydro.bc_hi[ax] > 2)
+      return refuse("boundary codes are 0, 1, 2");
+  const int nroot = c.nr * c.nr * (c.ndim == 3 ? c.nr : 1);
+  if (c.cap < nroot) return refuse("cap is smaller than the root blocks");
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+    g_create_err = "no CUDA device";
+    return SHZ_E_NODEV;
+  }
+  if (c.hydro.device < 0 || c.hydro.device >= count) return refuse("no such device");
+  Dev dv(c.hydro.device);
+  shz_amr* a = new shz_amr();
+  a->cfg = c;
+  a->device = c.hydro.device;
+  a->CB = c.ndim == 3 ? 4096 : 256;
+  a->WN = c.ndim == 3 ? 8000 : 400;
+  a->PN = c.ndim == 3 ? 5832 : 324;
+  shz::KParams& P = a->L.P;
+  std::memset(&P, 0, sizeof P);
+  P.dx = dx0_of(c);
+  P.gamma = (float)c.hydro.gamma;
+  P.gm1 = (float)(c.hydro.gamma - 1);
+  P.inv_gm1 = (float)(1.0 / (c.hydro.gamma - 1));
+  P.inv_gamma = (float)(1.0 / c.hydro.gamma);
+  P.rho_floor = (float)c.hydro.rho_floor;
+  P.p_floor = (float)c.hydro.p_floor;
+  P.e_floor = (float)(c.hydro.p_floor / (c.hydro.gamma - 1));
+  P.eta_dual = (float)c.hydro.eta_dual;
+  P.shock_thresh = (float)c.hydro.shock_thresh;
+  P.signal = (float)c.hydro.signal_dims;
+  P.hll = c.hydro.riemann == SHZ_RIEMANN_HLL ? 1 : 0;
+  a->L.ndim = c.ndim;
+  a->L.recon = c.hydro.recon;
+  a->L.isen = c.hydro.isentropic != 0;
+  a->L.nr = c.nr;
+  a->L.dx0 = dx0_of(c);
+  auto bail = [&](int code, const char* what) {
+    g_create_err = what;
+    shz_amr_destroy(a);
+    return code;
+  };
+  const size_t cap = c.cap;
+  if (cudaStreamCreateWithFlags(&a->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(SHZ_E_CUDA, "stream");
+  bool ok = true;
+  for (int p = 0; p < 2; p++) {
+    ok = ok && cudaMalloc(&a->u1[p], cap * a->CB * sizeof(float4)) == cudaSuccess;
+    ok = ok && cudaMalloc(&a->u2[p], cap * a->CB * sizeof(float4)) == cudaSuccess;
+  }
+  ok = ok && cudaMalloc(&a->w1, cap * a->WN * sizeof(float4)) == cudaSuccess;
+  ok = ok && cudaMalloc(&a->w2, cap * a->WN * sizeof(float4)) == cudaSuccess;
+  ok = ok && cudaMalloc(&a->p1, cap * a->PN * sizeof(float4)) == cudaSuccess;
+  ok = ok && cudaMalloc(&a->p2, cap * a->PN * sizeof(float4)) == cudaSuccess;
+  ok = ok && cudaMalloc(&a->d_bt, cap * shz::amr::BT_STRIDE * sizeof(int)) == cudaSuccess;
+  ok = ok && cudaMalloc(&a->d_all, cap * sizeof(int)) == cudaSuccess;
+  ok = ok && cudaMalloc(&a->d_leaves, cap * sizeof(int)) == cudaSuccess;
+  ok = ok && cudaMalloc(&a->d_rg, cap * shz::amr::RG_STRIDE * sizeof(int)) == cudaSuccess;
+  ok = ok && cudaMalloc(&a->d_flags, cap * sizeof(float)) == cudaSuccess;
+  ok = ok && cudaMalloc(&a->clk, sizeof(shz::DevClock)) == cudaSuccess;
+  ok = ok && cudaMalloc(&a->rates, 3 * sizeof(unsigned)) == cudaSuccess;
+  ok = ok && cudaMalloc(&a->diag_part, (size_t)shz::amr_diag_blocks(c.cap) * 9 * sizeof(double)) == cudaSuccess;
+  ok = ok && cudaMalloc(&a->diag_out, 9 * sizeof(double)) == cudaSuccess;
+  ok = ok && cudaMalloc(&a->d_ghost, (size_t)a->WN * 5 * sizeof(int)) == cudaSuccess;
+  if (!ok) {
+    cudaGetLastError();
+    char buf[160];
+    snprintf(buf, sizeof buf, "the atlases of %d block slots (%.2f GB) do not fit", c.cap,
+             cap * (4.0 * a->CB + 2.0 * a->WN + 2.0 * a->PN) * 16 / 1e9);
+    return bail(SHZ_E_OOM, buf);
+  }
+  a->L.bt = a->d_bt;
+  a->L.w1 = a->w1;
+  a->L.w2 = a->w2;
+  a->L.p1 = a->p1;
+  a->L.p2 = a->p2;
+  // the tree of root blocks, a quiet uniform state, the clock at 0
+  try {
+    a->tree.reset(new BlockTree(c.ndim, c.nr, c.max_level, c.cap, c.hydro.bc_lo, c.hydro.bc_hi));
+  } catch (const std::exception& e) {
+    return bail(SHZ_E_CONFIG, e.what());
+  }
+  if (upload_tables(a) || write_clock(a, 0.0, 0)) return bail(SHZ_E_CUDA, a->err.c_str());
+  *out = a;
+  return SHZ_OK;
+}
+
+void shz_amr_destroy(shz_amr* a) {
+  if (!a) return;
+  Dev dv(a->device);
+  if (a->stream) cudaStreamSynchronize(a->stream);
+  drop_graphs(a);
+  for (int p = 0; p < 2; p++) {
+    cudaFree(a->u1[p]);
+    cudaFree(a->u2[p]);
+  }
+  void* bufs[] = {a->w1, a->w2, a->p1, a->p2, a->d_bt, a->d_all, a->d_leaves, a->d_rg, a->d_flags,
+                  a->clk, a->rates, a->diag_part, a->diag_out, a->d_ghost};
+  for (void* b : bufs)
+    if (b) cudaFree(b);
+  if (a->stream) cudaStreamDestroy(a->stream);
+  delete a;
+}
+
+int shz_amr_reset_problem(shz_amr* a, const shz_problem* prob) {
+  if (!a || !prob) return SHZ_E_CONFIG;
+  if (!shz::problem_known(prob->kind)) return fail(a, SHZ_E_CONFIG, "unknown problem kind %d", prob->kind);
+  Dev dv(a->device);
+  const shz_amr_config& c = a->cfg;
+  try {
+    a->tree.reset(new BlockTree(c.ndim, c.nr, c.max_level, c.cap, c.hydro.bc_lo, c.hydro.bc_hi));
+  } catch (const std::exception& e) {
+    return fail(a, SHZ_E_CONFIG, "%s", e.what());
+  }
+  int rc = upload_tables(a);
+  if (rc) return rc;
+  a->cur = 0;
+  a->slot = 0;
+  const shz::ProblemCtx q = shz::prepare_problem(fine_config(c), *prob);
+  const double dx0 = dx0_of(c), half = c.box / 2;
+  // The initial mesh: adapt over the sampled state, each pass re-sampling every leaf.
+  for (int pass = 0; pass <= c.max_level; pass++) {
+    if ((rc = sample_leaves(a, q))) return rc;
+    if (pass == c.max_level) break;
+    std::vector<double> feature(c.cap, 0.0);
+    for (int s : a->h_leaves) {
+      const int32_t* row = a->h_bt.data() + (size_t)s * shz::amr::BT_STRIDE;
+      const double side = dx0 / (double)(1 << row[0]) * shz::amr::BS;
+      double lo[3], hi[3];
+      for (int ax = 0; ax < 3; ax++) {
+        lo[ax] = row[1 + ax] * side - half;
+        hi[ax] = lo[ax] + side;
+      }
+      if (crosses(q, lo, hi, c.ndim)) feature[s] = 2.0 * c.refine_hi + 1.0;
+    }
+    int changed = 0;
+    if ((rc = check_and_regrid(a, &feature, &changed))) return rc;
+    if (!changed) break;
+  }
+  a->since_check = 0;
+  return write_clock(a, 0.0, 0);
+}
+
+int shz_amr_step(shz_amr* a, int32_t n) {
+  if (!a || n < 0) return SHZ_E_CONFIG;
+  Dev dv(a->device);
+  for (int i = 0; i < n; i++) {
+    int rc = step_once(a);
+    if (rc) return rc;
+    if (a->cfg.regrid_every > 0 && ++a->since_check >= a->cfg.regrid_every) {
+      a->since_check = 0;
+      int changed = 0;
+      if ((rc = check_and_regrid(a, nullptr, &changed))) return rc;
+    }
+  }
+  return 0;
+}
+
+int shz_amr_regrid(shz_amr* a, int32_t* changed) {
+  if (!a || !changed) return SHZ_E_CONFIG;
+  Dev dv(a->device);
+  int ch = 0;
+  int rc = check_and_regrid(a, nullptr, &ch);
+  *changed = ch;
+  return rc;
+}
+
+int shz_amr_clock(shz_amr* a, double* t, double* dt, int64_t* steps) {
+  if (!a) return SHZ_E_CONFIG;
+  Dev dv(a->device);
+  shz::DevClock h;
+  int rc = read_clock(a, &h);
+  if (rc) return rc;
+  if (t) *t = h.t;
+  if (dt) *dt = h.dt;
+  if (steps) *steps = h.steps;
+  if (h.bad) return fail(a, SHZ_E_NAN, "the clock is NaN after %lld steps", h.steps);
+  return 0;
+}
+
+int shz_amr_run(shz_amr* a, const shz_run_opts* o, shz_run_result* r) {
+  if (!a || !o || !r) return SHZ_E_CONFIG;
+  Dev dv(a->device);
+  const auto t0 = std::chrono::steady_clock::now();
+  auto ms = [&]() { return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count(); };
+  const bool has_until = !std::isnan(o->until);
+  if (o->steps < 0 && !has_until) return fail(a, SHZ_E_CONFIG, "run() needs `steps`, `until`, or both");
+  shz::DevClock c;
+  int rc = read_clock(a, &c);
+  if (rc) return rc;
+  const long long start = c.steps;
+  double last_dt = c.last_dt;
+  const double t_end_was = a->cfg.hydro.t_end;
+  const double stop = has_until ? std::min(o->until, t_end_was) : t_end_was;
+  if (stop != t_end_was) AMR_CUDA(a, cudaMemcpyAsync(&a->clk->t_end, &stop, sizeof(double), cudaMemcpyHostToDevice, a->stream));
+  int stopped = SHZ_STOP_STEPS;
+  int grow = 1;
+  for (;;) {
+    const long long taken = c.steps - start;
+    const long long left = o->steps < 0 ? std::numeric_limits<long long>::max() : o->steps - taken;
+    if (left <= 0) { stopped = SHZ_STOP_STEPS; break; }
+    if (has_until && c.t >= o->until * (1 - 1e-12)) { stopped = SHZ_STOP_TIME; break; }
+    if (std::isfinite(t_end_was) && c.t >= t_end_was * (1 - 1e-12)) { stopped = SHZ_STOP_END; break; }
+    if (o->timeout_ms > 0 && ms() > o->timeout_ms) { stopped = SHZ_STOP_TIMEOUT; break; }
+    long long batch = std::min<long long>(left, grow);
+    if (std::isfinite(stop) && last_dt > 0) {
+      const double ahead = std::ceil((stop - c.t) / last_dt - 1e-6);
+      if (ahead >= 1 && ahead < (double)batch) batch = (long long)ahead;
+    }
+    if ((rc = shz_amr_step(a, (int)std::max<long long>(batch, 1)))) break;
+    if ((rc = read_clock(a, &c))) break;
+    if (c.bad) { rc = fail(a, SHZ_E_NAN, "the clock is NaN after %lld steps", c.steps); break; }
+    if (c.last_dt > 0) last_dt = c.last_dt;
+    if (c.steps - start == taken) {
+      stopped = has_until && c.t >= o->until * (1 - 1e-9) ? SHZ_STOP_TIME : SHZ_STOP_END;
+      break;
+    }
+    grow = std::min(grow * 2, 64);
+  }
+  if (stop != t_end_was) {
+    cudaMemcpyAsync(&a->clk->t_end, &t_end_was, sizeof(double), cudaMemcpyHostToDevice, a->stream);
+    cudaStreamSynchronize(a->stream);
+  }
+  if (rc) return rc;
+  r->t = c.t;
+  r->dt = c.dt;
+  r->steps = c.steps;
+  r->taken = c.steps - start;
+  r->seconds = ms() / 1000.0;
+  r->stopped = stopped;
+  r->last_dt = last_dt;
+  return 0;
+}
+
+int shz_amr_diagnostics(shz_amr* a, shz_diag* d) {
+  if (!a || !d) return SHZ_E_CONFIG;
+  Dev dv(a->device);
+  AMR_CUDA(a, shz::amr_launch_diag(a->L, a->d_leaves, n_leaves(a), a->u1[a->cur], a->u2[a->cur], a->diag_part, a->diag_out,
+                                   a->stream));
+  a->launches += 2;
+  double v[9];
+  AMR_CUDA(a, cudaMemcpyAsync(v, a->diag_out, sizeof v, cudaMemcpyDeviceToHost, a->stream));
+  shz::DevClock c;
+  int rc = read_clock(a, &c);
+  if (rc) return rc;
+  d->t = c.t;
+  d->dt = c.dt;
+  d->steps = c.steps;
+  d->mass = v[0];
+  d->momentum[0] = v[1];
+  d->momentum[1] = v[2];
+  d->momentum[2] = v[3];
+  d->e_kin = v[4];
+  d->e_int = v[5];
+  d->e_tot = v[6];
+  d->floored = v[7];
+  d->max_mach = v[8];
+  return 0;
+}
+
+int shz_amr_leaves(shz_amr* a, int32_t* n, int32_t* slots, int32_t* levels, int32_t* coords) {
+  if (!a || !n) return SHZ_E_CONFIG;
+  *n = n_leaves(a);
+  for (int i = 0; i < n_leaves(a); i++) {
+    const int s = a->h_leaves[i];
+    const int32_t* row = a->h_bt.data() + (size_t)s * shz::amr::BT_STRIDE;
+    if (slots) slots[i] = s;
+    if (levels) levels[i] = row[0];
+    if (coords)
+      for (int ax = 0; ax < 3; ax++) coords[3 * i + ax] = row[1 + ax];
+  }
+  return 0;
+}
+
+int shz_amr_table(shz_amr* a, int32_t* out) {
+  if (!a || !out) return SHZ_E_CONFIG;
+  Dev dv(a->device);
+  AMR_CUDA(a, cudaMemcpyAsync(out, a->d_bt, sizeof(int32_t) * a->cfg.cap * shz::amr::BT_STRIDE, cudaMemcpyDeviceToHost,
+                              a->stream));
+  AMR_CUDA(a, cudaStreamSynchronize(a->stream));
+  return 0;
+}
+
+int shz_amr_get_leaves_state(shz_amr* a, float* u1, float* u2) {
+  if (!a || !u1 || !u2) return SHZ_E_CONFIG;
+  Dev dv(a->device);
+  const size_t bytes = (size_t)a->CB * sizeof(float4);
+  for (int i = 0; i < n_leaves(a); i++) {
+    const size_t s = (size_t)a->h_leaves[i] * a->CB;
+    AMR_CUDA(a, cudaMemcpyAsync(u1 + (size_t)i * a->CB * 4, a->u1[a->cur] + s, bytes, cudaMemcpyDeviceToHost, a->stream));
+    AMR_CUDA(a, cudaMemcpyAsync(u2 + (size_t)i * a->CB * 4, a->u2[a->cur] + s, bytes, cudaMemcpyDeviceToHost, a->stream));
+  }
+  AMR_CUDA(a, cudaStreamSynchronize(a->stream));
+  return 0;
+}
+
+int shz_amr_flags(shz_amr* a, float* out) {
+  if (!a || !out) return SHZ_E_CONFIG;
+  const size_t n = std::min<size_t>(a->h_flags.size(), (size_t)a->cfg.cap);
+  std::memset(out, 0, sizeof(float) * a->cfg.cap);
+  std::memcpy(out, a->h_flags.data(), n * sizeof(float));
+  return 0;
+}
+
+int shz_amr_ghost_map(shz_amr* a, int32_t slot, int32_t* out) {
+  if (!a || !out || slot < 0 || slot >= a->cfg.cap) return SHZ_E_CONFIG;
+  Dev dv(a->device);
+  AMR_CUDA(a, shz::amr_launch_ghost_map(a->L, slot, a->d_ghost, a->stream));
+  AMR_CUDA(a, cudaMemcpyAsync(out, a->d_ghost, sizeof(int32_t) * a->WN * 5, cudaMemcpyDeviceToHost, a->stream));
+  AMR_CUDA(a, cudaStreamSynchronize(a->stream));
+  return 0;
+}
+
+int shz_amr_profile(shz_amr* a, int32_t n, shz_profile_result* out) {
+  if (!a || !out || n < 1) return SHZ_E_CONFIG;
+  Dev dv(a->device);
+  cudaEvent_t e0, e1;
+  AMR_CUDA(a, cudaEventCreate(&e0));
+  AMR_CUDA(a, cudaEventCreate(&e1));
+  const long long l0 = a->launches;
+  AMR_CUDA(a, cudaEventRecord(e0, a->stream));
+  int rc = shz_amr_step(a, n);
+  AMR_CUDA(a, cudaEventRecord(e1, a->stream));
+  AMR_CUDA(a, cudaEventSynchronize(e1));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  out->steps = n;
+  out->total_ms = ms;
+  out->sweep_ms = ms;
+  out->launches = a->launches - l0;
+  return 0;
+}
+
+int64_t shz_amr_kernel_launches(const shz_amr* a) { return a ? a->launches : 0; }
+
+}  // extern "C"

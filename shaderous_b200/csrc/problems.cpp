@@ -53,97 +53,114 @@ int64_t sedov_count(const shz_config& c, double radius) {
 
 }  // namespace
 
+ProblemCtx prepare_problem(const shz_config& c, const shz_problem& p) {
+  ProblemCtx x;
+  x.p = p;
+  x.gamma = c.gamma;
+  x.nd = ndim_of(c);
+  x.L[0] = c.n[0] * c.dx;
+  x.L[1] = c.n[1] * c.dx;
+  x.L[2] = c.n[2] * c.dx;
+  if (p.kind == SHZ_PROB_SEDOV) {
+    x.sedov_r = p.a[3] * c.dx;
+    const int64_t cnt = sedov_count(c, x.sedov_r);
+    const double e_dep = p.a[2] / ((double)(cnt > 0 ? cnt : 1) * std::pow(c.dx, x.nd));
+    x.sedov_p = (c.gamma - 1) * e_dep;
+  }
+  return x;
+}
+
+// The primitives (rho, vx, vy, vz, p, s) at a cell centre (x, y, z), box centred on 0; `cell`
+// numbers the cell for the seeded noise.
+void sample_problem(const ProblemCtx& q, double x, double y, double z, uint64_t cell, double* w) {
+  const shz_problem& p = q.p;
+  const int nd = q.nd;
+  const double Lx = q.L[0], Ly = q.L[1], Lz = q.L[2];
+  double rho = 1, vx = 0, vy = 0, vz = 0, pr = 1, s = 0;
+  switch (p.kind) {
+    case SHZ_PROB_SOD: {
+      const double xn = p.axis == 0 ? x : (p.axis == 1 ? y : z);
+      const bool left = xn < 0;
+      rho = left ? p.a[0] : p.a[3];
+      const double u = left ? p.a[1] : p.a[4];
+      pr = left ? p.a[2] : p.a[5];
+      (p.axis == 0 ? vx : (p.axis == 1 ? vy : vz)) = u;
+      s = left ? 1 : 0;
+      break;
+    }
+    case SHZ_PROB_KH: {
+      // A dense slab |y - 1/2| < 1/4 of [0,1]^2 sliding through lighter gas; a seeded mode and
+      // gaussian noise in vy (the kick of src/setup/parts/flows/kelvin_helmholtz.ts, with the
+      // perturbation of the benchmark's own statement).
+      const double X = x + Lx / 2, Y = y + Ly / 2;
+      const bool inner = std::fabs(Y - 0.5 * Ly) < 0.25 * Ly;
+      rho = inner ? p.a[0] : p.a[1];
+      vx = inner ? p.a[2] : -p.a[2];
+      vy = p.a[4] * std::sin(4 * PI * X / Lx) + p.a[5] * gauss(p.seed, cell);
+      pr = p.a[3];
+      s = inner ? 1 : 0;
+      break;
+    }
+    case SHZ_PROB_TGV: {
+      // On [0, 2 pi]^3 (box centred on 0, so shifted by half the box).
+      const double X = (x + Lx / 2) * (2 * PI / Lx), Y = (y + Ly / 2) * (2 * PI / Ly), Z = (z + Lz / 2) * (2 * PI / Lz);
+      rho = p.a[0];
+      vx = p.a[2] * std::sin(X) * std::cos(Y) * std::cos(Z);
+      vy = -p.a[2] * std::cos(X) * std::sin(Y) * std::cos(Z);
+      vz = 0;
+      pr = p.a[1];
+      s = 0;
+      break;
+    }
+    case SHZ_PROB_SEDOV: {
+      const double r = std::sqrt(x * x + (nd >= 2 ? y * y : 0) + (nd == 3 ? z * z : 0));
+      rho = p.a[0];
+      pr = r < q.sedov_r ? q.sedov_p : p.a[1];
+      s = r < q.sedov_r ? 1 : 0;
+      break;
+    }
+    case SHZ_PROB_ADVECT: {
+      const double X = x + Lx / 2;
+      rho = p.a[0] + p.a[1] * std::sin(2 * PI * X / Lx);
+      vx = p.a[2]; vy = p.a[3]; vz = p.a[4];
+      pr = p.a[5];
+      s = X < 0.5 * Lx ? 1 : 0;
+      break;
+    }
+    case SHZ_PROB_BLAST: {
+      const double r = std::sqrt(x * x + (nd >= 2 ? y * y : 0) + (nd == 3 ? z * z : 0));
+      const bool in = r < p.a[4];
+      rho = in ? p.a[0] : p.a[2];
+      pr = in ? p.a[1] : p.a[3];
+      s = in ? 1 : 0;
+      break;
+    }
+    case SHZ_PROB_GAUSS: {
+      const double r2 = x * x + y * y;
+      rho = p.a[0] + std::exp(-r2 / p.a[1]);
+      vx = p.a[2]; vy = p.a[3];
+      vz = p.a[4] * std::sin(8 * PI * z);
+      pr = p.a[5] + 0.5 * std::exp(-r2 / p.a[6]);
+      s = 0;
+      break;
+    }
+    default:
+      break;
+  }
+  w[0] = rho; w[1] = vx; w[2] = vy; w[3] = vz; w[4] = pr; w[5] = s;
+}
+
 int problem_prims(const shz_config& c, const shz_problem& p, int k0, int k1, double* out) {
   const int nx = c.n[0], ny = c.n[1], nz = c.n[2];
   const double dx = c.dx;
-  const int nd = ndim_of(c);
-  double sedov_p = 0, sedov_r = 0;
-  if (p.kind == SHZ_PROB_SEDOV) {
-    sedov_r = p.a[3] * dx;
-    const int64_t cnt = sedov_count(c, sedov_r);
-    const double e_dep = p.a[2] / ((double)(cnt > 0 ? cnt : 1) * std::pow(dx, nd));
-    sedov_p = (c.gamma - 1) * e_dep;
-  }
-  const double Lx = nx * dx, Ly = ny * dx, Lz = nz * dx;
+  const ProblemCtx q = prepare_problem(c, p);
 #pragma omp parallel for collapse(2) schedule(static)
   for (int k = k0; k < k1; k++)
     for (int j = 0; j < ny; j++)
       for (int i = 0; i < nx; i++) {
         const double x = (i + 0.5 - nx / 2.0) * dx, y = (j + 0.5 - ny / 2.0) * dx, z = (k + 0.5 - nz / 2.0) * dx;
         const uint64_t cell = ((uint64_t)k * ny + j) * nx + i;
-        double* w = out + ((int64_t)(k - k0) * ny * nx + (int64_t)j * nx + i) * 6;
-        double rho = 1, vx = 0, vy = 0, vz = 0, pr = 1, s = 0;
-        switch (p.kind) {
-          case SHZ_PROB_SOD: {
-            const double xn = p.axis == 0 ? x : (p.axis == 1 ? y : z);
-            const bool left = xn < 0;
-            rho = left ? p.a[0] : p.a[3];
-            const double u = left ? p.a[1] : p.a[4];
-            pr = left ? p.a[2] : p.a[5];
-            (p.axis == 0 ? vx : (p.axis == 1 ? vy : vz)) = u;
-            s = left ? 1 : 0;
-            break;
-          }
-          case SHZ_PROB_KH: {
-            // A dense slab |y - 1/2| < 1/4 of [0,1]^2 sliding through lighter gas; a seeded mode
-            // and gaussian noise in vy (the kick of src/setup/parts/flows/kelvin_helmholtz.ts,
-            // with the perturbation of the benchmark's own statement).
-            const double X = x + Lx / 2, Y = y + Ly / 2;
-            const bool inner = std::fabs(Y - 0.5 * Ly) < 0.25 * Ly;
-            rho = inner ? p.a[0] : p.a[1];
-            vx = inner ? p.a[2] : -p.a[2];
-            vy = p.a[4] * std::sin(4 * PI * X / Lx) + p.a[5] * gauss(p.seed, cell);
-            pr = p.a[3];
-            s = inner ? 1 : 0;
-            break;
-          }
-          case SHZ_PROB_TGV: {
-            // On [0, 2 pi]^3 (box centred on 0, so shifted by half the box).
-            const double X = (x + Lx / 2) * (2 * PI / Lx), Y = (y + Ly / 2) * (2 * PI / Ly), Z = (z + Lz / 2) * (2 * PI / Lz);
-            rho = p.a[0];
-            vx = p.a[2] * std::sin(X) * std::cos(Y) * std::cos(Z);
-            vy = -p.a[2] * std::cos(X) * std::sin(Y) * std::cos(Z);
-            vz = 0;
-            pr = p.a[1];
-            s = 0;
-            break;
-          }
-          case SHZ_PROB_SEDOV: {
-            const double r = std::sqrt(x * x + (nd >= 2 ? y * y : 0) + (nd == 3 ? z * z : 0));
-            rho = p.a[0];
-            pr = r < sedov_r ? sedov_p : p.a[1];
-            s = r < sedov_r ? 1 : 0;
-            break;
-          }
-          case SHZ_PROB_ADVECT: {
-            const double X = x + Lx / 2;
-            rho = p.a[0] + p.a[1] * std::sin(2 * PI * X / Lx);
-            vx = p.a[2]; vy = p.a[3]; vz = p.a[4];
-            pr = p.a[5];
-            s = X < 0.5 * Lx ? 1 : 0;
-            break;
-          }
-          case SHZ_PROB_BLAST: {
-            const double r = std::sqrt(x * x + (nd >= 2 ? y * y : 0) + (nd == 3 ? z * z : 0));
-            const bool in = r < p.a[4];
-            rho = in ? p.a[0] : p.a[2];
-            pr = in ? p.a[1] : p.a[3];
-            s = in ? 1 : 0;
-            break;
-          }
-          case SHZ_PROB_GAUSS: {
-            const double r2 = x * x + y * y;
-            rho = p.a[0] + std::exp(-r2 / p.a[1]);
-            vx = p.a[2]; vy = p.a[3];
-            vz = p.a[4] * std::sin(8 * PI * z);
-            pr = p.a[5] + 0.5 * std::exp(-r2 / p.a[6]);
-            s = 0;
-            break;
-          }
-          default:
-            break;
-        }
-        w[0] = rho; w[1] = vx; w[2] = vy; w[3] = vz; w[4] = pr; w[5] = s;
+        sample_problem(q, x, y, z, cell, out + ((int64_t)(k - k0) * ny * nx + (int64_t)j * nx + i) * 6);
       }
   return 0;
 }

@@ -31,6 +31,7 @@
 #include <cstdint>
 #include <cstdio>
 
+#include "hydro_cell.cuh"
 #include "hydro_math.cuh"
 #include "sweep.h"
 
@@ -90,79 +91,6 @@ __device__ __forceinline__ void read_w(const float* __restrict__ sWb, int wx, in
   using G = Geo<DIM, RECON>;
 #pragma unroll
   for (int c = 0; c < 6; c++) w[c] = sWb[c * G::WN + wy * G::WX + wx];
-}
-
-// The per-cell result of the predictor (hydro.ts:272-322 predictRaw): the half-step state q,
-// the shock flag and the first-order flag.
-struct Pred {
-  float q[6];
-  float flag;
-  bool fo;
-};
-
-// hydro.ts:294-321: slopes -> shock flag -> Hancock half step -> positivity fallback, given the
-// edge increments su/sd per active axis and the convergence and pressure jump the neighbours give.
-template <int DIM>
-__device__ __forceinline__ void hancock(const float* c, float conv, float jump, const float (*su)[6], const float (*sd)[6],
-                                        float h, const KParams& P, Pred& out) {
-  float big = 0.f, fall = 0.f, dv = 0.f;
-  float adv[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-  float gradp[3] = {0.f, 0.f, 0.f};
-#pragma unroll
-  for (int a = 0; a < DIM; a++) {
-    big = fmaxf(big, fmaxf(fabsf(su[a][4]), fabsf(sd[a][4])));
-    fall = fminf(fall, fminf(0.5f * su[a][0], -0.5f * sd[a][0]));
-    const float va = c[1 + a];
-#pragma unroll
-    for (int v = 0; v < 6; v++) adv[v] += va * (0.5f * (su[a][v] + sd[a][v]));
-    dv += 0.5f * (su[a][1 + a] + sd[a][1 + a]);
-    gradp[a] = 0.5f * (su[a][4] + sd[a][4]);
-  }
-  out.flag = (conv < 0.f && jump > P.shock_thresh) ? 1.f : 0.f;
-  const float rho = c[0], cs = c[6];
-  const float inv_rho = 1.f / rho;
-  float qh[6];
-  qh[0] = rho - h * (adv[0] + rho * dv);
-#pragma unroll
-  for (int d = 0; d < 3; d++) qh[1 + d] = c[1 + d] - h * (adv[1 + d] + gradp[d] * inv_rho);
-  qh[4] = c[4] - h * (adv[4] + rho * cs * cs * dv);
-  qh[5] = c[5] - h * adv[5];
-  const float rmin = qh[0] + fall;
-  const float pmin = qh[4] - 0.5f * big;
-  out.fo = !(rmin > 0.f && pmin > 0.f);
-#pragma unroll
-  for (int v = 0; v < 6; v++) out.q[v] = out.fo ? c[v] : qh[v];
-}
-
-// Face state q + 0.5 sgn inc (q alone when first order: the increments are zeroed), with the
-// cell's shock flag (hydro.ts:362 side's f(n)).
-__device__ __forceinline__ void face_state(const Pred& pr, const float* inc, float sgn, float* f) {
-  const float k = pr.fo ? 0.f : 0.5f * sgn;
-#pragma unroll
-  for (int v = 0; v < 6; v++) f[v] = pr.q[v] + k * inc[v];
-  f[6] = pr.flag;
-}
-
-// The update of one cell (hydro.ts:422-446): conservative update, dual-energy switch and floors.
-// acc = (dm, dmx, dmy, dmz, de, dei, ds, dvn) summed with the reference's signs; ph = the
-// cell's half-step pressure.
-__device__ __forceinline__ void update_cell(const float4 a, const float4 b, const float* acc, float ph, float dtdx,
-                                            const KParams& P, float4& na, float4& nb) {
-  const float rho = fmaxf(a.x + dtdx * acc[0], P.rho_floor);
-  const float mx = a.y + dtdx * acc[1], my = a.z + dtdx * acc[2], mz = a.w + dtdx * acc[3];
-  float E = b.x + dtdx * acc[4];
-  float eint = b.y + dtdx * (acc[5] + fmaxf(ph, P.p_floor) * acc[7]);
-  const float ke = (0.5f * (mx * mx + my * my + mz * mz)) / rho;
-  const float eth = E - ke;
-  const float emin = P.e_floor;
-  if (eth > P.eta_dual * E && eth >= emin) {
-    eint = eth;
-  } else {
-    if (!(eint >= emin)) eint = emin;
-    E = ke + eint;
-  }
-  na = make_float4(rho, mx, my, mz);
-  nb = make_float4(E, eint, b.z + dtdx * acc[6], b.w);
 }
 
 __device__ __forceinline__ float warp_max(float v) {
