@@ -54,7 +54,71 @@ def parse():
     ap.add_argument("--recon", default="ppm")
     ap.add_argument("--e2e-steps", type=int, default=200)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-amr", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=200)
     return ap.parse_args()
+
+
+def amr_sedov(levels=4, nr=8, radius_cells=3.5, steps=24, cap=26000, grown=False):
+    """3D Sedov blast on the block grid: 16^3-cell blocks, levels 0-levels above nr^3 roots (finest
+    nr * 16 << levels cells per side), E = 1 spread over the finest cells within radius_cells of
+    the centre, Löhner refinement above 0.1 (below 0.05 merges), a refinement check every 8 steps.
+    Zone-updates are leaf cells x steps, the leaves counted at the start and end of the timed run."""
+    from shaderous_b200 import Config, Problem
+    from shaderous_b200.amr import AmrConfig, AmrSim
+
+    hyd = Config(gamma=5 / 3, bc_lo=(1, 1, 1), bc_hi=(1, 1, 1), recon="koren", isentropic=True, cfl=0.5, p_floor=1e-12)
+    cfg = AmrConfig(hydro=hyd, ndim=3, nr=nr, max_level=levels, cap=cap, refine_hi=0.1, refine_lo=0.05, regrid_every=8)
+    t0 = time.perf_counter()
+    with AmrSim(cfg) as a:
+        if grown:
+            # the same energy (E = 1, gamma = 5/3) as a uniform hot sphere of radius 0.2
+            r = 0.2
+            prob = Problem("blast", a=(1.0, (2.0 / 3.0) / (4.0 / 3.0 * math.pi * r ** 3), 1.0, 1e-5, r))
+        else:
+            prob = Problem("sedov", a=(1.0, 1e-5, 1.0, radius_cells))
+        a.reset(prob)
+        t_init = time.perf_counter() - t0
+        a.profile(8)  # warm-up, including one refinement check
+        n0 = len(a.leaves()[0])
+        l0 = a.kernel_launches
+        prof = a.profile(steps)
+        n1 = len(a.leaves()[0])
+        _, lv, _ = a.leaves()
+        launches = a.kernel_launches - l0
+    leaf_cells = 0.5 * (n0 + n1) * 4096
+    return {"value": leaf_cells * steps / (prof["total_ms"] / 1000.0), "unit": UNIT, "steps": steps,
+            "ms_per_step": prof["total_ms"] / steps, "leaf_blocks": [n0, n1], "levels": int(lv.max()) + 1,
+            "finest_cells_per_side": nr * 16 << levels, "radius_finest_cells": 0.2 * (nr * 16 << levels) if grown else radius_cells,
+            "init_s": t_init, "gpu_launches": launches,
+            "note": "time includes the refinement checks (flag, host adapt, regrid) every 8 steps"}
+
+
+def serving(n_requests=200, seed=2024, budget=150e9):
+    """A seeded stream of Sod / Kelvin-Helmholtz / blast requests with Poisson arrivals, served with
+    continuous batching, and the same stream run one request after another through the plain
+    uniform-grid step."""
+    from shaderous_b200.serve import Server, ServerConfig, plain_run_stream, request_stream
+
+    reqs = request_stream(n_requests, seed=seed, rate=100.0, sizes2=(64, 512), sizes3=(32, 128), steps=(100, 500))
+    cfg = ServerConfig(budget_bytes=budget, max_grids=512, round_steps=8)
+    try:
+        srv = Server(cfg)
+    except Exception:
+        cfg.budget_bytes = budget / 3
+        srv = Server(cfg)
+    with srv:
+        batched = srv.run_stream(reqs)
+    plain = plain_run_stream(cfg, reqs)
+    keep = ["completed", "makespan_s", "p50_s", "p99_s", "mean_s", "zone_updates", "zu_per_s", "max_concurrent",
+            "kernel_launches"]
+    return {"requests": n_requests,
+            "stream": f"seeded (seed {seed}) Poisson arrivals at 100/s; Sod, KH or blast; 2D 64^2-512^2 and 3D "
+                      f"32^3-128^3 log-uniform; 100-500 steps; rho ratio U[1,10], p ratio log-U[1,1000], gamma "
+                      f"1.4 or 5/3; koren+HLLC; budget {cfg.budget_bytes / 1e9:.0f} GB",
+            "batched": {k: batched[k] for k in keep}, "plain": {k: plain[k] for k in keep},
+            "aggregate_speedup": batched["zu_per_s"] / plain["zu_per_s"] if plain["zu_per_s"] else None}
 
 
 def workload(n: int, recon: str):
@@ -277,10 +341,18 @@ def main():
     if not np.isfinite(h_out1[:: max(1, ncell // 4096)].numpy()).all():
         raise RuntimeError("non-finite state after the end-to-end run")
 
+    sim.destroy()
+    del h_in1, h_in2, h_out1, h_out2
+    amr = serve = None
+    if rank == 0 and not args.no_amr:
+        amr = {"spec": amr_sedov(), "developed": amr_sedov(steps=16, grown=True)}
+        amr["developed"]["note"] += ("; the same blast with the energy spread within 0.2 of the box, the mesh of the "
+                                     "grown blast (about 20k blocks) that the spec's run reaches later")
+    if rank == 0 and not args.no_serving:
+        serve = serving(args.serve_requests)
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_sample(args.recon)
-    sim.destroy()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -306,6 +378,10 @@ def main():
     }
     if cpu:
         line["cpu_baseline"] = cpu
+    if amr:
+        line["amr_sedov"] = amr
+    if serve:
+        line["serving"] = serve
     print(json.dumps(line), flush=True)
 
 

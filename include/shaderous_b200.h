@@ -281,6 +281,64 @@ int shz_amr_ghost_map(shz_amr* a, int32_t slot, int32_t* out);
 int shz_amr_profile(shz_amr* a, int32_t n, shz_profile_result* out);
 int64_t shz_amr_kernel_launches(const shz_amr* a);
 
+/*
+ * Serving: independent hydro runs ("requests") of uneven sizes kept resident in HBM and advanced
+ * together. Every request is a uniform grid of 16^ndim-cell blocks; the blocks of all running
+ * requests form one work list that the adaptive grid's passes walk each step (one CUDA graph per
+ * step, per-request parameters and clocks). Requests are admitted against a memory budget as
+ * block slots free up, between rounds of `round_steps` steps (continuous batching). No
+ * counterpart in the reference, whose nearest form is its sequential `sweep` runs
+ * (tools/headless/cli.mjs:367-380).
+ */
+typedef struct shz_request {
+  int32_t ndim;          /* 2 or 3 */
+  int32_t n;             /* cells per side, a multiple of 16 */
+  int32_t steps;         /* steps to take */
+  int32_t bc;            /* boundary code on every face */
+  double gamma;
+  double arrival;        /* seconds after the stream starts (shz_server_run_stream) */
+  shz_problem problem;   /* initial condition on the unit box */
+} shz_request;
+
+typedef struct shz_server_config {
+  shz_config hydro;      /* scheme and floors for every request (gamma and bc come per request) */
+  double budget_bytes;   /* device memory for resident request state */
+  int32_t max_grids;     /* requests in flight at most */
+  int32_t round_steps;   /* steps between admission and completion checks */
+  int32_t keep_states;   /* 1: keep each finished request's state for shz_server_state */
+} shz_server_config;
+
+typedef struct shz_server_stats {
+  int64_t completed;
+  double makespan_s;       /* first arrival to last completion */
+  double p50_s, p99_s;     /* completion latency: finish - arrival */
+  double mean_s;
+  double zone_updates;     /* cells x steps over all requests */
+  double zu_per_s;         /* zone_updates / makespan */
+  int64_t max_concurrent;  /* requests in flight at once, at most */
+  int64_t rounds;
+  int64_t kernel_launches;
+} shz_server_stats;
+
+typedef struct shz_server shz_server;
+int shz_server_create(const shz_server_config* cfg, shz_server** out);
+void shz_server_destroy(shz_server* s);
+const char* shz_server_error(const shz_server* s);
+/* Queue a request now; *id numbers it. */
+int shz_server_submit(shz_server* s, const shz_request* req, int64_t* id);
+/* Run rounds until every queued request has finished (or max_rounds rounds, if > 0). */
+int shz_server_drain(shz_server* s, int32_t max_rounds);
+/* Run a stream: request i is queued once the wall clock passes reqs[i].arrival seconds after the
+ * call starts; returns when all are done, with latency statistics. */
+int shz_server_run_stream(shz_server* s, const shz_request* reqs, int32_t n, shz_server_stats* out);
+/* The conservation totals of a finished request, and (keep_states) its final state as uniform
+ * arrays of n^ndim cells, x fastest. */
+int shz_server_result(shz_server* s, int64_t id, shz_diag* diag);
+int shz_server_state(shz_server* s, int64_t id, float* u1, float* u2);
+/* The same stream run one request after another, each through the plain uniform-grid step
+ * (shz_create / shz_reset_problem / shz_run / shz_destroy), for comparison. */
+int shz_plain_run_stream(const shz_server_config* cfg, const shz_request* reqs, int32_t n, shz_server_stats* out);
+
 /* Launches of the library's own kernels on this handle since creation. */
 int64_t shz_kernel_launches(const shz_sim* sim);
 

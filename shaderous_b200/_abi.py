@@ -99,6 +99,43 @@ class shz_amr_config(C.Structure):
     ]
 
 
+class shz_request(C.Structure):
+    _fields_ = [
+        ("ndim", C.c_int32),
+        ("n", C.c_int32),
+        ("steps", C.c_int32),
+        ("bc", C.c_int32),
+        ("gamma", C.c_double),
+        ("arrival", C.c_double),
+        ("problem", shz_problem),
+    ]
+
+
+class shz_server_config(C.Structure):
+    _fields_ = [
+        ("hydro", shz_config),
+        ("budget_bytes", C.c_double),
+        ("max_grids", C.c_int32),
+        ("round_steps", C.c_int32),
+        ("keep_states", C.c_int32),
+    ]
+
+
+class shz_server_stats(C.Structure):
+    _fields_ = [
+        ("completed", C.c_int64),
+        ("makespan_s", C.c_double),
+        ("p50_s", C.c_double),
+        ("p99_s", C.c_double),
+        ("mean_s", C.c_double),
+        ("zone_updates", C.c_double),
+        ("zu_per_s", C.c_double),
+        ("max_concurrent", C.c_int64),
+        ("rounds", C.c_int64),
+        ("kernel_launches", C.c_int64),
+    ]
+
+
 class shz_profile_result(C.Structure):
     _fields_ = [("steps", C.c_int32), ("total_ms", C.c_double), ("sweep_ms", C.c_double), ("launches", C.c_int64)]
 
@@ -157,6 +194,15 @@ SIGNATURES = [
     ("shz_amr_ghost_map", C.c_int, [C.c_void_p, C.c_int32, C.c_void_p]),
     ("shz_amr_profile", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(shz_profile_result)]),
     ("shz_amr_kernel_launches", C.c_int64, [C.c_void_p]),
+    ("shz_server_create", C.c_int, [C.POINTER(shz_server_config), C.POINTER(C.c_void_p)]),
+    ("shz_server_destroy", None, [C.c_void_p]),
+    ("shz_server_error", C.c_char_p, [C.c_void_p]),
+    ("shz_server_submit", C.c_int, [C.c_void_p, C.POINTER(shz_request), C.POINTER(C.c_int64)]),
+    ("shz_server_drain", C.c_int, [C.c_void_p, C.c_int32]),
+    ("shz_server_run_stream", C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(shz_server_stats)]),
+    ("shz_server_result", C.c_int, [C.c_void_p, C.c_int64, C.POINTER(shz_diag)]),
+    ("shz_server_state", C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]),
+    ("shz_plain_run_stream", C.c_int, [C.POINTER(shz_server_config), C.c_void_p, C.c_int32, C.POINTER(shz_server_stats)]),
     ("shz_totals_noalloc", C.c_int, [C.POINTER(shz_config), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("shz_totals_noalloc_error", C.c_char_p, []),
 ]

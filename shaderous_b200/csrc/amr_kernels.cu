@@ -27,6 +27,9 @@ namespace shz {
 namespace amrk {
 
 constexpr int BS = 16, NG = 2, PAD = BS + 2 * NG, PP = BS + 2, BTS = 32, RGS = 12;
+// Word of a block-table row that holds the block's grid: an index into the per-grid parameters
+// and clocks (a batch advances blocks of many independent grids in one pass).
+constexpr int GRID_WORD = 26;
 constexpr int NT = 256;  // threads per CTA
 
 template <int DIM>
@@ -235,7 +238,7 @@ __device__ __forceinline__ Cons prolong_child(const Cons& uc, const Slopes& s, c
 template <int DIM, int R>
 __device__ __forceinline__ Cons from_coarse(const int* __restrict__ bt, const float4* __restrict__ u1,
                                             const float4* __restrict__ u2, int nr, int slot, const int* l, int cs,
-                                            float rho_floor) {
+                                            float rho_floor) {  // nr: root blocks per side of the block's grid
   const int nc = nr * BS << bt_at(bt, cs, 0);
   int gf[3], lc[3], par[3];
 #pragma unroll
@@ -280,16 +283,19 @@ __device__ __forceinline__ float rate_guard_f(float r) { return (r == r) ? r : _
 // 1. Primitives of every block in the list with two ghost layers; the rate / dx maximum over the
 // leaves' own cells (assemble.wgsl:78-154; PER_DX in clock.wgsl).
 template <int DIM, int R>
-__global__ void __launch_bounds__(NT) amr_assemble(const KParams P, const int* __restrict__ bt, int nr, double dx0,
+__global__ void __launch_bounds__(NT) amr_assemble(const KParams* __restrict__ gp, const int* __restrict__ bt,
                                                    const int* __restrict__ list, int n, const float4* __restrict__ u1,
                                                    const float4* __restrict__ u2, float4* __restrict__ w1,
-                                                   float4* __restrict__ w2, unsigned* __restrict__ rate_out) {
+                                                   float4* __restrict__ w2, unsigned* __restrict__ rates, int rslot) {
   __shared__ float sRed[NT / 32];
-  float rmax = 0.f;
   for (int i = blockIdx.x; i < n; i += gridDim.x) {
+    float rmax = 0.f;
     const int slot = __ldg(list + i);
+    const int g = bt_at(bt, slot, GRID_WORD);
+    const KParams& P = gp[g];
+    const int nr = P.n[0];
     const bool leaf = leaf_of(bt, slot);
-    const float inv_dx = (float)(ldexp(1.0, bt_at(bt, slot, 0)) / dx0);
+    const float inv_dx = (float)(ldexp(1.0, bt_at(bt, slot, 0)) / P.dx);
     for (int t = threadIdx.x; t < BG<DIM>::WN; t += NT) {
       int l[3] = {t % PAD - NG, (t / PAD) % PAD - NG, DIM == 3 ? t / (PAD * PAD) - NG : 0};
       const Src s = ghost_src_any<DIM>(bt, slot, l);
@@ -312,9 +318,9 @@ __global__ void __launch_bounds__(NT) amr_assemble(const KParams P, const int* _
       for (int a = 0; a < DIM; a++) inside = inside && l[a] >= 0 && l[a] < BS;
       if (inside) rmax = fmaxf(rmax, rate_guard_f(fabsf(w[1]) + fabsf(w[2]) + fabsf(w[3]) + P.signal * w[6]) * inv_dx);
     }
+    const float m = block_max(rmax, sRed);
+    if (threadIdx.x == 0 && leaf) atomicMax(rates + 2 * g + rslot, __float_as_uint(m));
   }
-  const float m = block_max(rmax, sRed);
-  if (threadIdx.x == 0) atomicMax(rate_out, __float_as_uint(m));
 }
 
 template <int DIM>
@@ -330,14 +336,16 @@ __device__ __forceinline__ void load_w(const float4* __restrict__ w1, const floa
 // same-level or boundary ghost is predicted at its source and mirrored; a ghost beside a coarser
 // block in place, its transverse slopes dropped at the rim of the face.
 template <int DIM, int R, bool ISEN>
-__global__ void __launch_bounds__(NT) amr_predict(const KParams P, const int* __restrict__ bt, double dx0,
+__global__ void __launch_bounds__(NT) amr_predict(const KParams* __restrict__ gp, const int* __restrict__ bt,
                                                   const int* __restrict__ list, int n, const float4* __restrict__ w1,
                                                   const float4* __restrict__ w2, float4* __restrict__ p1,
-                                                  float4* __restrict__ p2, const DevClock* __restrict__ clk) {
-  const double dt = clk->dt;
+                                                  float4* __restrict__ p2, const DevClock* __restrict__ clks) {
   for (int i = blockIdx.x; i < n; i += gridDim.x) {
     const int slot = __ldg(list + i);
-    const float h = (float)((0.5 * dt) * ldexp(1.0, bt_at(bt, slot, 0)) / dx0);
+    const int g = bt_at(bt, slot, GRID_WORD);
+    const KParams& P = gp[g];
+    const double dt = clks[g].dt;
+    const float h = (float)((0.5 * dt) * ldexp(1.0, bt_at(bt, slot, 0)) / P.dx);
     for (int t = threadIdx.x; t < BG<DIM>::PN; t += NT) {
       int l[3] = {t % PP - 1, (t / PP) % PP - 1, DIM == 3 ? t / (PP * PP) - 1 : 0};
       const Src s = ghost_src<DIM>(bt, slot, l);
@@ -461,20 +469,22 @@ __device__ __forceinline__ void match_face(const KParams& P, const int* __restri
 // also the block's upper face) into shared memory, and its z faces in registers, so every face
 // is solved once.
 template <int DIM, int R, bool ISEN>
-__global__ void __launch_bounds__(NT) amr_update(const KParams P, const int* __restrict__ bt, double dx0,
+__global__ void __launch_bounds__(NT) amr_update(const KParams* __restrict__ gp, const int* __restrict__ bt,
                                                  const int* __restrict__ list, int n, const float4* __restrict__ u1,
                                                  const float4* __restrict__ u2, const float4* __restrict__ w1,
                                                  const float4* __restrict__ w2, const float4* __restrict__ p1,
                                                  const float4* __restrict__ p2, float4* __restrict__ o1,
-                                                 float4* __restrict__ o2, const DevClock* __restrict__ clk) {
+                                                 float4* __restrict__ o2, const DevClock* __restrict__ clks) {
   __shared__ float sFx[8][BS * (BS + 1)];
   __shared__ float sFy[8][BS * (BS + 1)];
-  const double dt = clk->dt;
-  const bool held = clk->held != 0;
   const int tx = threadIdx.x % BS, ty = threadIdx.x / BS;
   for (int i = blockIdx.x; i < n; i += gridDim.x) {
     const int slot = __ldg(list + i);
-    const float dtdx = (float)(dt * ldexp(1.0, bt_at(bt, slot, 0)) / dx0);
+    const int g = bt_at(bt, slot, GRID_WORD);
+    const KParams& P = gp[g];
+    const double dt = clks[g].dt;
+    const bool held = clks[g].held != 0;
+    const float dtdx = (float)(dt * ldexp(1.0, bt_at(bt, slot, 0)) / P.dx);
     float Fzlo[8];
     const int nk = DIM == 3 ? BS : 1;
     for (int k = 0; k < nk; k++) {
@@ -597,12 +607,14 @@ __global__ void __launch_bounds__(NT) amr_flag(const int* __restrict__ list, int
 // consistent (each child's own kinetic energy plus its interpolated internal energy, less one
 // shared offset that keeps the mean total energy the coarse cell's).
 template <int DIM, int R>
-__global__ void __launch_bounds__(NT) amr_regrid(const KParams P, const int* __restrict__ rg, const int* __restrict__ list,
+__global__ void __launch_bounds__(NT) amr_regrid(const KParams* __restrict__ gp, const int* __restrict__ bt,
+                                                 const int* __restrict__ rg, const int* __restrict__ list,
                                                  int n, const float4* __restrict__ u1, const float4* __restrict__ u2,
                                                  const float4* __restrict__ w1, const float4* __restrict__ w2,
                                                  float4* __restrict__ o1, float4* __restrict__ o2) {
   for (int i = blockIdx.x; i < n; i += gridDim.x) {
     const int slot = __ldg(list + i);
+    const KParams& P = gp[bt_at(bt, slot, GRID_WORD)];
     const int kind = __ldg(rg + slot * RGS), src = __ldg(rg + slot * RGS + 1), oct = __ldg(rg + slot * RGS + 2);
     for (int t = threadIdx.x; t < BG<DIM>::CB; t += NT) {
       int l[3] = {t % BS, (t / BS) % BS, DIM == 3 ? t / (BS * BS) : 0};
@@ -680,7 +692,7 @@ struct AccD {
   }
 };
 template <int DIM>
-__global__ void __launch_bounds__(NT) amr_diag(const KParams P, const int* __restrict__ bt, double dx0,
+__global__ void __launch_bounds__(NT) amr_diag(const KParams* __restrict__ gp, const int* __restrict__ bt,
                                                const int* __restrict__ list, int n, const float4* __restrict__ u1,
                                                const float4* __restrict__ u2, double* __restrict__ part) {
   AccD acc[8];
@@ -688,7 +700,8 @@ __global__ void __launch_bounds__(NT) amr_diag(const KParams P, const int* __res
   double mach = 0.0;
   for (int i = blockIdx.x; i < n; i += gridDim.x) {
     const int slot = __ldg(list + i);
-    const double dx = dx0 / ldexp(1.0, bt_at(bt, slot, 0));
+    const KParams& P = gp[bt_at(bt, slot, GRID_WORD)];
+    const double dx = P.dx / ldexp(1.0, bt_at(bt, slot, 0));
     const double dv = DIM == 3 ? dx * dx * dx : dx * dx;
     for (int t = threadIdx.x; t < BG<DIM>::CB; t += NT) {
       const size_t o = (size_t)slot * BG<DIM>::CB + t;
@@ -772,40 +785,40 @@ int grid_for(int n, int per_sm) {
   }
 
 cudaError_t amr_launch_assemble(const AmrLaunch& L, const int* list, int n, const float4* u1, const float4* u2,
-                                unsigned* rate_out, cudaStream_t s) {
+                                unsigned* rates, int rslot, cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
   const int g = grid_for(n, 4);
   if (L.ndim == 3) {
-    SHZ_RECON_SWITCH(L.recon, false, (amrk::amr_assemble<3, R><<<g, amrk::NT, 0, s>>>(L.P, L.bt, L.nr, L.dx0, list, n, u1, u2, L.w1, L.w2, rate_out)))
+    SHZ_RECON_SWITCH(L.recon, false, (amrk::amr_assemble<3, R><<<g, amrk::NT, 0, s>>>(L.gp, L.bt, list, n, u1, u2, L.w1, L.w2, rates, rslot)))
   } else {
-    SHZ_RECON_SWITCH(L.recon, false, (amrk::amr_assemble<2, R><<<g, amrk::NT, 0, s>>>(L.P, L.bt, L.nr, L.dx0, list, n, u1, u2, L.w1, L.w2, rate_out)))
+    SHZ_RECON_SWITCH(L.recon, false, (amrk::amr_assemble<2, R><<<g, amrk::NT, 0, s>>>(L.gp, L.bt, list, n, u1, u2, L.w1, L.w2, rates, rslot)))
   }
   return cudaGetLastError();
 }
 
-cudaError_t amr_launch_predict(const AmrLaunch& L, const int* list, int n, const DevClock* clk, cudaStream_t s) {
+cudaError_t amr_launch_predict(const AmrLaunch& L, const int* list, int n, const DevClock* clks, cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
   const int g = grid_for(n, 4);
   if (L.ndim == 3) {
-    if (L.isen) { SHZ_RECON_SWITCH(L.recon, true, (amrk::amr_predict<3, R, true><<<g, amrk::NT, 0, s>>>(L.P, L.bt, L.dx0, list, n, L.w1, L.w2, L.p1, L.p2, clk))) }
-    else { SHZ_RECON_SWITCH(L.recon, false, (amrk::amr_predict<3, R, false><<<g, amrk::NT, 0, s>>>(L.P, L.bt, L.dx0, list, n, L.w1, L.w2, L.p1, L.p2, clk))) }
+    if (L.isen) { SHZ_RECON_SWITCH(L.recon, true, (amrk::amr_predict<3, R, true><<<g, amrk::NT, 0, s>>>(L.gp, L.bt, list, n, L.w1, L.w2, L.p1, L.p2, clks))) }
+    else { SHZ_RECON_SWITCH(L.recon, false, (amrk::amr_predict<3, R, false><<<g, amrk::NT, 0, s>>>(L.gp, L.bt, list, n, L.w1, L.w2, L.p1, L.p2, clks))) }
   } else {
-    if (L.isen) { SHZ_RECON_SWITCH(L.recon, true, (amrk::amr_predict<2, R, true><<<g, amrk::NT, 0, s>>>(L.P, L.bt, L.dx0, list, n, L.w1, L.w2, L.p1, L.p2, clk))) }
-    else { SHZ_RECON_SWITCH(L.recon, false, (amrk::amr_predict<2, R, false><<<g, amrk::NT, 0, s>>>(L.P, L.bt, L.dx0, list, n, L.w1, L.w2, L.p1, L.p2, clk))) }
+    if (L.isen) { SHZ_RECON_SWITCH(L.recon, true, (amrk::amr_predict<2, R, true><<<g, amrk::NT, 0, s>>>(L.gp, L.bt, list, n, L.w1, L.w2, L.p1, L.p2, clks))) }
+    else { SHZ_RECON_SWITCH(L.recon, false, (amrk::amr_predict<2, R, false><<<g, amrk::NT, 0, s>>>(L.gp, L.bt, list, n, L.w1, L.w2, L.p1, L.p2, clks))) }
   }
   return cudaGetLastError();
 }
 
 cudaError_t amr_launch_update(const AmrLaunch& L, const int* list, int n, const float4* u1, const float4* u2, float4* o1,
-                              float4* o2, const DevClock* clk, cudaStream_t s) {
+                              float4* o2, const DevClock* clks, cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
   const int g = grid_for(n, 4);
   if (L.ndim == 3) {
-    if (L.isen) { SHZ_RECON_SWITCH(L.recon, true, (amrk::amr_update<3, R, true><<<g, amrk::NT, 0, s>>>(L.P, L.bt, L.dx0, list, n, u1, u2, L.w1, L.w2, L.p1, L.p2, o1, o2, clk))) }
-    else { SHZ_RECON_SWITCH(L.recon, false, (amrk::amr_update<3, R, false><<<g, amrk::NT, 0, s>>>(L.P, L.bt, L.dx0, list, n, u1, u2, L.w1, L.w2, L.p1, L.p2, o1, o2, clk))) }
+    if (L.isen) { SHZ_RECON_SWITCH(L.recon, true, (amrk::amr_update<3, R, true><<<g, amrk::NT, 0, s>>>(L.gp, L.bt, list, n, u1, u2, L.w1, L.w2, L.p1, L.p2, o1, o2, clks))) }
+    else { SHZ_RECON_SWITCH(L.recon, false, (amrk::amr_update<3, R, false><<<g, amrk::NT, 0, s>>>(L.gp, L.bt, list, n, u1, u2, L.w1, L.w2, L.p1, L.p2, o1, o2, clks))) }
   } else {
-    if (L.isen) { SHZ_RECON_SWITCH(L.recon, true, (amrk::amr_update<2, R, true><<<g, amrk::NT, 0, s>>>(L.P, L.bt, L.dx0, list, n, u1, u2, L.w1, L.w2, L.p1, L.p2, o1, o2, clk))) }
-    else { SHZ_RECON_SWITCH(L.recon, false, (amrk::amr_update<2, R, false><<<g, amrk::NT, 0, s>>>(L.P, L.bt, L.dx0, list, n, u1, u2, L.w1, L.w2, L.p1, L.p2, o1, o2, clk))) }
+    if (L.isen) { SHZ_RECON_SWITCH(L.recon, true, (amrk::amr_update<2, R, true><<<g, amrk::NT, 0, s>>>(L.gp, L.bt, list, n, u1, u2, L.w1, L.w2, L.p1, L.p2, o1, o2, clks))) }
+    else { SHZ_RECON_SWITCH(L.recon, false, (amrk::amr_update<2, R, false><<<g, amrk::NT, 0, s>>>(L.gp, L.bt, list, n, u1, u2, L.w1, L.w2, L.p1, L.p2, o1, o2, clks))) }
   }
   return cudaGetLastError();
 }
@@ -823,10 +836,45 @@ cudaError_t amr_launch_regrid(const AmrLaunch& L, const int* rg, const int* list
   if (n <= 0) return cudaSuccess;
   const int g = grid_for(n, 4);
   if (L.ndim == 3) {
-    SHZ_RECON_SWITCH(L.recon, false, (amrk::amr_regrid<3, R><<<g, amrk::NT, 0, s>>>(L.P, rg, list, n, u1, u2, L.w1, L.w2, o1, o2)))
+    SHZ_RECON_SWITCH(L.recon, false, (amrk::amr_regrid<3, R><<<g, amrk::NT, 0, s>>>(L.gp, L.bt, rg, list, n, u1, u2, L.w1, L.w2, o1, o2)))
   } else {
-    SHZ_RECON_SWITCH(L.recon, false, (amrk::amr_regrid<2, R><<<g, amrk::NT, 0, s>>>(L.P, rg, list, n, u1, u2, L.w1, L.w2, o1, o2)))
+    SHZ_RECON_SWITCH(L.recon, false, (amrk::amr_regrid<2, R><<<g, amrk::NT, 0, s>>>(L.gp, L.bt, rg, list, n, u1, u2, L.w1, L.w2, o1, o2)))
   }
+  return cudaGetLastError();
+}
+
+// The clocks of many grids at once, one thread each: as clock_kernel (sweep.cu), reading grid
+// g's rate from rates[2 g + rslot] and clearing the other slot for the next step; a grid that
+// has taken max_steps steps holds.
+__global__ void clock_multi_kernel(DevClock* __restrict__ clks, unsigned* __restrict__ rates, int rslot, int ngrids) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ngrids) return;
+  DevClock& c = clks[g];
+  const float rate = __uint_as_float(rates[2 * g + rslot]);
+  rates[2 * g + (rslot ^ 1)] = 0u;
+  const double t = c.t;
+  double dt = c.cfl_dx / fmax((double)rate, 1e-30);
+  if (!(rate == rate) || isinf(rate)) c.bad = 1;
+  dt = fmin(dt, c.dt_max);
+  const double te = c.t_end;
+  if (te < HUGE_VAL) {
+    const double rem = te - t;
+    if (rem <= 1e-12 * fabs(te)) dt = 0.0;
+    else dt = fmin(dt, rem);
+  }
+  if (c.bad || c.steps >= c.max_steps) dt = 0.0;
+  c.dt = dt;
+  c.held = dt > 0.0 ? 0 : 1;
+  if (dt > 0.0) {
+    c.t = t + dt;
+    c.steps += 1;
+    c.last_dt = dt;
+  }
+}
+
+cudaError_t launch_clock_multi(DevClock* clks, unsigned* rates, int rslot, int ngrids, cudaStream_t s) {
+  if (ngrids <= 0) return cudaSuccess;
+  clock_multi_kernel<<<(ngrids + 127) / 128, 128, 0, s>>>(clks, rates, rslot, ngrids);
   return cudaGetLastError();
 }
 
@@ -835,8 +883,8 @@ int amr_diag_blocks(int n) { return grid_for(n, 2); }
 cudaError_t amr_launch_diag(const AmrLaunch& L, const int* list, int n, const float4* u1, const float4* u2, double* part,
                             double* out, cudaStream_t s) {
   const int g = amr_diag_blocks(n);
-  if (L.ndim == 3) amrk::amr_diag<3><<<g, amrk::NT, 0, s>>>(L.P, L.bt, L.dx0, list, n, u1, u2, part);
-  else amrk::amr_diag<2><<<g, amrk::NT, 0, s>>>(L.P, L.bt, L.dx0, list, n, u1, u2, part);
+  if (L.ndim == 3) amrk::amr_diag<3><<<g, amrk::NT, 0, s>>>(L.gp, L.bt, list, n, u1, u2, part);
+  else amrk::amr_diag<2><<<g, amrk::NT, 0, s>>>(L.gp, L.bt, list, n, u1, u2, part);
   amrk::amr_diag_final<<<1, 32, 0, s>>>(part, g, out);
   return cudaGetLastError();
 }

@@ -6,14 +6,14 @@
 
 namespace shz {
 
-// What every pass needs: hydro parameters, the block table and the two derived atlases.
+// What every pass needs: the scheme, the per-grid parameters and clocks, the block table and
+// the two derived atlases. Word 26 of a block's table row names its grid; a grid's KParams hold
+// its level-0 cell size in dx and its root blocks per side in n[0].
 struct AmrLaunch {
-  KParams P;
   int ndim;
   int recon;
   bool isen;
-  int nr;       // root blocks per side
-  double dx0;   // cell size at level 0
+  const KParams* gp;   // device, per grid
   const int* bt;
   float4* w1;   // primitives with ghosts, 20^ndim texels per slot
   float4* w2;
@@ -21,11 +21,14 @@ struct AmrLaunch {
   float4* p2;
 };
 
+// rates: two 32-bit maxima per grid; the assemble folds the leaves' rate / dx into slot rslot.
 cudaError_t amr_launch_assemble(const AmrLaunch& L, const int* list, int n, const float4* u1, const float4* u2,
-                                unsigned* rate_out, cudaStream_t s);
-cudaError_t amr_launch_predict(const AmrLaunch& L, const int* list, int n, const DevClock* clk, cudaStream_t s);
+                                unsigned* rates, int rslot, cudaStream_t s);
+// The clocks of `ngrids` grids at once (one thread each): dt from each grid's rate slot.
+cudaError_t launch_clock_multi(DevClock* clks, unsigned* rates, int rslot, int ngrids, cudaStream_t s);
+cudaError_t amr_launch_predict(const AmrLaunch& L, const int* list, int n, const DevClock* clks, cudaStream_t s);
 cudaError_t amr_launch_update(const AmrLaunch& L, const int* list, int n, const float4* u1, const float4* u2, float4* o1,
-                              float4* o2, const DevClock* clk, cudaStream_t s);
+                              float4* o2, const DevClock* clks, cudaStream_t s);
 cudaError_t amr_launch_flag(const AmrLaunch& L, const int* list, int n, float* flags, cudaStream_t s);
 cudaError_t amr_launch_regrid(const AmrLaunch& L, const int* rg, const int* list, int n, const float4* u1,
                               const float4* u2, float4* o1, float4* o2, cudaStream_t s);

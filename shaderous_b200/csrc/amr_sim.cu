@@ -34,9 +34,10 @@ struct shz_amr {
   float4* u2[2] = {nullptr, nullptr};
   float4 *w1 = nullptr, *w2 = nullptr, *p1 = nullptr, *p2 = nullptr;
   int *d_bt = nullptr, *d_all = nullptr, *d_leaves = nullptr, *d_rg = nullptr;
+  shz::KParams* d_gp = nullptr;  // this run's parameters: grid 0 of the passes' per-grid table
   float* d_flags = nullptr;
   shz::DevClock* clk = nullptr;
-  unsigned* rates = nullptr;  // slots 0, 1: the steps'; 2: the refinement check's
+  unsigned* rates = nullptr;  // slots 0, 1: the steps'; 2, 3: the refinement check's
   double *diag_part = nullptr, *diag_out = nullptr;
   int* d_ghost = nullptr;
   std::vector<int32_t> h_bt, h_all, h_leaves, h_rg;
@@ -96,6 +97,7 @@ int upload_tables(shz_amr* a) {
   const int cap = a->cfg.cap;
   a->h_bt.resize((size_t)cap * shz::amr::BT_STRIDE);
   a->tree->table(a->h_bt.data());
+  for (int s = 0; s < cap; s++) a->h_bt[(size_t)s * shz::amr::BT_STRIDE + 26] = 0;  // every block is grid 0's
   std::vector<int32_t> per;
   a->tree->lists(a->h_all, a->h_leaves, per);
   AMR_CUDA(a, cudaMemcpyAsync(a->d_bt, a->h_bt.data(), a->h_bt.size() * sizeof(int32_t), cudaMemcpyHostToDevice, a->stream));
@@ -115,8 +117,9 @@ int write_clock(shz_amr* a, double t, long long steps) {
   h.dt_max = a->cfg.hydro.dt_max;
   h.cfl_dx = a->cfg.hydro.cfl;  // the rates are per unit of each block's own cell size
   h.steps = steps;
+  h.max_steps = std::numeric_limits<long long>::max();
   AMR_CUDA(a, cudaMemcpyAsync(a->clk, &h, sizeof h, cudaMemcpyHostToDevice, a->stream));
-  AMR_CUDA(a, cudaMemsetAsync(a->rates, 0, 3 * sizeof(unsigned), a->stream));
+  AMR_CUDA(a, cudaMemsetAsync(a->rates, 0, 4 * sizeof(unsigned), a->stream));
   AMR_CUDA(a, cudaStreamSynchronize(a->stream));
   return 0;
 }
@@ -132,8 +135,8 @@ int n_leaves(const shz_amr* a) { return (int)a->h_leaves.size(); }
 
 // One step's four kernels, enqueued.
 int enqueue_step(shz_amr* a) {
-  AMR_CUDA(a, shz::amr_launch_assemble(a->L, a->d_all, n_all(a), a->u1[a->cur], a->u2[a->cur], a->rates + a->slot, a->stream));
-  AMR_CUDA(a, shz::launch_clock(a->clk, a->rates, a->slot, a->stream));
+  AMR_CUDA(a, shz::amr_launch_assemble(a->L, a->d_all, n_all(a), a->u1[a->cur], a->u2[a->cur], a->rates, a->slot, a->stream));
+  AMR_CUDA(a, shz::launch_clock_multi(a->clk, a->rates, a->slot, 1, a->stream));
   AMR_CUDA(a, shz::amr_launch_predict(a->L, a->d_leaves, n_leaves(a), a->clk, a->stream));
   AMR_CUDA(a, shz::amr_launch_update(a->L, a->d_leaves, n_leaves(a), a->u1[a->cur], a->u2[a->cur], a->u1[1 - a->cur],
                                      a->u2[1 - a->cur], a->clk, a->stream));
@@ -164,8 +167,8 @@ int step_once(shz_amr* a) {
 
 // The refinement indicators of the current state: a fresh assemble, then the Löhner pass.
 int compute_flags(shz_amr* a) {
-  AMR_CUDA(a, cudaMemsetAsync(a->rates + 2, 0, sizeof(unsigned), a->stream));
-  AMR_CUDA(a, shz::amr_launch_assemble(a->L, a->d_all, n_all(a), a->u1[a->cur], a->u2[a->cur], a->rates + 2, a->stream));
+  AMR_CUDA(a, cudaMemsetAsync(a->rates + 2, 0, 2 * sizeof(unsigned), a->stream));
+  AMR_CUDA(a, shz::amr_launch_assemble(a->L, a->d_all, n_all(a), a->u1[a->cur], a->u2[a->cur], a->rates + 2, 0, a->stream));
   AMR_CUDA(a, cudaMemsetAsync(a->d_flags, 0, sizeof(float) * a->cfg.cap, a->stream));
   AMR_CUDA(a, shz::amr_launch_flag(a->L, a->d_leaves, n_leaves(a), a->d_flags, a->stream));
   a->launches += 2;
@@ -331,9 +334,10 @@ int shz_amr_create(const shz_amr_config* cfg, shz_amr** out) {
   a->CB = c.ndim == 3 ? 4096 : 256;
   a->WN = c.ndim == 3 ? 8000 : 400;
   a->PN = c.ndim == 3 ? 5832 : 324;
-  shz::KParams& P = a->L.P;
+  shz::KParams P;
   std::memset(&P, 0, sizeof P);
   P.dx = dx0_of(c);
+  P.n[0] = c.nr;
   P.gamma = (float)c.hydro.gamma;
   P.gm1 = (float)(c.hydro.gamma - 1);
   P.inv_gm1 = (float)(1.0 / (c.hydro.gamma - 1));
@@ -348,8 +352,6 @@ int shz_amr_create(const shz_amr_config* cfg, shz_amr** out) {
   a->L.ndim = c.ndim;
   a->L.recon = c.hydro.recon;
   a->L.isen = c.hydro.isentropic != 0;
-  a->L.nr = c.nr;
-  a->L.dx0 = dx0_of(c);
   auto bail = [&](int code, const char* what) {
     g_create_err = what;
     shz_amr_destroy(a);
@@ -372,7 +374,8 @@ int shz_amr_create(const shz_amr_config* cfg, shz_amr** out) {
   ok = ok && cudaMalloc(&a->d_rg, cap * shz::amr::RG_STRIDE * sizeof(int)) == cudaSuccess;
   ok = ok && cudaMalloc(&a->d_flags, cap * sizeof(float)) == cudaSuccess;
   ok = ok && cudaMalloc(&a->clk, sizeof(shz::DevClock)) == cudaSuccess;
-  ok = ok && cudaMalloc(&a->rates, 3 * sizeof(unsigned)) == cudaSuccess;
+  ok = ok && cudaMalloc(&a->rates, 4 * sizeof(unsigned)) == cudaSuccess;
+  ok = ok && cudaMalloc(&a->d_gp, sizeof(shz::KParams)) == cudaSuccess;
   ok = ok && cudaMalloc(&a->diag_part, (size_t)shz::amr_diag_blocks(c.cap) * 9 * sizeof(double)) == cudaSuccess;
   ok = ok && cudaMalloc(&a->diag_out, 9 * sizeof(double)) == cudaSuccess;
   ok = ok && cudaMalloc(&a->d_ghost, (size_t)a->WN * 5 * sizeof(int)) == cudaSuccess;
@@ -384,6 +387,8 @@ int shz_amr_create(const shz_amr_config* cfg, shz_amr** out) {
     return bail(SHZ_E_OOM, buf);
   }
   a->L.bt = a->d_bt;
+  a->L.gp = a->d_gp;
+  if (cudaMemcpy(a->d_gp, &P, sizeof P, cudaMemcpyHostToDevice) != cudaSuccess) return bail(SHZ_E_CUDA, "parameters upload");
   a->L.w1 = a->w1;
   a->L.w2 = a->w2;
   a->L.p1 = a->p1;
@@ -408,7 +413,7 @@ void shz_amr_destroy(shz_amr* a) {
     cudaFree(a->u1[p]);
     cudaFree(a->u2[p]);
   }
-  void* bufs[] = {a->w1, a->w2, a->p1, a->p2, a->d_bt, a->d_all, a->d_leaves, a->d_rg, a->d_flags,
+  void* bufs[] = {a->w1, a->w2, a->p1, a->p2, a->d_bt, a->d_all, a->d_leaves, a->d_rg, a->d_flags, a->d_gp,
                   a->clk, a->rates, a->diag_part, a->diag_out, a->d_ghost};
   for (void* b : bufs)
     if (b) cudaFree(b);

@@ -31,6 +31,7 @@ struct DevClock {
   double cfl_dx;
   double last_dt;
   long long steps;
+  long long max_steps;  // the clock holds once this many steps are taken (a batched request's length)
   int held;
   int bad;
 };

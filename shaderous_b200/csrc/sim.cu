@@ -140,6 +140,7 @@ int write_clock(shz_sim* s, double t, long long steps) {
   h.cfl_dx = s->cfg.cfl * s->cfg.dx;
   h.last_dt = 0;
   h.steps = steps;
+  h.max_steps = std::numeric_limits<long long>::max();
   h.held = 0;
   h.bad = 0;
   CUDA_OR_FAIL(s, cudaMemcpyAsync(s->clk, &h, sizeof h, cudaMemcpyHostToDevice, s->stream));
