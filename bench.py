@@ -57,6 +57,9 @@ def parse():
     ap.add_argument("--no-amr", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--serve-requests", type=int, default=200)
+    ap.add_argument("--section", choices=["all", "amr", "serving"], default="all",
+                    help="amr / serving: only that measurement, printed as its own JSON line")
+    ap.add_argument("--amr-variant", choices=["both", "spec", "developed"], default="both")
     return ap.parse_args()
 
 
@@ -268,6 +271,17 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.section != "all":
+        out = {}
+        if args.section == "amr":
+            if args.amr_variant in ("both", "spec"):
+                out["spec"] = amr_sedov(steps=max(args.steps, 8))
+            if args.amr_variant in ("both", "developed"):
+                out["developed"] = amr_sedov(steps=max(args.steps, 8), grown=True)
+        else:
+            out = serving(args.serve_requests)
+        print(json.dumps({"section": args.section, "result": out}), flush=True)
         return
 
     import torch
