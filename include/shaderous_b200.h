@@ -251,6 +251,10 @@ typedef struct shz_amr_config {
   double refine_hi;     /* refine leaves whose indicator exceeds this */
   double refine_lo;     /* merge siblings whose indicators are all below this */
   int32_t regrid_every; /* steps between refinement checks (0: never) */
+  int32_t two_pass;     /* 0: one fused sweep per leaf (predict, fluxes and update from the
+                           primitives); 1: the reference's two passes, predict into a half-step
+                           atlas then update (amr_sim.ts:2709-2946), which costs that atlas's
+                           memory; both give the same state to rounding */
 } shz_amr_config;
 typedef struct shz_amr shz_amr;
 

@@ -96,6 +96,7 @@ class shz_amr_config(C.Structure):
         ("refine_hi", C.c_double),
         ("refine_lo", C.c_double),
         ("regrid_every", C.c_int32),
+        ("two_pass", C.c_int32),
     ]
 
 

@@ -27,12 +27,14 @@ class AmrConfig:
     refine_hi: float = 0.1
     refine_lo: float = 0.05
     regrid_every: int = 8
+    two_pass: bool = False  # predict into a half-step atlas, then update (the reference's passes)
 
     def to_c(self) -> _abi.shz_amr_config:
         c = _abi.shz_amr_config()
         c.hydro = self.hydro.to_c()
         c.ndim, c.nr, c.max_level, c.cap = self.ndim, self.nr, self.max_level, self.cap
         c.box, c.refine_hi, c.refine_lo, c.regrid_every = self.box, self.refine_hi, self.refine_lo, self.regrid_every
+        c.two_pass = 1 if self.two_pass else 0
         return c
 
     @property

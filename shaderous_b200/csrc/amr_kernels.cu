@@ -5,11 +5,13 @@
 //   - the primitives with two ghost layers: 20^ndim cells x (w1 = rho, v; w2 = p, s, cs, 0);
 //   - the half-step states over the block and one ghost layer: 18^ndim cells x
 //     (p1 = rho, v; p2 = p, s, shock flag, first-order flag).
-// One step is four kernels, captured in a CUDA graph by the host:
+// One step is three kernels, captured in a CUDA graph by the host:
 //   1. amr_assemble over every block (leaves and parents): primitives with ghost fill.
-//   2. clock_kernel: dt.
-//   3. amr_predict over the leaves: half steps.
-//   4. amr_update over the leaves: fluxes, fine-flux matching and the update.
+//   2. clock_multi_kernel: dt.
+//   3. amr_sweep over the leaves: half steps, fluxes, fine-flux matching and the update, in one
+//      pass over the primitives.
+// The reference's own pass structure is kept beside it as a cross-check (two_pass): amr_predict
+// writes the half steps to their atlas and amr_update reads them.
 // This follows the reference's AmrSim.encodeSteps (src/amr/amr_sim.ts:2709-2946), and its rules
 // for the ghost fill (amr/grid.wgsl:186-222 ghost_src; amr/cons.wgsl:19-125 restriction and
 // prolongation; amr/assemble.wgsl:47-75 from_coarse), the predictor at the source
@@ -61,6 +63,7 @@ __device__ __forceinline__ int ptex(const int* l) {
 // level coarser (slot = that coarser leaf), kind 2 an edge or corner ghost.
 struct Src {
   int kind, slot;
+  int from;  // the block in whose frame l is given (kind 1: the fine block beside the coarse leaf)
   int l[3];
   float flip[3];
 };
@@ -70,6 +73,7 @@ __device__ __forceinline__ Src ghost_src(const int* __restrict__ bt, int slot, c
   Src s;
   s.kind = 0;
   s.slot = slot;
+  s.from = slot;
   s.l[0] = l[0]; s.l[1] = l[1]; s.l[2] = l[2];
   s.flip[0] = s.flip[1] = s.flip[2] = 1.f;
   int out = 0, axis = 0;
@@ -100,22 +104,52 @@ __device__ __forceinline__ Src ghost_src(const int* __restrict__ bt, int slot, c
   return s;
 }
 
-// An edge or corner ghost takes the value of the face ghost beside it: the cell clamped into the
-// block along every out-of-range axis but the first. (Nothing in the scheme reads these except
-// the shock flag of a rim ghost next to a coarser block.)
+// An edge or corner ghost, resolved one axis at a time: across the first out-of-range axis to
+// the same-level neighbour (or the boundary image), then the rest in that block's own frame, so
+// that it holds the value that the neighbour's own ghost there holds. That is what the
+// reference's predictor sees when it predicts a face ghost at its source (amr/predict.wgsl:184),
+// and hops in either order reach the same cell. Where a hop meets a coarser block before the last
+// axis, the remaining axes are clamped into the block (the face ghost beside it): such a ghost is
+// predicted in place with those axes' slopes masked. (The reference leaves edge ghosts unwritten,
+// amr/assemble.wgsl:86; its masked rim ghosts then read whatever the texture held.)
 template <int DIM>
 __device__ __forceinline__ Src ghost_src_any(const int* __restrict__ bt, int slot, const int* l) {
-  Src s = ghost_src<DIM>(bt, slot, l);
-  if (s.kind != 2) return s;
+  int cur = slot;
   int m[3] = {l[0], l[1], l[2]};
-  bool first = true;
+  float flip[3] = {1.f, 1.f, 1.f};
 #pragma unroll
-  for (int a = 0; a < DIM; a++)
-    if (m[a] < 0 || m[a] >= BS) {
-      if (first) first = false;
-      else m[a] = min(max(m[a], 0), BS - 1);
+  for (int hop = 0; hop < DIM; hop++) {
+    int out = 0, axis = -1;
+#pragma unroll
+    for (int a = 0; a < DIM; a++)
+      if (m[a] < 0 || m[a] >= BS) {
+        out++;
+        if (axis < 0) axis = a;
+      }
+    if (out <= 1) break;
+    const int upper = m[axis] >= BS ? 1 : 0;
+    const int nb = bt_at(bt, cur, 6 + 2 * axis + upper);
+    if (nb >= 0) {
+      cur = nb;
+      m[axis] += upper ? -BS : BS;
+    } else if (nb <= -2) {
+      if (-1 - nb == 2) {
+        m[axis] = upper ? 2 * BS - 1 - m[axis] : -1 - m[axis];
+        flip[axis] = -flip[axis];
+      } else {
+        m[axis] = upper ? BS - 1 : 0;
+      }
+    } else {
+      // a coarser block across this axis: the face ghost beside the texel
+#pragma unroll
+      for (int a = 0; a < DIM; a++)
+        if (a != axis) m[a] = min(max(m[a], 0), BS - 1);
     }
-  return ghost_src<DIM>(bt, slot, m);
+  }
+  Src s = ghost_src<DIM>(bt, cur, m);
+#pragma unroll
+  for (int a = 0; a < 3; a++) s.flip[a] *= flip[a];
+  return s;
 }
 
 struct Cons {
@@ -306,7 +340,10 @@ __global__ void __launch_bounds__(NT) amr_assemble(const KParams* __restrict__ g
         u.a.z *= s.flip[1];
         u.a.w *= s.flip[2];
       } else {
-        u = from_coarse<DIM, R>(bt, u1, u2, nr, slot, s.l, s.slot, P.rho_floor);
+        u = from_coarse<DIM, R>(bt, u1, u2, nr, s.from, s.l, s.slot, P.rho_floor);
+        u.a.y *= s.flip[0];
+        u.a.z *= s.flip[1];
+        u.a.w *= s.flip[2];
       }
       float w[7];
       prim_from_cons(u.a, u.b, P, 1.f, 1.f, 1.f, w);
@@ -763,6 +800,468 @@ __global__ void amr_ghost_map(const int* __restrict__ bt, int slot, int* __restr
   }
 }
 
+// ---------------------------------------------------------------------------------------------
+// The fused block sweep: predict, fluxes and update of a leaf in one pass over its primitive
+// atlas (which assemble filled, ghosts and edges included), so that each edge increment is formed
+// once and no half-step atlas is written. A CTA takes a block as the uniform sweep (sweep.cu)
+// takes a column: its (16 + 2)^2 threads march the 16 planes along z; the primitives of three
+// planes sit in shared memory.
+//
+// Ghosts, by the block-table entry of their face:
+//   same level (a slot): predicted in place: the atlas holds the neighbour's cells and, across
+//     edges, what the neighbour's own ghosts hold, so this is the prediction at the source
+//     (amr/predict.wgsl:196-206);
+//   one level coarser (NB_COARSE): predicted in place, the slopes along the face's transverse
+//     axes dropped at the rim of the face (amr/predict.wgsl:207-214);
+//   a domain boundary: the half-step state of the cell it maps to, mirrored for a wall, with edge
+//     increments at the ghost position (hydro.ts:329-358, as amr/predict.wgsl's at-source rule).
+// A face whose same-level neighbour is refined takes the mean of the fine fluxes through it
+// (amr/update.wgsl:207-295), the fine cells predicted from the fine leaf's atlas by predict_texel.
+
+constexpr int SX = BS + 2;        // threads per row: the block and one ghost on each side
+constexpr int SNT = SX * SX;      // 324 threads
+constexpr int SPN = SX * SX;      // predictor region per plane
+constexpr int SWN = PAD * PAD;    // primitive texels per plane
+
+__device__ __forceinline__ void read_w6(const float* __restrict__ plane, int x, int y, float* w) {
+#pragma unroll
+  for (int c = 0; c < 6; c++) w[c] = plane[c * SWN + (y + NG) * PAD + (x + NG)];
+}
+
+template <int DIM>
+__device__ __forceinline__ void load_w6(const float4* __restrict__ w1, const float4* __restrict__ w2, int slot, const int* l,
+                                        float* w) {
+  const size_t o = (size_t)slot * BG<DIM>::WN + wtex<DIM>(l);
+  const float4 a = __ldg(w1 + o), b = __ldg(w2 + o);
+  w[0] = a.x; w[1] = a.y; w[2] = a.z; w[3] = a.w;
+  w[4] = b.x; w[5] = b.y;
+}
+
+// The predictor of texel l0 of block `slot`, read from its primitive atlas, under the ghost rules
+// above; with the edge increments along `axis` at l0 itself (for its face states on that axis).
+template <int DIM, int R, bool ISEN>
+__device__ __forceinline__ void predict_texel(const KParams& P, const int* __restrict__ bt, const float4* __restrict__ w1,
+                                              const float4* __restrict__ w2, int slot, const int* l0, float h, int axis,
+                                              Pred& pr, float* su, float* sd) {
+  int l[3] = {l0[0], l0[1], l0[2]};
+  float flip[3] = {1.f, 1.f, 1.f}, mask[3] = {1.f, 1.f, 1.f};
+  int out = 0, oa = 0;
+#pragma unroll
+  for (int a = 0; a < DIM; a++)
+    if (l[a] < 0 || l[a] >= BS) { out++; oa = a; }
+  bool moved = false;
+  if (out == 1) {
+    const int upper = l[oa] >= BS ? 1 : 0;
+    const int nb = bt_at(bt, slot, 6 + 2 * oa + upper);
+    if (nb == -1) {
+#pragma unroll
+      for (int a = 0; a < DIM; a++)
+        if (a != oa) mask[a] = (l[a] == 0 || l[a] == BS - 1) ? 0.f : 1.f;
+    } else if (nb <= -2) {
+      if (-1 - nb == 2) {
+        l[oa] = upper ? 2 * BS - 1 - l[oa] : -1 - l[oa];
+        flip[oa] = -1.f;
+      } else {
+        l[oa] = upper ? BS - 1 : 0;
+      }
+      moved = true;
+    }
+  }
+  float c[7], sua[DIM][6], sda[DIM][6];
+  float conv = 0.f, jump = 0.f;
+  load_w6<DIM>(w1, w2, slot, l, c);
+  with_cs(c, P);
+#pragma unroll
+  for (int a = 0; a < DIM; a++) {
+    float m[7], p[7];
+    int lm[3] = {l[0], l[1], l[2]}, lp[3] = {l[0], l[1], l[2]};
+    lm[a] -= 1;
+    lp[a] += 1;
+    load_w6<DIM>(w1, w2, slot, lm, m);
+    load_w6<DIM>(w1, w2, slot, lp, p);
+    axis_edges<R, ISEN>(m, m, c, p, p, P.inv_gamma, sua[a], sda[a]);
+    conv += p[1 + a] - m[1 + a];
+    jump = fmaxf(jump, fabsf(p[4] - m[4]) / fminf(p[4], m[4]));
+  }
+  hancock_masked<DIM>(c, conv, jump, sua, sda, mask, h, P, pr);
+  pr.q[1] *= flip[0];
+  pr.q[2] *= flip[1];
+  pr.q[3] *= flip[2];
+  if (moved) {
+    float g[7], m[7], p[7];
+    int lm[3] = {l0[0], l0[1], l0[2]}, lp[3] = {l0[0], l0[1], l0[2]};
+    lm[axis] -= 1;
+    lp[axis] += 1;
+    load_w6<DIM>(w1, w2, slot, l0, g);
+    with_cs(g, P);
+    load_w6<DIM>(w1, w2, slot, lm, m);
+    load_w6<DIM>(w1, w2, slot, lp, p);
+    axis_edges<R, ISEN>(m, m, g, p, p, P.inv_gamma, su, sd);
+  } else {
+#pragma unroll
+    for (int v = 0; v < 6; v++) {
+      su[v] = sua[axis][v];
+      sd[v] = sda[axis][v];
+    }
+  }
+}
+
+// The mean of the fine fluxes through the face of cell l on side `hi` of axis AXIS, whose
+// same-level neighbour np is refined: computed from the fine leaf's own atlas as the fine leaf's
+// sweep computes them. (Out of line: it runs at a few faces of a few blocks, and inlined it
+// would crowd the registers of the march.)
+struct Flux8 {
+  float v[8];
+};
+template <int DIM, int R, bool ISEN, int AXIS>
+__device__ __noinline__ Flux8 fine_mean_flux(const KParams* __restrict__ Pp, const int* __restrict__ bt,
+                                             const float4* __restrict__ w1, const float4* __restrict__ w2, int np, int l0,
+                                             int l1, int l2, bool hi, float hf) {
+  const KParams& P = *Pp;
+  Flux8 out;
+#pragma unroll
+  for (int v = 0; v < 8; v++) out.v[v] = 0.f;
+  const int l[3] = {l0, l1, l2};
+  const bool upper = !hi;
+  int hb[3] = {l[0] >= BS / 2, l[1] >= BS / 2, DIM == 3 ? (l[2] >= BS / 2) : 0};
+  int bits[3] = {hb[0], hb[1], hb[2]};
+  bits[AXIS] = upper ? 1 : 0;
+  if (DIM == 2) bits[2] = 0;
+  const int ch = bt_at(bt, np, 12 + (bits[0] | (bits[1] << 1) | (bits[2] << 2)));
+  if (ch < 0) return out;
+  int a0[3] = {2 * (l[0] - (BS / 2) * hb[0]), 2 * (l[1] - (BS / 2) * hb[1]), DIM == 3 ? 2 * (l[2] - (BS / 2) * hb[2]) : 0};
+  a0[AXIS] = upper ? BS - 1 : -1;
+  constexpr int T1 = (AXIS + 1) % 3, T2 = (AXIS + 2) % 3;
+  const int n1 = (DIM == 2 && T1 == 2) ? 1 : 2;
+  const int n2 = (DIM == 2 && T2 == 2) ? 1 : 2;
+  for (int j = 0; j < n2; j++)
+    for (int i = 0; i < n1; i++) {
+      int a[3] = {a0[0], a0[1], a0[2]};
+      a[T1] += i;
+      a[T2] += j;
+      int b[3] = {a[0], a[1], a[2]};
+      b[AXIS] += 1;
+      Pred pa, pb;
+      float sua[6], sda[6], sub[6], sdb[6];
+      predict_texel<DIM, R, ISEN>(P, bt, w1, w2, ch, a, hf, AXIS, pa, sua, sda);
+      predict_texel<DIM, R, ISEN>(P, bt, w1, w2, ch, b, hf, AXIS, pb, sub, sdb);
+      float L[7], Rr[7], f[8];
+      face_state(pa, sua, 1.f, L);
+      face_state(pb, sdb, -1.f, Rr);
+      riemann<AXIS>(L, Rr, P, f);
+#pragma unroll
+      for (int v = 0; v < 8; v++) out.v[v] += f[v];
+    }
+  const float w = 1.f / (float)(n1 * n2);
+#pragma unroll
+  for (int v = 0; v < 8; v++) out.v[v] *= w;
+  return out;
+}
+
+// Shared memory of the block sweep, in floats.
+constexpr int SW_RING = 3 * 6 * SWN;  // three planes of primitives
+constexpr int SW_FACE = 2 * 7 * SPN;  // x and y upper face states of a plane
+constexpr int SW_FLUX = 2 * 8 * SPN;  // x and y lower-face fluxes of a plane (also the half-step exchange)
+constexpr int SW_KEEP = 8 * SPN;      // z boundary ghosts: a plane's half steps or the ghost's increments
+constexpr size_t SWEEP_SMEM = (size_t)(SW_RING + SW_FACE + SW_FLUX + SW_KEEP) * sizeof(float);
+
+template <int DIM, int R, bool ISEN>
+__global__ void __maxnreg__(80)
+    amr_sweep(const KParams* __restrict__ gp, const int* __restrict__ bt, const int* __restrict__ list, int n,
+              const float4* __restrict__ u1, const float4* __restrict__ u2, const float4* __restrict__ w1,
+              const float4* __restrict__ w2, float4* __restrict__ o1, float4* __restrict__ o2,
+              const DevClock* __restrict__ clks) {
+  extern __shared__ __align__(16) float smem[];
+  float* sW = smem;
+  float* sFace = sW + SW_RING;
+  float* sFlux = sFace + SW_FACE;
+  float* sKeep = sFlux + SW_FLUX;
+  __shared__ int sNb[6];
+  const int tid = threadIdx.x;
+  const int tx = tid % SX, ty = tid / SX;
+  const int lx = tx - 1, ly = DIM >= 2 ? ty - 1 : 0;
+  const bool row_t = ty >= 1 && ty <= BS;
+  const bool col_t = tx >= 1 && tx <= BS;
+  const bool tile_t = row_t && col_t;
+  auto ring = [&](int plane) -> float* { return sW + ((plane + 6) % 3) * 6 * SWN; };
+
+  for (int i = blockIdx.x; i < n; i += gridDim.x) {
+    const int slot = __ldg(list + i);
+    const int g = bt_at(bt, slot, GRID_WORD);
+    const KParams* Pp = gp + g;
+    const KParams& P = *Pp;
+    const double dt = clks[g].dt;
+    const double dxl = P.dx / ldexp(1.0, bt_at(bt, slot, 0));
+    const float dtdx = (float)(dt / dxl);
+    const float h = (float)((0.5 * dt) / dxl);
+    const size_t base = (size_t)slot * BG<DIM>::CB;
+    if (clks[g].held) {
+      for (int t = tid; t < BG<DIM>::CB; t += SNT) {
+        o1[base + t] = __ldg(u1 + base + t);
+        o2[base + t] = __ldg(u2 + base + t);
+      }
+      continue;
+    }
+    __syncthreads();  // the previous block's last reads of shared memory
+    if (tid < 6) sNb[tid] = bt_at(bt, slot, 6 + tid);
+    // This thread's ghost role across x or y: the face and, for a domain boundary, the thread
+    // holding the inner cell that the ghost maps to (mirror or edge cell: both the adjacent one).
+    int gface = -1;
+    if (tx == 0 && row_t) gface = 0;
+    if (tx == SX - 1 && row_t) gface = 1;
+    if (DIM >= 2 && ty == 0 && col_t) gface = 2;
+    if (DIM >= 2 && ty == SX - 1 && col_t) gface = 3;
+    const int gnb = gface >= 0 ? bt_at(bt, slot, 6 + gface) : 0;
+    const bool g_coarse = gface >= 0 && gnb == -1;
+    const bool g_bc = gface >= 0 && gnb <= -2;
+    const int g_src = !g_bc ? -1 : (gface == 0 ? tid + 1 : gface == 1 ? tid - 1 : gface == 2 ? tid + SX : tid - SX);
+    const bool g_flip = g_bc && (-1 - gnb) == 2;
+    const int g_axis = gface >> 1;
+    bool xyg = false;
+#pragma unroll
+    for (int f = 0; f < 4; f++) xyg = xyg || bt_at(bt, slot, 6 + f) <= -2;
+    // the faces' fine-flux matching (a same-level neighbour that is refined)
+    unsigned fine = 0;
+#pragma unroll
+    for (int f = 0; f < 2 * DIM; f++) {
+      const int nb = bt_at(bt, slot, 6 + f);
+      if (nb >= 0 && !leaf_of(bt, nb)) fine |= 1u << f;
+    }
+    const int zlo_nb = DIM == 3 ? bt_at(bt, slot, 10) : 0, zhi_nb = DIM == 3 ? bt_at(bt, slot, 11) : 0;
+
+    float zhi_prev[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    float ph_prev = 0.f;
+
+    auto load_plane = [&](int pl) {
+      float* dst = ring(pl);
+      const size_t zb = (size_t)slot * BG<DIM>::WN + (DIM == 3 ? (size_t)(pl + NG) * SWN : 0);
+      for (int t = tid; t < SWN; t += SNT) {
+        const float4 a = __ldg(w1 + zb + t), b = __ldg(w2 + zb + t);
+        dst[0 * SWN + t] = a.x;
+        dst[1 * SWN + t] = a.y;
+        dst[2 * SWN + t] = a.z;
+        dst[3 * SWN + t] = a.w;
+        dst[4 * SWN + t] = b.x;
+        dst[5 * SWN + t] = b.y;
+      }
+    };
+    if constexpr (DIM == 3) {
+      load_plane(-2);
+      load_plane(-1);
+    }
+    // 3D: planes -1 .. 16, the first and last the z ghosts; 2D: the one plane.
+    const int jb = DIM == 3 ? -1 : 0, je = DIM == 3 ? BS : 0;
+    for (int j = jb; j <= je; j++) {
+      load_plane(DIM == 3 ? j + 1 : 0);
+      __syncthreads();
+      const float* pj = ring(DIM == 3 ? j : 0);
+      const bool zghost = DIM == 3 && (j == -1 || j == BS);
+      const int znb = j == -1 ? zlo_nb : zhi_nb;  // (meaningful on the z ghost planes)
+
+      // the predictor at plane j
+      float c[7];
+      read_w6(pj, lx, ly, c);
+      with_cs(c, P);
+      float su[DIM][6], sd[DIM][6];
+      float conv = 0.f, jump = 0.f;
+      {
+        float m[7], p[7];
+        read_w6(pj, lx - 1, ly, m);
+        read_w6(pj, lx + 1, ly, p);
+        axis_edges<R, ISEN>(m, m, c, p, p, P.inv_gamma, su[0], sd[0]);
+        conv += p[1] - m[1];
+        jump = fmaxf(jump, fabsf(p[4] - m[4]) / fminf(p[4], m[4]));
+        if constexpr (DIM >= 2) {
+          read_w6(pj, lx, ly - 1, m);
+          read_w6(pj, lx, ly + 1, p);
+          axis_edges<R, ISEN>(m, m, c, p, p, P.inv_gamma, su[1], sd[1]);
+          conv += p[2] - m[2];
+          jump = fmaxf(jump, fabsf(p[4] - m[4]) / fminf(p[4], m[4]));
+        }
+        if constexpr (DIM == 3) {
+          read_w6(ring(j - 1), lx, ly, m);
+          read_w6(ring(j + 1), lx, ly, p);
+          axis_edges<R, ISEN>(m, m, c, p, p, P.inv_gamma, su[2], sd[2]);
+          conv += p[3] - m[3];
+          jump = fmaxf(jump, fabsf(p[4] - m[4]) / fminf(p[4], m[4]));
+        }
+      }
+      // a ghost beside a coarser block: the slopes along the face's transverse axes dropped at
+      // the rim of the face
+      float mask[3] = {1.f, 1.f, 1.f};
+      {
+        const int lz = DIM == 3 ? j : 0;
+        const float rx = (lx == 0 || lx == BS - 1) ? 0.f : 1.f;
+        const float ry = (ly == 0 || ly == BS - 1) ? 0.f : 1.f;
+        const float rz = (lz == 0 || lz == BS - 1) ? 0.f : 1.f;
+        if (zghost && znb == -1) {
+          mask[0] = rx;
+          mask[1] = ry;
+        } else if (g_coarse) {
+          if (g_axis == 0) mask[1] = ry;
+          else mask[0] = rx;
+          if (DIM == 3) mask[2] = rz;
+        }
+      }
+      Pred pr;
+      hancock_masked<DIM>(c, conv, jump, su, sd, mask, h, P, pr);
+
+      const bool tile_plane = j >= 0 && j < (DIM == 3 ? BS : 1);
+      if (xyg && tile_plane) {
+        // x and y boundary ghosts take the half step of the inner cell they map to
+#pragma unroll
+        for (int v = 0; v < 6; v++) sFlux[v * SPN + tid] = pr.q[v];
+        sFlux[6 * SPN + tid] = pr.flag;
+        sFlux[7 * SPN + tid] = pr.fo ? 1.f : 0.f;
+        __syncthreads();
+        if (g_src >= 0) {
+#pragma unroll
+          for (int v = 0; v < 6; v++) pr.q[v] = sFlux[v * SPN + g_src];
+          if (g_flip) pr.q[1 + g_axis] = -pr.q[1 + g_axis];
+          pr.flag = sFlux[6 * SPN + g_src];
+          pr.fo = sFlux[7 * SPN + g_src] != 0.f;
+        }
+      }
+      if constexpr (DIM == 3) {
+        // z boundary ghosts: the lower one takes plane 0's half step with its own increments
+        // (kept from plane -1); the upper one plane 15's (kept from plane 15). Each thread keeps
+        // and reads back its own column: no barrier needed.
+        if (j == -1 && zlo_nb <= -2) {
+#pragma unroll
+          for (int v = 0; v < 6; v++) sKeep[v * SPN + tid] = su[2][v];
+        }
+        if (j == 0 && zlo_nb <= -2) {
+          Pred gq = pr;
+          if (-1 - zlo_nb == 2) gq.q[3] = -gq.q[3];
+          float inc[6];
+#pragma unroll
+          for (int v = 0; v < 6; v++) inc[v] = sKeep[v * SPN + tid];
+          face_state(gq, inc, 1.f, zhi_prev);
+        }
+        if (j == BS - 1 && zhi_nb <= -2) {
+#pragma unroll
+          for (int v = 0; v < 6; v++) sKeep[v * SPN + tid] = pr.q[v];
+          sKeep[6 * SPN + tid] = pr.flag;
+          sKeep[7 * SPN + tid] = pr.fo ? 1.f : 0.f;
+        }
+        if (j == BS && zhi_nb <= -2) {
+#pragma unroll
+          for (int v = 0; v < 6; v++) pr.q[v] = sKeep[v * SPN + tid];
+          if (-1 - zhi_nb == 2) pr.q[3] = -pr.q[3];
+          pr.flag = sKeep[6 * SPN + tid];
+          pr.fo = sKeep[7 * SPN + tid] != 0.f;
+        }
+      }
+      if (tile_plane) {
+        float f[7];
+        face_state(pr, su[0], 1.f, f);
+#pragma unroll
+        for (int v = 0; v < 7; v++) sFace[v * SPN + tid] = f[v];
+        if constexpr (DIM >= 2) {
+          face_state(pr, su[1], 1.f, f);
+#pragma unroll
+          for (int v = 0; v < 7; v++) sFace[(7 + v) * SPN + tid] = f[v];
+        }
+      }
+      __syncthreads();
+
+      const int lz = DIM == 3 ? j : 0;
+      if (tile_plane) {
+        if (row_t && tx >= 1) {
+          // the x face below cell lx (lx = 0 .. 16)
+          float L[7], Rr[7], F[8];
+#pragma unroll
+          for (int v = 0; v < 7; v++) L[v] = sFace[v * SPN + tid - 1];
+          face_state(pr, sd[0], -1.f, Rr);
+          riemann<0>(L, Rr, P, F);
+          if ((lx == 0 && (fine & 1u)) || (lx == BS && (fine & 2u))) {
+            const Flux8 m = fine_mean_flux<DIM, R, ISEN, 0>(Pp, bt, w1, w2, sNb[lx == 0 ? 0 : 1], lx == 0 ? 0 : BS - 1,
+                                                            ly, lz, lx != 0, 2.f * h);
+#pragma unroll
+            for (int v = 0; v < 8; v++) F[v] = m.v[v];
+          }
+#pragma unroll
+          for (int v = 0; v < 8; v++) sFlux[v * SPN + tid] = F[v];
+        }
+        if constexpr (DIM >= 2) {
+          if (col_t && ty >= 1) {
+            float L[7], Rr[7], F[8];
+#pragma unroll
+            for (int v = 0; v < 7; v++) L[v] = sFace[(7 + v) * SPN + tid - SX];
+            face_state(pr, sd[1], -1.f, Rr);
+            riemann<1>(L, Rr, P, F);
+            if ((ly == 0 && (fine & 4u)) || (ly == BS && (fine & 8u))) {
+              const Flux8 m = fine_mean_flux<DIM, R, ISEN, 1>(Pp, bt, w1, w2, sNb[ly == 0 ? 2 : 3], lx,
+                                                              ly == 0 ? 0 : BS - 1, lz, ly != 0, 2.f * h);
+#pragma unroll
+              for (int v = 0; v < 8; v++) F[v] = m.v[v];
+            }
+#pragma unroll
+            for (int v = 0; v < 8; v++) sFlux[(8 + v) * SPN + tid] = F[v];
+          }
+        }
+      }
+      float Fz[8];
+      if constexpr (DIM == 3) {
+        if (tile_t && j >= 0) {
+          // the z face below plane j
+          float Rr[7];
+          face_state(pr, sd[2], -1.f, Rr);
+          riemann<2>(zhi_prev, Rr, P, Fz);
+          if ((j == 0 && (fine & 16u)) || (j == BS && (fine & 32u))) {
+            const Flux8 m = fine_mean_flux<DIM, R, ISEN, 2>(Pp, bt, w1, w2, sNb[j == 0 ? 4 : 5], lx, ly,
+                                                            j == 0 ? 0 : BS - 1, j != 0, 2.f * h);
+#pragma unroll
+            for (int v = 0; v < 8; v++) Fz[v] = m.v[v];
+          }
+        }
+      }
+      __syncthreads();
+
+      if (tile_t) {
+        if constexpr (DIM == 3) {
+          if (j >= 1) {
+            // plane j - 1 is complete: its upper z face is Fz
+#pragma unroll
+            for (int v = 0; v < 8; v++) acc[v] -= Fz[v];
+            const size_t o = base + ((size_t)(j - 1) * BS + ly) * BS + lx;
+            float4 na, nb4;
+            update_cell(__ldg(u1 + o), __ldg(u2 + o), acc, ph_prev, dtdx, P, na, nb4);
+            o1[o] = na;
+            o2[o] = nb4;
+          }
+        }
+        if (tile_plane) {
+#pragma unroll
+          for (int v = 0; v < 8; v++) {
+            float a = sFlux[v * SPN + tid];
+            a -= sFlux[v * SPN + tid + 1];
+            if constexpr (DIM >= 2) {
+              a += sFlux[(8 + v) * SPN + tid];
+              a -= sFlux[(8 + v) * SPN + tid + SX];
+            }
+            if constexpr (DIM == 3) a += Fz[v];
+            acc[v] = a;
+          }
+          ph_prev = pr.q[4];
+          if constexpr (DIM < 3) {
+            const size_t o = base + (size_t)ly * BS + lx;
+            float4 na, nb4;
+            update_cell(__ldg(u1 + o), __ldg(u2 + o), acc, ph_prev, dtdx, P, na, nb4);
+            o1[o] = na;
+            o2[o] = nb4;
+          }
+        }
+      }
+      if constexpr (DIM == 3) {
+        // the upper z face state of plane j (a lower boundary ghost's is set at plane 0)
+        if (!(j == -1 && zlo_nb <= -2)) face_state(pr, su[2], 1.f, zhi_prev);
+      }
+    }
+  }
+}
+
 }  // namespace amrk
 
 // ---------------------------------------------------------------------------------------------
@@ -821,6 +1320,38 @@ cudaError_t amr_launch_update(const AmrLaunch& L, const int* list, int n, const 
     else { SHZ_RECON_SWITCH(L.recon, false, (amrk::amr_update<2, R, false><<<g, amrk::NT, 0, s>>>(L.gp, L.bt, list, n, u1, u2, L.w1, L.w2, L.p1, L.p2, o1, o2, clks))) }
   }
   return cudaGetLastError();
+}
+
+namespace {
+template <int DIM, int R, bool ISEN>
+cudaError_t sweep_one(const AmrLaunch& L, const int* list, int n, const float4* u1, const float4* u2, float4* o1,
+                      float4* o2, const DevClock* clks, cudaStream_t s) {
+  auto k = amrk::amr_sweep<DIM, R, ISEN>;
+  // (set once per instantiation; an attribute call is not a stream operation, so a first call
+  // inside a stream capture is fine)
+  static const cudaError_t attr = [&] {
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)amrk::SWEEP_SMEM);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
+    return e;
+  }();
+  if (attr != cudaSuccess) return attr;
+  k<<<grid_for(n, 2), amrk::SNT, amrk::SWEEP_SMEM, s>>>(L.gp, L.bt, list, n, u1, u2, L.w1, L.w2, o1, o2, clks);
+  return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t amr_launch_sweep(const AmrLaunch& L, const int* list, int n, const float4* u1, const float4* u2, float4* o1,
+                             float4* o2, const DevClock* clks, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  if (L.ndim == 3) {
+    if (L.isen) { SHZ_RECON_SWITCH(L.recon, true, return (sweep_one<3, R, true>(L, list, n, u1, u2, o1, o2, clks, s))) }
+    else { SHZ_RECON_SWITCH(L.recon, false, return (sweep_one<3, R, false>(L, list, n, u1, u2, o1, o2, clks, s))) }
+  } else {
+    if (L.isen) { SHZ_RECON_SWITCH(L.recon, true, return (sweep_one<2, R, true>(L, list, n, u1, u2, o1, o2, clks, s))) }
+    else { SHZ_RECON_SWITCH(L.recon, false, return (sweep_one<2, R, false>(L, list, n, u1, u2, o1, o2, clks, s))) }
+  }
+  return cudaSuccess;
 }
 
 cudaError_t amr_launch_flag(const AmrLaunch& L, const int* list, int n, float* flags, cudaStream_t s) {

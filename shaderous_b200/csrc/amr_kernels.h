@@ -17,7 +17,7 @@ struct AmrLaunch {
   const int* bt;
   float4* w1;   // primitives with ghosts, 20^ndim texels per slot
   float4* w2;
-  float4* p1;   // half steps, 18^ndim texels per slot
+  float4* p1;   // half steps, 18^ndim texels per slot (the two-pass step only; else null)
   float4* p2;
 };
 
@@ -29,6 +29,10 @@ cudaError_t launch_clock_multi(DevClock* clks, unsigned* rates, int rslot, int n
 cudaError_t amr_launch_predict(const AmrLaunch& L, const int* list, int n, const DevClock* clks, cudaStream_t s);
 cudaError_t amr_launch_update(const AmrLaunch& L, const int* list, int n, const float4* u1, const float4* u2, float4* o1,
                               float4* o2, const DevClock* clks, cudaStream_t s);
+// Predict, fluxes and update of every leaf in one pass over the primitive atlas (no half-step
+// atlas): the step's third kernel, standing for predict + update.
+cudaError_t amr_launch_sweep(const AmrLaunch& L, const int* list, int n, const float4* u1, const float4* u2, float4* o1,
+                             float4* o2, const DevClock* clks, cudaStream_t s);
 cudaError_t amr_launch_flag(const AmrLaunch& L, const int* list, int n, float* flags, cudaStream_t s);
 cudaError_t amr_launch_regrid(const AmrLaunch& L, const int* rg, const int* list, int n, const float4* u1,
                               const float4* u2, float4* o1, float4* o2, cudaStream_t s);

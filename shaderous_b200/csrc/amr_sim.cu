@@ -1,7 +1,8 @@
 // The adaptive-grid run (shz_amr_*): the host side of the reference's AmrSim
 // (src/amr/amr_sim.ts). It owns the block tree (amr_tree.cpp), the atlases in HBM, the block
-// table and slot lists on the device, and one stream. A step is one CUDA graph of four kernels
-// (assemble, clock, predict, update: amr_kernels.cu); every regrid_every steps the Löhner flags
+// table and slot lists on the device, and one stream. A step is one CUDA graph of three kernels
+// (assemble, clock, the fused block sweep: amr_kernels.cu), or of four with two_pass (predict and
+// update in place of the sweep); every regrid_every steps the Löhner flags
 // are read back, BlockTree.adapt decides the new mesh on the host, the new tables go up and the
 // regrid kernel fills the new leaves (amr_sim.ts:2648 applyRegrid, :3033 encodeFlags, :3525 readFlags).
 #include <cuda_runtime.h>
@@ -133,17 +134,22 @@ int read_clock(shz_amr* a, shz::DevClock* h) {
 int n_all(const shz_amr* a) { return (int)a->h_all.size(); }
 int n_leaves(const shz_amr* a) { return (int)a->h_leaves.size(); }
 
-// One step's four kernels, enqueued.
+// One step's kernels, enqueued.
 int enqueue_step(shz_amr* a) {
   AMR_CUDA(a, shz::amr_launch_assemble(a->L, a->d_all, n_all(a), a->u1[a->cur], a->u2[a->cur], a->rates, a->slot, a->stream));
   AMR_CUDA(a, shz::launch_clock_multi(a->clk, a->rates, a->slot, 1, a->stream));
-  AMR_CUDA(a, shz::amr_launch_predict(a->L, a->d_leaves, n_leaves(a), a->clk, a->stream));
-  AMR_CUDA(a, shz::amr_launch_update(a->L, a->d_leaves, n_leaves(a), a->u1[a->cur], a->u2[a->cur], a->u1[1 - a->cur],
-                                     a->u2[1 - a->cur], a->clk, a->stream));
+  if (a->cfg.two_pass) {
+    AMR_CUDA(a, shz::amr_launch_predict(a->L, a->d_leaves, n_leaves(a), a->clk, a->stream));
+    AMR_CUDA(a, shz::amr_launch_update(a->L, a->d_leaves, n_leaves(a), a->u1[a->cur], a->u2[a->cur], a->u1[1 - a->cur],
+                                       a->u2[1 - a->cur], a->clk, a->stream));
+  } else {
+    AMR_CUDA(a, shz::amr_launch_sweep(a->L, a->d_leaves, n_leaves(a), a->u1[a->cur], a->u2[a->cur], a->u1[1 - a->cur],
+                                      a->u2[1 - a->cur], a->clk, a->stream));
+  }
   return 0;
 }
 
-// One step, as the CUDA graph of its four kernels for this (state parity, rate slot); the graphs
+// One step, as the CUDA graph of its kernels for this (state parity, rate slot); the graphs
 // are captured once per mesh and replayed.
 int step_once(shz_amr* a) {
   cudaGraphExec_t& g = a->graphs[a->cur * 2 + a->slot];
@@ -159,7 +165,7 @@ int step_once(shz_amr* a) {
     if (e != cudaSuccess) return fail(a, SHZ_E_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
   }
   AMR_CUDA(a, cudaGraphLaunch(g, a->stream));
-  a->launches += 4;
+  a->launches += a->cfg.two_pass ? 4 : 3;
   a->cur ^= 1;
   a->slot ^= 1;
   return 0;
@@ -366,8 +372,10 @@ int shz_amr_create(const shz_amr_config* cfg, shz_amr** out) {
   }
   ok = ok && cudaMalloc(&a->w1, cap * a->WN * sizeof(float4)) == cudaSuccess;
   ok = ok && cudaMalloc(&a->w2, cap * a->WN * sizeof(float4)) == cudaSuccess;
-  ok = ok && cudaMalloc(&a->p1, cap * a->PN * sizeof(float4)) == cudaSuccess;
-  ok = ok && cudaMalloc(&a->p2, cap * a->PN * sizeof(float4)) == cudaSuccess;
+  if (c.two_pass) {
+    ok = ok && cudaMalloc(&a->p1, cap * a->PN * sizeof(float4)) == cudaSuccess;
+    ok = ok && cudaMalloc(&a->p2, cap * a->PN * sizeof(float4)) == cudaSuccess;
+  }
   ok = ok && cudaMalloc(&a->d_bt, cap * shz::amr::BT_STRIDE * sizeof(int)) == cudaSuccess;
   ok = ok && cudaMalloc(&a->d_all, cap * sizeof(int)) == cudaSuccess;
   ok = ok && cudaMalloc(&a->d_leaves, cap * sizeof(int)) == cudaSuccess;
@@ -383,7 +391,7 @@ int shz_amr_create(const shz_amr_config* cfg, shz_amr** out) {
     cudaGetLastError();
     char buf[160];
     snprintf(buf, sizeof buf, "the atlases of %d block slots (%.2f GB) do not fit", c.cap,
-             cap * (4.0 * a->CB + 2.0 * a->WN + 2.0 * a->PN) * 16 / 1e9);
+             cap * (4.0 * a->CB + 2.0 * a->WN + (c.two_pass ? 2.0 * a->PN : 0.0)) * 16 / 1e9);
     return bail(SHZ_E_OOM, buf);
   }
   a->L.bt = a->d_bt;

@@ -61,6 +61,7 @@ Block* BlockTree::create(int level, const int c[3], Block* parent) {
   if (slot > high_slot) high_slot = slot;
   arena_.push_back(Block{slot, level, {c[0], c[1], c[2]}, parent, {}});
   Block* b = &arena_.back();
+  ++version_;
   slots_[slot] = b;
   blocks_[key(level, c[0], c[1], c[2])] = b;
   return b;
@@ -68,6 +69,7 @@ Block* BlockTree::create(int level, const int c[3], Block* parent) {
 
 void BlockTree::remove(Block* b) {
   blocks_.erase(key(b->level, b->c[0], b->c[1], b->c[2]));
+  ++version_;
   slots_[b->slot] = nullptr;
   free_.push_back(b->slot);
 }
@@ -261,26 +263,40 @@ bool BlockTree::near(const Block* a, const Block* q) const {
   return true;
 }
 
-// tree.ts:449-467 makeRoom.
+// tree.ts:449-467 makeRoom. The candidates' tests are the reference's, in its order; those that
+// do not involve b (touched, live, leaf children, canCoarsen) are pure functions of the tree and
+// the touched set, which change together, so they are evaluated once per version of the tree:
+// adapt calls this for every flagged leaf, and on a full slot budget each call scans thousands
+// of candidates.
 bool BlockTree::make_room(Block* b, double level, const std::vector<Evictable>& ev,
-                          const std::unordered_set<const Block*>& touched, double tier, std::vector<Block*>& out) {
+                          const std::unordered_set<const Block*>& touched, double tier, std::vector<Block*>& out,
+                          EvictCache& cache) {
   out.clear();
   if (!b->leaf() || b->level >= level_limit) return false;
   std::unordered_set<const Block*> need;
   int shortage = refine_cost(b, need) - (int)free_.size();
   if (shortage <= 0) return false;
-  for (const Evictable& e : ev) {
+  if (cache.version != version_ || cache.ok.size() != ev.size()) {
+    cache.ok.assign(ev.size(), -1);  // -1: not yet evaluated at this version
+    cache.version = version_;
+  }
+  for (size_t i = 0; i < ev.size(); i++) {
+    const Evictable& e = ev[i];
     Block* p = e.p;
     if (e.tier < tier || (e.tier == tier && e.score >= EVICT_MARGIN * level)) break;
-    if (touched.count(p) || !live(p) || p->leaf()) continue;
-    bool bad = false;
-    for (Block* ch : p->children) bad |= !ch->leaf() || touched.count(ch) > 0;
-    if (bad) continue;
+    if (cache.ok[i] < 0) {
+      bool ok = !(touched.count(p) || !live(p) || p->leaf());
+      if (ok)
+        for (Block* ch : p->children) ok = ok && ch->leaf() && touched.count(ch) == 0;
+      ok = ok && can_coarsen(p);
+      cache.ok[i] = ok ? 1 : 0;
+    }
+    if (!cache.ok[i]) continue;
     if (need.count(p)) continue;
     bool close = false;
     for (const Block* q : need)
       if (near(p, q)) { close = true; break; }
-    if (close || !can_coarsen(p)) continue;
+    if (close) continue;
     out.push_back(p);
     shortage -= nchild;
     if (shortage <= 0) return true;
@@ -378,6 +394,7 @@ std::vector<RegridOp> BlockTree::adapt(const std::function<double(const Block*)>
   });
   bool have_ev = false;
   std::vector<Evictable> ev;
+  EvictCache ev_cache;
   std::vector<Block*> room;
   for (Block* b : wanted) {
     if (!b->leaf() || !live(b)) continue;
@@ -386,7 +403,7 @@ std::vector<RegridOp> BlockTree::adapt(const std::function<double(const Block*)>
         ev = evictable(before, ind, tier);
         have_ev = true;
       }
-      if (make_room(b, ind[b], ev, touched, tiers[b], room)) {
+      if (make_room(b, ind[b], ev, touched, tiers[b], room, ev_cache)) {
         for (Block* p : room) run.step(ADAPT_EVICT, p);
         run.step(ADAPT_REFINE, b);
       }

@@ -114,13 +114,20 @@ class BlockTree {
   std::vector<Evictable> evictable(const std::vector<Block*>& leaves, const std::unordered_map<const Block*, double>& ind,
                                    const std::function<double(const Block*)>& tier) const;
   bool near(const Block* a, const Block* q) const;
+  // The part of make_room's test of a candidate that does not depend on the block being refined,
+  // per entry of `ev`, for one version of the tree (recomputed when the tree has changed).
+  struct EvictCache {
+    std::vector<signed char> ok;
+    uint64_t version = ~0ull;
+  };
   bool make_room(Block* b, double level, const std::vector<Evictable>& ev, const std::unordered_set<const Block*>& touched,
-                 double tier, std::vector<Block*>& out);
+                 double tier, std::vector<Block*>& out, EvictCache& cache);
 
   std::deque<Block> arena_;  // blocks are never freed while the tree lives (identity for live())
   std::unordered_map<int64_t, Block*> blocks_;
   std::vector<Block*> slots_;
   std::vector<int> free_;  // a stack: back() is the top
+  uint64_t version_ = 0;   // bumped by every create and remove
   int64_t span_;
   std::vector<std::array<int, 3>> diagonals_;
 };

@@ -4,7 +4,8 @@
 // Each request is a uniform grid of 16^ndim-cell blocks: a level-0 block tree whose rows the
 // server writes into one shared block table, with the request's own parameter and clock index in
 // word 26. An engine per dimensionality owns the shared atlases; a round is `round_steps` steps,
-// each one CUDA graph of four kernels over the blocks of every running request. Between rounds the
+// each one CUDA graph of three kernels (assemble, clocks, the fused block sweep) over the blocks of
+// every running request. Between rounds the
 // host reads the clocks back, finishes the requests that have taken their steps (float64 totals,
 // optionally their state), frees their slots, and admits queued requests whose blocks fit, their
 // initial states sampled on the host while the GPU runs the round.
@@ -52,11 +53,11 @@ struct Grid {
 };
 
 struct Engine {
-  int ndim = 3, CB = 0, WN = 0, PN = 0;
+  int ndim = 3, CB = 0, WN = 0;
   int cap = 0, gmax = 0;
   float4* u1[2] = {nullptr, nullptr};
   float4* u2[2] = {nullptr, nullptr};
-  float4 *w1 = nullptr, *w2 = nullptr, *p1 = nullptr, *p2 = nullptr;
+  float4 *w1 = nullptr, *w2 = nullptr;
   int *d_bt = nullptr, *d_list = nullptr, *d_glist = nullptr;
   shz::KParams* d_gp = nullptr;
   shz::DevClock* d_clk = nullptr;
@@ -73,7 +74,7 @@ struct Engine {
   cudaStream_t stream = nullptr;
   shz::AmrLaunch L{};
   long long launches = 0;
-  int64_t slot_bytes() const { return (int64_t)(4 * CB + 2 * WN + 2 * PN) * 16; }
+  int64_t slot_bytes() const { return (int64_t)(4 * CB + 2 * WN) * 16; }
 };
 
 }  // namespace
@@ -137,7 +138,6 @@ int engine_init(shz_server* s, Engine& e, int ndim, double budget) {
   e.ndim = ndim;
   e.CB = ndim == 3 ? 4096 : 256;
   e.WN = ndim == 3 ? 8000 : 400;
-  e.PN = ndim == 3 ? 5832 : 324;
   e.gmax = s->cfg.max_grids;
   e.cap = (int)std::max<int64_t>(0, (int64_t)(budget / (double)e.slot_bytes()));
   e.L.ndim = ndim;
@@ -152,8 +152,6 @@ int engine_init(shz_server* s, Engine& e, int ndim, double budget) {
   }
   SV_CUDA(s, cudaMalloc(&e.w1, cap * e.WN * sizeof(float4)));
   SV_CUDA(s, cudaMalloc(&e.w2, cap * e.WN * sizeof(float4)));
-  SV_CUDA(s, cudaMalloc(&e.p1, cap * e.PN * sizeof(float4)));
-  SV_CUDA(s, cudaMalloc(&e.p2, cap * e.PN * sizeof(float4)));
   SV_CUDA(s, cudaMalloc(&e.d_bt, cap * 32 * sizeof(int)));
   SV_CUDA(s, cudaMalloc(&e.d_list, cap * sizeof(int)));
   SV_CUDA(s, cudaMalloc(&e.d_glist, cap * sizeof(int)));
@@ -180,8 +178,8 @@ int engine_init(shz_server* s, Engine& e, int ndim, double budget) {
   e.L.bt = e.d_bt;
   e.L.w1 = e.w1;
   e.L.w2 = e.w2;
-  e.L.p1 = e.p1;
-  e.L.p2 = e.p2;
+  e.L.p1 = nullptr;  // (the fused sweep keeps no half-step atlas)
+  e.L.p2 = nullptr;
   return 0;
 }
 
@@ -192,7 +190,7 @@ void engine_free(Engine& e) {
     cudaFree(e.u1[p]);
     cudaFree(e.u2[p]);
   }
-  void* b[] = {e.w1, e.w2, e.p1, e.p2, e.d_bt, e.d_list, e.d_glist, e.d_gp, e.d_clk, e.d_rates, e.d_part, e.d_out};
+  void* b[] = {e.w1, e.w2, e.d_bt, e.d_list, e.d_glist, e.d_gp, e.d_clk, e.d_rates, e.d_part, e.d_out};
   for (void* x : b)
     if (x) cudaFree(x);
   if (e.stream) cudaStreamDestroy(e.stream);
@@ -338,9 +336,8 @@ int enqueue_step(shz_server* s, Engine& e) {
   const int n = (int)e.h_list.size();
   SV_CUDA(s, shz::amr_launch_assemble(e.L, e.d_list, n, e.u1[e.cur], e.u2[e.cur], e.d_rates, e.rslot, e.stream));
   SV_CUDA(s, shz::launch_clock_multi(e.d_clk, e.d_rates, e.rslot, e.gmax, e.stream));
-  SV_CUDA(s, shz::amr_launch_predict(e.L, e.d_list, n, e.d_clk, e.stream));
-  SV_CUDA(s, shz::amr_launch_update(e.L, e.d_list, n, e.u1[e.cur], e.u2[e.cur], e.u1[1 - e.cur], e.u2[1 - e.cur], e.d_clk,
-                                    e.stream));
+  SV_CUDA(s, shz::amr_launch_sweep(e.L, e.d_list, n, e.u1[e.cur], e.u2[e.cur], e.u1[1 - e.cur], e.u2[1 - e.cur], e.d_clk,
+                                   e.stream));
   return 0;
 }
 
@@ -363,7 +360,7 @@ int launch_round(shz_server* s, Engine& e) {
       if (ie != cudaSuccess) return fail(s, SHZ_E_CUDA, "instantiate: %s", cudaGetErrorString(ie));
     }
     SV_CUDA(s, cudaGraphLaunch(g, e.stream));
-    e.launches += 4;
+    e.launches += 3;
     e.cur ^= 1;
     e.rslot ^= 1;
   }
