@@ -273,7 +273,9 @@ int shz_amr_clock(shz_amr* a, double* t, double* dt, int64_t* steps);
 int shz_amr_regrid(shz_amr* a, int32_t* changed);
 /* The leaves, coarsest first (lists().leaves): slots, levels and block coordinates (3 per leaf). */
 int shz_amr_leaves(shz_amr* a, int32_t* n_leaves, int32_t* slots, int32_t* levels, int32_t* coords);
-/* The block table on the device (cap * 32 ints), read back: the same as the tree's. */
+/* The block table on the device (cap * 32 ints), read back: the tree's, plus two words the passes
+ * use: 26 the block's grid (0 here) and 27 a leaf's first entry in the fine-flux buffer of its
+ * faces matched to refined neighbours (-1 for none). */
 int shz_amr_table(shz_amr* a, int32_t* out);
 /* State of the leaves in lists().leaves order: 16^ndim cells each, x fastest, float4 u1 and u2. */
 int shz_amr_get_leaves_state(shz_amr* a, float* u1, float* u2);

@@ -5,11 +5,13 @@
 //   - the primitives with two ghost layers: 20^ndim cells x (w1 = rho, v; w2 = p, s, cs, 0);
 //   - the half-step states over the block and one ghost layer: 18^ndim cells x
 //     (p1 = rho, v; p2 = p, s, shock flag, first-order flag).
-// One step is three kernels, captured in a CUDA graph by the host:
+// One step is three or four kernels, captured in a CUDA graph by the host:
 //   1. amr_assemble over every block (leaves and parents): primitives with ghost fill.
 //   2. clock_multi_kernel: dt.
-//   3. amr_sweep over the leaves: half steps, fluxes, fine-flux matching and the update, in one
-//      pass over the primitives.
+//   3. amr_fine_flux over the faces whose same-level neighbour is refined: the mean fine fluxes
+//      (only when the mesh has such faces).
+//   4. amr_sweep over the leaves: half steps, fluxes and the update, in one pass over the
+//      primitives, the matched faces' fluxes read from the buffer step 3 filled.
 // The reference's own pass structure is kept beside it as a cross-check (two_pass): amr_predict
 // writes the half steps to their atlas and amr_update reads them.
 // This follows the reference's AmrSim.encodeSteps (src/amr/amr_sim.ts:2709-2946), and its rules
@@ -19,6 +21,7 @@
 // (amr/update.wgsl:207-295). Every kernel walks a device list of block slots with a fixed grid of
 // CTAs, one block at a time per CTA.
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <cstdint>
 
 #include "amr_kernels.h"
@@ -32,6 +35,9 @@ constexpr int BS = 16, NG = 2, PAD = BS + 2 * NG, PP = BS + 2, BTS = 32, RGS = 1
 // Word of a block-table row that holds the block's grid: an index into the per-grid parameters
 // and clocks (a batch advances blocks of many independent grids in one pass).
 constexpr int GRID_WORD = 26;
+// Word of a leaf's row that holds the index of its first matched face in the fine-flux buffer
+// (faces whose same-level neighbour is refined, in face order); -1 for none.
+constexpr int FINE_WORD = 27;
 constexpr int NT = 256;  // threads per CTA
 
 template <int DIM>
@@ -908,13 +914,12 @@ __device__ __forceinline__ void predict_texel(const KParams& P, const int* __res
 
 // The mean of the fine fluxes through the face of cell l on side `hi` of axis AXIS, whose
 // same-level neighbour np is refined: computed from the fine leaf's own atlas as the fine leaf's
-// sweep computes them. (Out of line: it runs at a few faces of a few blocks, and inlined it
-// would crowd the registers of the march.)
+// sweep computes them.
 struct Flux8 {
   float v[8];
 };
 template <int DIM, int R, bool ISEN, int AXIS>
-__device__ __noinline__ Flux8 fine_mean_flux(const KParams* __restrict__ Pp, const int* __restrict__ bt,
+__device__ __forceinline__ Flux8 fine_mean_flux(const KParams* __restrict__ Pp, const int* __restrict__ bt,
                                              const float4* __restrict__ w1, const float4* __restrict__ w2, int np, int l0,
                                              int l1, int l2, bool hi, float hf) {
   const KParams& P = *Pp;
@@ -958,6 +963,40 @@ __device__ __noinline__ Flux8 fine_mean_flux(const KParams* __restrict__ Pp, con
   return out;
 }
 
+// Fine-flux matching, ahead of the sweep (amr/update.wgsl:207-295): for every face of a leaf
+// whose same-level neighbour is refined, the mean of the fine fluxes through each of its cells,
+// into the buffer entry the host assigned (entries: leaf slot, face, index). One thread per face
+// cell, so that the few blocks with such faces do not hold up a sweep's CTA.
+template <int DIM, int R, bool ISEN>
+__global__ void __launch_bounds__(NT) amr_fine_flux(const KParams* __restrict__ gp, const int* __restrict__ bt,
+                                                    const int* __restrict__ flist, int nf, const float4* __restrict__ w1,
+                                                    const float4* __restrict__ w2, const DevClock* __restrict__ clks,
+                                                    float4* __restrict__ fbuf) {
+  constexpr int FC = DIM == 3 ? BS * BS : BS;  // cells of a face
+  const long long total = (long long)nf * FC;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int e = (int)(t / FC), c = (int)(t % FC);
+    const int slot = __ldg(flist + 3 * e), f = __ldg(flist + 3 * e + 1), k = __ldg(flist + 3 * e + 2);
+    const int g = bt_at(bt, slot, GRID_WORD);
+    if (clks[g].held) continue;
+    const KParams* Pp = gp + g;
+    const double dt = clks[g].dt;
+    const float hf = (float)((0.5 * dt) / (Pp->dx / ldexp(1.0, bt_at(bt, slot, 0) + 1)));  // h at the fine level
+    const int axis = f >> 1;
+    const bool hi = (f & 1) != 0;
+    const int np = bt_at(bt, slot, 6 + f);
+    const int t1 = c % BS, t2 = c / BS;
+    const int edge = hi ? BS - 1 : 0;
+    Flux8 F;
+    if (axis == 0) F = fine_mean_flux<DIM, R, ISEN, 0>(Pp, bt, w1, w2, np, edge, t1, t2, hi, hf);
+    else if (axis == 1) F = fine_mean_flux<DIM, R, ISEN, 1>(Pp, bt, w1, w2, np, t1, edge, t2, hi, hf);
+    else F = fine_mean_flux<DIM, R, ISEN, 2>(Pp, bt, w1, w2, np, t1, t2, edge, hi, hf);
+    float4* o = fbuf + ((size_t)k * FC + c) * 2;
+    o[0] = make_float4(F.v[0], F.v[1], F.v[2], F.v[3]);
+    o[1] = make_float4(F.v[4], F.v[5], F.v[6], F.v[7]);
+  }
+}
+
 // Shared memory of the block sweep, in floats.
 constexpr int SW_RING = 3 * 6 * SWN;  // three planes of primitives
 constexpr int SW_FACE = 2 * 7 * SPN;  // x and y upper face states of a plane
@@ -970,13 +1009,15 @@ __global__ void __maxnreg__(80)
     amr_sweep(const KParams* __restrict__ gp, const int* __restrict__ bt, const int* __restrict__ list, int n,
               const float4* __restrict__ u1, const float4* __restrict__ u2, const float4* __restrict__ w1,
               const float4* __restrict__ w2, float4* __restrict__ o1, float4* __restrict__ o2,
-              const DevClock* __restrict__ clks) {
+              const DevClock* __restrict__ clks, const float4* __restrict__ fbuf) {
+  constexpr int FC = DIM == 3 ? BS * BS : BS;  // cells of a face
   extern __shared__ __align__(16) float smem[];
   float* sW = smem;
   float* sFace = sW + SW_RING;
   float* sFlux = sFace + SW_FACE;
   float* sKeep = sFlux + SW_FLUX;
-  __shared__ int sNb[6];
+  // the block's grid parameters, copied once per block: the march reads them at every face
+  __shared__ __align__(16) KParams sP;
   const int tid = threadIdx.x;
   const int tx = tid % SX, ty = tid / SX;
   const int lx = tx - 1, ly = DIM >= 2 ? ty - 1 : 0;
@@ -988,10 +1029,8 @@ __global__ void __maxnreg__(80)
   for (int i = blockIdx.x; i < n; i += gridDim.x) {
     const int slot = __ldg(list + i);
     const int g = bt_at(bt, slot, GRID_WORD);
-    const KParams* Pp = gp + g;
-    const KParams& P = *Pp;
     const double dt = clks[g].dt;
-    const double dxl = P.dx / ldexp(1.0, bt_at(bt, slot, 0));
+    const double dxl = gp[g].dx / ldexp(1.0, bt_at(bt, slot, 0));
     const float dtdx = (float)(dt / dxl);
     const float h = (float)((0.5 * dt) / dxl);
     const size_t base = (size_t)slot * BG<DIM>::CB;
@@ -1003,7 +1042,10 @@ __global__ void __maxnreg__(80)
       continue;
     }
     __syncthreads();  // the previous block's last reads of shared memory
-    if (tid < 6) sNb[tid] = bt_at(bt, slot, 6 + tid);
+    static_assert(sizeof(KParams) % 4 == 0, "KParams is copied as words");
+    if (tid < (int)(sizeof(KParams) / 4))
+      reinterpret_cast<int*>(&sP)[tid] = __ldg(reinterpret_cast<const int*>(gp + g) + tid);
+    const KParams& P = sP;
     // This thread's ghost role across x or y: the face and, for a domain boundary, the thread
     // holding the inner cell that the ghost maps to (mirror or edge cell: both the adjacent one).
     int gface = -1;
@@ -1020,13 +1062,22 @@ __global__ void __maxnreg__(80)
     bool xyg = false;
 #pragma unroll
     for (int f = 0; f < 4; f++) xyg = xyg || bt_at(bt, slot, 6 + f) <= -2;
-    // the faces' fine-flux matching (a same-level neighbour that is refined)
+    // the faces' fine-flux matching (a same-level neighbour that is refined): their fluxes are
+    // in the buffer, from amr_fine_flux, at entries fine0 on in face order
     unsigned fine = 0;
 #pragma unroll
     for (int f = 0; f < 2 * DIM; f++) {
       const int nb = bt_at(bt, slot, 6 + f);
       if (nb >= 0 && !leaf_of(bt, nb)) fine |= 1u << f;
     }
+    const int fine0 = bt_at(bt, slot, FINE_WORD);
+    if (fine0 < 0 || fbuf == nullptr) fine = 0;
+    auto matched = [&](int f, int cidx, float* F) {
+      const float4* q = fbuf + ((size_t)(fine0 + __popc(fine & ((1u << f) - 1u))) * FC + cidx) * 2;
+      const float4 a = __ldg(q), b = __ldg(q + 1);
+      F[0] = a.x; F[1] = a.y; F[2] = a.z; F[3] = a.w;
+      F[4] = b.x; F[5] = b.y; F[6] = b.z; F[7] = b.w;
+    };
     const int zlo_nb = DIM == 3 ? bt_at(bt, slot, 10) : 0, zhi_nb = DIM == 3 ? bt_at(bt, slot, 11) : 0;
 
     float zhi_prev[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
@@ -1175,12 +1226,7 @@ __global__ void __maxnreg__(80)
           for (int v = 0; v < 7; v++) L[v] = sFace[v * SPN + tid - 1];
           face_state(pr, sd[0], -1.f, Rr);
           riemann<0>(L, Rr, P, F);
-          if ((lx == 0 && (fine & 1u)) || (lx == BS && (fine & 2u))) {
-            const Flux8 m = fine_mean_flux<DIM, R, ISEN, 0>(Pp, bt, w1, w2, sNb[lx == 0 ? 0 : 1], lx == 0 ? 0 : BS - 1,
-                                                            ly, lz, lx != 0, 2.f * h);
-#pragma unroll
-            for (int v = 0; v < 8; v++) F[v] = m.v[v];
-          }
+          if ((lx == 0 && (fine & 1u)) || (lx == BS && (fine & 2u))) matched(lx == 0 ? 0 : 1, ly + BS * lz, F);
 #pragma unroll
           for (int v = 0; v < 8; v++) sFlux[v * SPN + tid] = F[v];
         }
@@ -1191,12 +1237,7 @@ __global__ void __maxnreg__(80)
             for (int v = 0; v < 7; v++) L[v] = sFace[(7 + v) * SPN + tid - SX];
             face_state(pr, sd[1], -1.f, Rr);
             riemann<1>(L, Rr, P, F);
-            if ((ly == 0 && (fine & 4u)) || (ly == BS && (fine & 8u))) {
-              const Flux8 m = fine_mean_flux<DIM, R, ISEN, 1>(Pp, bt, w1, w2, sNb[ly == 0 ? 2 : 3], lx,
-                                                              ly == 0 ? 0 : BS - 1, lz, ly != 0, 2.f * h);
-#pragma unroll
-              for (int v = 0; v < 8; v++) F[v] = m.v[v];
-            }
+            if ((ly == 0 && (fine & 4u)) || (ly == BS && (fine & 8u))) matched(ly == 0 ? 2 : 3, lx + BS * lz, F);
 #pragma unroll
             for (int v = 0; v < 8; v++) sFlux[(8 + v) * SPN + tid] = F[v];
           }
@@ -1209,12 +1250,7 @@ __global__ void __maxnreg__(80)
           float Rr[7];
           face_state(pr, sd[2], -1.f, Rr);
           riemann<2>(zhi_prev, Rr, P, Fz);
-          if ((j == 0 && (fine & 16u)) || (j == BS && (fine & 32u))) {
-            const Flux8 m = fine_mean_flux<DIM, R, ISEN, 2>(Pp, bt, w1, w2, sNb[j == 0 ? 4 : 5], lx, ly,
-                                                            j == 0 ? 0 : BS - 1, j != 0, 2.f * h);
-#pragma unroll
-            for (int v = 0; v < 8; v++) Fz[v] = m.v[v];
-          }
+          if ((j == 0 && (fine & 16u)) || (j == BS && (fine & 32u))) matched(j == 0 ? 4 : 5, lx + BS * ly, Fz);
         }
       }
       __syncthreads();
@@ -1336,10 +1372,24 @@ cudaError_t sweep_one(const AmrLaunch& L, const int* list, int n, const float4* 
     return e;
   }();
   if (attr != cudaSuccess) return attr;
-  k<<<grid_for(n, 2), amrk::SNT, amrk::SWEEP_SMEM, s>>>(L.gp, L.bt, list, n, u1, u2, L.w1, L.w2, o1, o2, clks);
+  k<<<grid_for(n, 2), amrk::SNT, amrk::SWEEP_SMEM, s>>>(L.gp, L.bt, list, n, u1, u2, L.w1, L.w2, o1, o2, clks, L.fbuf);
   return cudaGetLastError();
 }
 }  // namespace
+
+cudaError_t amr_launch_fine_flux(const AmrLaunch& L, const int* flist, int nf, const DevClock* clks, cudaStream_t s) {
+  if (nf <= 0) return cudaSuccess;
+  const long long cells = (long long)nf * (L.ndim == 3 ? 256 : 16);
+  const int g = (int)std::min<long long>((cells + amrk::NT - 1) / amrk::NT, 148LL * 8);
+  if (L.ndim == 3) {
+    if (L.isen) { SHZ_RECON_SWITCH(L.recon, true, (amrk::amr_fine_flux<3, R, true><<<g, amrk::NT, 0, s>>>(L.gp, L.bt, flist, nf, L.w1, L.w2, clks, L.fbuf))) }
+    else { SHZ_RECON_SWITCH(L.recon, false, (amrk::amr_fine_flux<3, R, false><<<g, amrk::NT, 0, s>>>(L.gp, L.bt, flist, nf, L.w1, L.w2, clks, L.fbuf))) }
+  } else {
+    if (L.isen) { SHZ_RECON_SWITCH(L.recon, true, (amrk::amr_fine_flux<2, R, true><<<g, amrk::NT, 0, s>>>(L.gp, L.bt, flist, nf, L.w1, L.w2, clks, L.fbuf))) }
+    else { SHZ_RECON_SWITCH(L.recon, false, (amrk::amr_fine_flux<2, R, false><<<g, amrk::NT, 0, s>>>(L.gp, L.bt, flist, nf, L.w1, L.w2, clks, L.fbuf))) }
+  }
+  return cudaGetLastError();
+}
 
 cudaError_t amr_launch_sweep(const AmrLaunch& L, const int* list, int n, const float4* u1, const float4* u2, float4* o1,
                              float4* o2, const DevClock* clks, cudaStream_t s) {

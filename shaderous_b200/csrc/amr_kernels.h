@@ -19,6 +19,9 @@ struct AmrLaunch {
   float4* w2;
   float4* p1;   // half steps, 18^ndim texels per slot (the two-pass step only; else null)
   float4* p2;
+  // Fine-flux buffer of the fused sweep: 2 float4 per face cell (16^(ndim-1) cells) per matched
+  // face; a leaf's row holds its first entry in word 27 (-1: none).
+  float4* fbuf = nullptr;
 };
 
 // rates: two 32-bit maxima per grid; the assemble folds the leaves' rate / dx into slot rslot.
@@ -29,8 +32,11 @@ cudaError_t launch_clock_multi(DevClock* clks, unsigned* rates, int rslot, int n
 cudaError_t amr_launch_predict(const AmrLaunch& L, const int* list, int n, const DevClock* clks, cudaStream_t s);
 cudaError_t amr_launch_update(const AmrLaunch& L, const int* list, int n, const float4* u1, const float4* u2, float4* o1,
                               float4* o2, const DevClock* clks, cudaStream_t s);
+// The mean fine fluxes of the matched faces listed in flist (leaf slot, face, buffer entry per
+// face), into L.fbuf; before the sweep.
+cudaError_t amr_launch_fine_flux(const AmrLaunch& L, const int* flist, int nf, const DevClock* clks, cudaStream_t s);
 // Predict, fluxes and update of every leaf in one pass over the primitive atlas (no half-step
-// atlas): the step's third kernel, standing for predict + update.
+// atlas), standing for predict + update.
 cudaError_t amr_launch_sweep(const AmrLaunch& L, const int* list, int n, const float4* u1, const float4* u2, float4* o1,
                              float4* o2, const DevClock* clks, cudaStream_t s);
 cudaError_t amr_launch_flag(const AmrLaunch& L, const int* list, int n, float* flags, cudaStream_t s);

@@ -1,8 +1,9 @@
 // The adaptive-grid run (shz_amr_*): the host side of the reference's AmrSim
 // (src/amr/amr_sim.ts). It owns the block tree (amr_tree.cpp), the atlases in HBM, the block
-// table and slot lists on the device, and one stream. A step is one CUDA graph of three kernels
-// (assemble, clock, the fused block sweep: amr_kernels.cu), or of four with two_pass (predict and
-// update in place of the sweep); every regrid_every steps the Löhner flags
+// table and slot lists on the device, and one stream. A step is one CUDA graph of three or four
+// kernels (assemble, clock, the matched faces' fine fluxes where the mesh has any, the fused block
+// sweep: amr_kernels.cu), or of four with two_pass (predict and update in place of the last two);
+// every regrid_every steps the Löhner flags
 // are read back, BlockTree.adapt decides the new mesh on the host, the new tables go up and the
 // regrid kernel fills the new leaves (amr_sim.ts:2648 applyRegrid, :3033 encodeFlags, :3525 readFlags).
 #include <cuda_runtime.h>
@@ -41,7 +42,12 @@ struct shz_amr {
   unsigned* rates = nullptr;  // slots 0, 1: the steps'; 2, 3: the refinement check's
   double *diag_part = nullptr, *diag_out = nullptr;
   int* d_ghost = nullptr;
-  std::vector<int32_t> h_bt, h_all, h_leaves, h_rg;
+  // faces matched to refined neighbours (fused sweep): (leaf slot, face, entry) triples and the
+  // buffer of their mean fine fluxes, grown with the mesh
+  int* d_flist = nullptr;
+  float4* fbuf = nullptr;
+  int nfine = 0, fine_cap = 0;
+  std::vector<int32_t> h_bt, h_all, h_leaves, h_rg, h_flist;
   std::vector<float> h_flags;
   int cur = 0, slot = 0;
   long long since_check = 0;
@@ -101,6 +107,43 @@ int upload_tables(shz_amr* a) {
   for (int s = 0; s < cap; s++) a->h_bt[(size_t)s * shz::amr::BT_STRIDE + 26] = 0;  // every block is grid 0's
   std::vector<int32_t> per;
   a->tree->lists(a->h_all, a->h_leaves, per);
+  // the fused sweep's matched faces: each leaf's faces whose same-level neighbour is refined get
+  // consecutive buffer entries, the first in word 27 of its row
+  a->h_flist.clear();
+  if (!a->cfg.two_pass) {
+    const int32_t* bt = a->h_bt.data();
+    const int S = shz::amr::BT_STRIDE;
+    for (int s : a->h_leaves) {
+      for (int f = 0; f < 2 * a->cfg.ndim; f++) {
+        const int nb = bt[(size_t)s * S + 6 + f];
+        if (nb < 0 || (bt[(size_t)nb * S + 4] & 2)) continue;
+        const int k = (int)(a->h_flist.size() / 3);
+        if (a->h_bt[(size_t)s * S + 27] < 0) a->h_bt[(size_t)s * S + 27] = k;
+        a->h_flist.insert(a->h_flist.end(), {s, f, k});
+      }
+    }
+  }
+  a->nfine = (int)(a->h_flist.size() / 3);
+  if (a->nfine > a->fine_cap) {
+    AMR_CUDA(a, cudaStreamSynchronize(a->stream));
+    cudaFree(a->d_flist);
+    cudaFree(a->fbuf);
+    a->d_flist = nullptr;
+    a->fbuf = nullptr;
+    a->fine_cap = 0;
+    const int want = a->nfine + a->nfine / 2 + 64;
+    const size_t fc = a->cfg.ndim == 3 ? 256 : 16;
+    if (cudaMalloc(&a->d_flist, (size_t)want * 3 * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&a->fbuf, (size_t)want * fc * 2 * sizeof(float4)) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(a, SHZ_E_OOM, "the fine-flux buffer of %d matched faces does not fit", want);
+    }
+    a->fine_cap = want;
+  }
+  a->L.fbuf = a->fbuf;
+  if (a->nfine > 0)
+    AMR_CUDA(a, cudaMemcpyAsync(a->d_flist, a->h_flist.data(), a->h_flist.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                                a->stream));
   AMR_CUDA(a, cudaMemcpyAsync(a->d_bt, a->h_bt.data(), a->h_bt.size() * sizeof(int32_t), cudaMemcpyHostToDevice, a->stream));
   AMR_CUDA(a, cudaMemcpyAsync(a->d_all, a->h_all.data(), a->h_all.size() * sizeof(int32_t), cudaMemcpyHostToDevice, a->stream));
   AMR_CUDA(a, cudaMemcpyAsync(a->d_leaves, a->h_leaves.data(), a->h_leaves.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
@@ -143,6 +186,7 @@ int enqueue_step(shz_amr* a) {
     AMR_CUDA(a, shz::amr_launch_update(a->L, a->d_leaves, n_leaves(a), a->u1[a->cur], a->u2[a->cur], a->u1[1 - a->cur],
                                        a->u2[1 - a->cur], a->clk, a->stream));
   } else {
+    AMR_CUDA(a, shz::amr_launch_fine_flux(a->L, a->d_flist, a->nfine, a->clk, a->stream));
     AMR_CUDA(a, shz::amr_launch_sweep(a->L, a->d_leaves, n_leaves(a), a->u1[a->cur], a->u2[a->cur], a->u1[1 - a->cur],
                                       a->u2[1 - a->cur], a->clk, a->stream));
   }
@@ -165,7 +209,7 @@ int step_once(shz_amr* a) {
     if (e != cudaSuccess) return fail(a, SHZ_E_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
   }
   AMR_CUDA(a, cudaGraphLaunch(g, a->stream));
-  a->launches += a->cfg.two_pass ? 4 : 3;
+  a->launches += a->cfg.two_pass ? 4 : (a->nfine > 0 ? 4 : 3);
   a->cur ^= 1;
   a->slot ^= 1;
   return 0;
@@ -422,7 +466,7 @@ void shz_amr_destroy(shz_amr* a) {
     cudaFree(a->u2[p]);
   }
   void* bufs[] = {a->w1, a->w2, a->p1, a->p2, a->d_bt, a->d_all, a->d_leaves, a->d_rg, a->d_flags, a->d_gp,
-                  a->clk, a->rates, a->diag_part, a->diag_out, a->d_ghost};
+                  a->clk, a->rates, a->diag_part, a->diag_out, a->d_ghost, a->d_flist, a->fbuf};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (a->stream) cudaStreamDestroy(a->stream);
