@@ -352,6 +352,34 @@ int64_t shz_kernel_launches(const shz_sim* sim);
 const char* shz_version(void);
 
 /*
+ * The launch-shape autotuner. No counterpart in the reference, whose WGSL passes have fixed
+ * workgroup sizes chosen per kernel at build time (src/gpu/*.ts).
+ *
+ * The first time a handle runs a tunable kernel for a (kernel, ndim, reconstruction, isentropic,
+ * size class) key, it times every candidate shape in place inside one real step, keeps the
+ * fastest in a process-wide table, and uses it from then on (also in captured CUDA graphs).
+ * Candidates differ only in launch shape, never in arithmetic: the state is the same whichever
+ * wins. Kernels and their knobs:
+ *   0 uniform sweep: tz = planes a CTA marches along z (3D);
+ *   1 AMR assemble: variant = register budget (0: 1, 1: 2, 2: 3 CTAs per SM), per_sm = CTAs of
+ *     the work-list grid per SM;
+ *   2 AMR fused sweep: per_sm;
+ *   3 AMR fine-flux pass: per_sm.
+ */
+typedef struct shz_tune_entry {
+  int32_t kernel, ndim, recon, isentropic, size_class;  /* the key; size class = floor(log2 units) */
+  int32_t variant, per_sm, tz;                          /* the choice (0: the kernel's default) */
+  int32_t candidates;                                   /* shapes timed */
+  float ms, default_ms;                                 /* mean time of the choice and of the default */
+} shz_tune_entry;
+/* Turn the tuner on (default) or off (every launch takes the default shape). Process-wide. */
+int shz_tune_enable(int32_t on);
+/* Forget every choice. */
+void shz_tune_reset(void);
+/* Copy up to `max` entries of the table; *n = entries in the table. */
+int shz_tune_entries(shz_tune_entry* out, int32_t max, int32_t* n);
+
+/*
  * Conservation totals of a state the caller owns, computed without allocating anything.
  * No counterpart in the reference.
  *

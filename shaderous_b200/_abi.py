@@ -137,6 +137,11 @@ class shz_server_stats(C.Structure):
     ]
 
 
+class shz_tune_entry(C.Structure):
+    _fields_ = [(f, C.c_int32) for f in ("kernel", "ndim", "recon", "isentropic", "size_class", "variant", "per_sm", "tz",
+                                         "candidates")] + [("ms", C.c_float), ("default_ms", C.c_float)]
+
+
 class shz_profile_result(C.Structure):
     _fields_ = [("steps", C.c_int32), ("total_ms", C.c_double), ("sweep_ms", C.c_double), ("launches", C.c_int64)]
 
@@ -162,6 +167,9 @@ SIGNATURES = [
     ("shz_profile", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(shz_profile_result)]),
     ("shz_kernel_launches", C.c_int64, [C.c_void_p]),
     ("shz_version", C.c_char_p, []),
+    ("shz_tune_enable", C.c_int, [C.c_int32]),
+    ("shz_tune_reset", None, []),
+    ("shz_tune_entries", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]),
     ("shz_tree_create", C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_int32),
                                   C.POINTER(C.c_int32), C.c_int32, C.POINTER(C.c_void_p)]),
     ("shz_tree_destroy", None, [C.c_void_p]),

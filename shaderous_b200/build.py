@@ -10,6 +10,7 @@ from __future__ import annotations
 
 import os
 import subprocess
+from concurrent.futures import ThreadPoolExecutor
 import sys
 from pathlib import Path
 
@@ -39,26 +40,34 @@ def _stale(target: Path, deps: list[Path]) -> bool:
     return any(d.stat().st_mtime > t for d in deps)
 
 
+def _compile(src: Path, obj: Path, verbose: bool) -> None:
+    cmd = [NVCC, "-O3", "-std=c++17", *ARCH, "-lineinfo", "--use_fast_math", "-Xcompiler", "-fPIC,-fopenmp,-O3",
+           "-I", str(ROOT / "include"), "-c", str(src), "-o", str(obj)]
+    if src.suffix == ".cu":
+        cmd[1:1] = ["-Xptxas", "-v"] if verbose else []
+    else:
+        cmd[1:1] = ["-x", "cu"]
+    subprocess.run(cmd, check=True)
+
+
 def build_library(force: bool = False, verbose: bool = False) -> Path:
+    """Compile the objects that are older than their source or any header (all of them in
+    parallel, one nvcc per core) and link the library when any object changed."""
     srcs = _sources()
-    if not force and not _stale(LIB, srcs + _headers() + [Path(__file__)]):
-        return LIB
+    deps = _headers() + [Path(__file__)]
     obj_dir = PKG / "_build"
     obj_dir.mkdir(exist_ok=True)
-    objs = []
-    for src in srcs:
-        obj = obj_dir / (src.stem + ".o")
-        cmd = [NVCC, "-O3", "-std=c++17", *ARCH, "-lineinfo", "--use_fast_math", "-Xcompiler", "-fPIC,-fopenmp,-O3",
-               "-I", str(ROOT / "include"), "-c", str(src), "-o", str(obj)]
-        if src.suffix == ".cu":
-            cmd[1:1] = ["-Xptxas", "-v"] if verbose else []
-        else:
-            cmd[1:1] = ["-x", "cu"]
-        subprocess.run(cmd, check=True)
-        objs.append(str(obj))
-    tmp = LIB.with_suffix(".so.tmp")
-    subprocess.run([NVCC, "-shared", *ARCH, "-o", str(tmp), *objs, "-Xcompiler", "-fopenmp", "-lgomp"], check=True)
-    os.replace(tmp, LIB)
+    objs = [obj_dir / (src.stem + ".o") for src in srcs]
+    todo = [(s, o) for s, o in zip(srcs, objs) if force or _stale(o, [s] + deps)]
+    if todo:
+        with ThreadPoolExecutor(max_workers=max(1, os.cpu_count() or 1)) as pool:
+            for f in [pool.submit(_compile, s, o, verbose) for s, o in todo]:
+                f.result()
+    if todo or force or _stale(LIB, objs):
+        tmp = LIB.with_suffix(".so.tmp")
+        subprocess.run([NVCC, "-shared", *ARCH, "-o", str(tmp), *map(str, objs), "-Xcompiler", "-fopenmp", "-lgomp"],
+                       check=True)
+        os.replace(tmp, LIB)
     return LIB
 
 

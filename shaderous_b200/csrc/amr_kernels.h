@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include "hydro_math.cuh"
+#include "tune.h"
 
 namespace shz {
 
@@ -25,8 +26,9 @@ struct AmrLaunch {
 };
 
 // rates: two 32-bit maxima per grid; the assemble folds the leaves' rate / dx into slot rslot.
+// c: the autotuner's choice (null: the default shape), as for the fine-flux pass and the sweep.
 cudaError_t amr_launch_assemble(const AmrLaunch& L, const int* list, int n, const float4* u1, const float4* u2,
-                                unsigned* rates, int rslot, cudaStream_t s);
+                                unsigned* rates, int rslot, cudaStream_t s, const tune::Choice* c = nullptr);
 // The clocks of `ngrids` grids at once (one thread each): dt from each grid's rate slot.
 cudaError_t launch_clock_multi(DevClock* clks, unsigned* rates, int rslot, int ngrids, cudaStream_t s);
 cudaError_t amr_launch_predict(const AmrLaunch& L, const int* list, int n, const DevClock* clks, cudaStream_t s);
@@ -34,11 +36,12 @@ cudaError_t amr_launch_update(const AmrLaunch& L, const int* list, int n, const 
                               float4* o2, const DevClock* clks, cudaStream_t s);
 // The mean fine fluxes of the matched faces listed in flist (leaf slot, face, buffer entry per
 // face), into L.fbuf; before the sweep.
-cudaError_t amr_launch_fine_flux(const AmrLaunch& L, const int* flist, int nf, const DevClock* clks, cudaStream_t s);
+cudaError_t amr_launch_fine_flux(const AmrLaunch& L, const int* flist, int nf, const DevClock* clks, cudaStream_t s,
+                                 const tune::Choice* c = nullptr);
 // Predict, fluxes and update of every leaf in one pass over the primitive atlas (no half-step
 // atlas), standing for predict + update.
 cudaError_t amr_launch_sweep(const AmrLaunch& L, const int* list, int n, const float4* u1, const float4* u2, float4* o1,
-                             float4* o2, const DevClock* clks, cudaStream_t s);
+                             float4* o2, const DevClock* clks, cudaStream_t s, const tune::Choice* c = nullptr);
 cudaError_t amr_launch_flag(const AmrLaunch& L, const int* list, int n, float* flags, cudaStream_t s);
 cudaError_t amr_launch_regrid(const AmrLaunch& L, const int* rg, const int* list, int n, const float4* u1,
                               const float4* u2, float4* o1, float4* o2, cudaStream_t s);
@@ -46,5 +49,22 @@ int amr_diag_blocks(int n);
 cudaError_t amr_launch_diag(const AmrLaunch& L, const int* list, int n, const float4* u1, const float4* u2, double* part,
                             double* out, cudaStream_t s);
 cudaError_t amr_launch_ghost_map(const AmrLaunch& L, int slot, int* out, cudaStream_t s);
+
+}  // namespace shz
+
+namespace shz {
+
+// Launch with the autotuner's shape for the key; when the key has none yet and `tune_now` is set
+// (an eager step, not a graph capture), time every candidate in place and keep the fastest.
+// *launches grows by the kernels launched.
+tune::Key amr_tune_key(int kernel, const AmrLaunch& L, long long units);
+cudaError_t amr_assemble_tuned(const AmrLaunch& L, const int* list, int n, const float4* u1, const float4* u2,
+                               unsigned* rates, int rslot, cudaStream_t s, bool tune_now, long long* launches);
+cudaError_t amr_fine_flux_tuned(const AmrLaunch& L, const int* flist, int nf, const DevClock* clks, cudaStream_t s,
+                                bool tune_now, long long* launches);
+cudaError_t amr_sweep_tuned(const AmrLaunch& L, const int* list, int n, const float4* u1, const float4* u2, float4* o1,
+                            float4* o2, const DevClock* clks, cudaStream_t s, bool tune_now, long long* launches);
+// Whether a step over n leaves (nf matched faces) would tune anything.
+bool amr_step_wants_tuning(const AmrLaunch& L, int n_assembled, int n_leaves, int nf);
 
 }  // namespace shz

@@ -53,6 +53,7 @@ struct shz_amr {
   long long since_check = 0;
   cudaStream_t stream = nullptr;
   cudaGraphExec_t graphs[4] = {nullptr, nullptr, nullptr, nullptr};
+  long long graph_launches[4] = {0, 0, 0, 0};  // kernels one replay of each graph launches
   long long launches = 0;
   std::string err;
   int device = 0;
@@ -153,6 +154,12 @@ int upload_tables(shz_amr* a) {
   return 0;
 }
 
+int read_clock(shz_amr* a, shz::DevClock* h) {
+  AMR_CUDA(a, cudaMemcpyAsync(h, a->clk, sizeof *h, cudaMemcpyDeviceToHost, a->stream));
+  AMR_CUDA(a, cudaStreamSynchronize(a->stream));
+  return 0;
+}
+
 int write_clock(shz_amr* a, double t, long long steps) {
   shz::DevClock h;
   std::memset(&h, 0, sizeof h);
@@ -168,27 +175,38 @@ int write_clock(shz_amr* a, double t, long long steps) {
   return 0;
 }
 
-int read_clock(shz_amr* a, shz::DevClock* h) {
-  AMR_CUDA(a, cudaMemcpyAsync(h, a->clk, sizeof *h, cudaMemcpyDeviceToHost, a->stream));
-  AMR_CUDA(a, cudaStreamSynchronize(a->stream));
-  return 0;
-}
 
 int n_all(const shz_amr* a) { return (int)a->h_all.size(); }
 int n_leaves(const shz_amr* a) { return (int)a->h_leaves.size(); }
 
-// One step's kernels, enqueued.
-int enqueue_step(shz_amr* a) {
-  AMR_CUDA(a, shz::amr_launch_assemble(a->L, a->d_all, n_all(a), a->u1[a->cur], a->u2[a->cur], a->rates, a->slot, a->stream));
+// One step's kernels, enqueued with the tuned launch shapes; *launches grows by the kernels
+// enqueued. With tune_now (an eager step, never a capture), kernels whose shape is not tuned yet
+// are timed in place over their candidates first (each candidate repeats the same step's work);
+// the clock is read back so that a held step (which only copies) tunes nothing.
+int enqueue_step(shz_amr* a, bool tune_now, long long* launches) {
+  // (the two passes predict same-level ghosts at their source, whose atlas may be a parent's;
+  // everything the fused sweep reads is a leaf's)
+  const int* asm_list = a->cfg.two_pass ? a->d_all : a->d_leaves;
+  const int asm_n = a->cfg.two_pass ? n_all(a) : n_leaves(a);
+  AMR_CUDA(a, shz::amr_assemble_tuned(a->L, asm_list, asm_n, a->u1[a->cur], a->u2[a->cur], a->rates, a->slot, a->stream,
+                                      tune_now, launches));
   AMR_CUDA(a, shz::launch_clock_multi(a->clk, a->rates, a->slot, 1, a->stream));
+  *launches += 1;
+  if (tune_now) {
+    shz::DevClock h;
+    int rc = read_clock(a, &h);
+    if (rc) return rc;
+    tune_now = !h.held;
+  }
   if (a->cfg.two_pass) {
     AMR_CUDA(a, shz::amr_launch_predict(a->L, a->d_leaves, n_leaves(a), a->clk, a->stream));
     AMR_CUDA(a, shz::amr_launch_update(a->L, a->d_leaves, n_leaves(a), a->u1[a->cur], a->u2[a->cur], a->u1[1 - a->cur],
                                        a->u2[1 - a->cur], a->clk, a->stream));
+    *launches += 2;
   } else {
-    AMR_CUDA(a, shz::amr_launch_fine_flux(a->L, a->d_flist, a->nfine, a->clk, a->stream));
-    AMR_CUDA(a, shz::amr_launch_sweep(a->L, a->d_leaves, n_leaves(a), a->u1[a->cur], a->u2[a->cur], a->u1[1 - a->cur],
-                                      a->u2[1 - a->cur], a->clk, a->stream));
+    AMR_CUDA(a, shz::amr_fine_flux_tuned(a->L, a->d_flist, a->nfine, a->clk, a->stream, tune_now, launches));
+    AMR_CUDA(a, shz::amr_sweep_tuned(a->L, a->d_leaves, n_leaves(a), a->u1[a->cur], a->u2[a->cur], a->u1[1 - a->cur],
+                                     a->u2[1 - a->cur], a->clk, a->stream, tune_now, launches));
   }
   return 0;
 }
@@ -196,20 +214,34 @@ int enqueue_step(shz_amr* a) {
 // One step, as the CUDA graph of its kernels for this (state parity, rate slot); the graphs
 // are captured once per mesh and replayed.
 int step_once(shz_amr* a) {
-  cudaGraphExec_t& g = a->graphs[a->cur * 2 + a->slot];
+  // a mesh whose kernels meet a size class the tuner has not seen: one eager step that tunes
+  if (!a->cfg.two_pass &&
+      shz::amr_step_wants_tuning(a->L, n_leaves(a), n_leaves(a), a->nfine)) {
+    long long n = 0;
+    const int rc = enqueue_step(a, true, &n);
+    if (rc) return rc;
+    a->launches += n;
+    a->cur ^= 1;
+    a->slot ^= 1;
+    return 0;
+  }
+  const int gi = a->cur * 2 + a->slot;
+  cudaGraphExec_t& g = a->graphs[gi];
   if (!g) {
     cudaGraph_t graph;
     AMR_CUDA(a, cudaStreamBeginCapture(a->stream, cudaStreamCaptureModeThreadLocal));
-    int rc = enqueue_step(a);
+    long long n = 0;
+    int rc = enqueue_step(a, false, &n);
     cudaError_t e = cudaStreamEndCapture(a->stream, &graph);
     if (rc) return rc;
     if (e != cudaSuccess) return fail(a, SHZ_E_CUDA, "capture of a step: %s", cudaGetErrorString(e));
     e = cudaGraphInstantiate(&g, graph, 0);
     cudaGraphDestroy(graph);
     if (e != cudaSuccess) return fail(a, SHZ_E_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
+    a->graph_launches[gi] = n;
   }
   AMR_CUDA(a, cudaGraphLaunch(g, a->stream));
-  a->launches += a->cfg.two_pass ? 4 : (a->nfine > 0 ? 4 : 3);
+  a->launches += a->graph_launches[gi];
   a->cur ^= 1;
   a->slot ^= 1;
   return 0;
@@ -218,7 +250,9 @@ int step_once(shz_amr* a) {
 // The refinement indicators of the current state: a fresh assemble, then the Löhner pass.
 int compute_flags(shz_amr* a) {
   AMR_CUDA(a, cudaMemsetAsync(a->rates + 2, 0, 2 * sizeof(unsigned), a->stream));
-  AMR_CUDA(a, shz::amr_launch_assemble(a->L, a->d_all, n_all(a), a->u1[a->cur], a->u2[a->cur], a->rates + 2, 0, a->stream));
+  AMR_CUDA(a, shz::amr_launch_assemble(a->L, a->cfg.two_pass ? a->d_all : a->d_leaves,
+                                       a->cfg.two_pass ? n_all(a) : n_leaves(a), a->u1[a->cur], a->u2[a->cur],
+                                       a->rates + 2, 0, a->stream));
   AMR_CUDA(a, cudaMemsetAsync(a->d_flags, 0, sizeof(float) * a->cfg.cap, a->stream));
   AMR_CUDA(a, shz::amr_launch_flag(a->L, a->d_leaves, n_leaves(a), a->d_flags, a->stream));
   a->launches += 2;

@@ -71,6 +71,7 @@ struct Engine {
   int cur = 0, rslot = 0;
   bool dirty = true;
   cudaGraphExec_t graphs[4] = {nullptr, nullptr, nullptr, nullptr};
+  long long graph_launches[4] = {0, 0, 0, 0};  // kernels one replay of each graph launches
   cudaStream_t stream = nullptr;
   shz::AmrLaunch L{};
   long long launches = 0;
@@ -332,12 +333,17 @@ int rebuild(shz_server* s, Engine& e) {
   return 0;
 }
 
-int enqueue_step(shz_server* s, Engine& e) {
+// One step over every running request's blocks, with the tuned launch shapes (tune_now: an eager
+// step that first times the candidates of untuned kernels in place); *launches grows by the
+// kernels enqueued.
+int enqueue_step(shz_server* s, Engine& e, bool tune_now, long long* launches) {
   const int n = (int)e.h_list.size();
-  SV_CUDA(s, shz::amr_launch_assemble(e.L, e.d_list, n, e.u1[e.cur], e.u2[e.cur], e.d_rates, e.rslot, e.stream));
+  SV_CUDA(s, shz::amr_assemble_tuned(e.L, e.d_list, n, e.u1[e.cur], e.u2[e.cur], e.d_rates, e.rslot, e.stream, tune_now,
+                                     launches));
   SV_CUDA(s, shz::launch_clock_multi(e.d_clk, e.d_rates, e.rslot, e.gmax, e.stream));
-  SV_CUDA(s, shz::amr_launch_sweep(e.L, e.d_list, n, e.u1[e.cur], e.u2[e.cur], e.u1[1 - e.cur], e.u2[1 - e.cur], e.d_clk,
-                                   e.stream));
+  *launches += 1;
+  SV_CUDA(s, shz::amr_sweep_tuned(e.L, e.d_list, n, e.u1[e.cur], e.u2[e.cur], e.u1[1 - e.cur], e.u2[1 - e.cur], e.d_clk,
+                                  e.stream, tune_now, launches));
   return 0;
 }
 
@@ -347,11 +353,23 @@ int launch_round(shz_server* s, Engine& e) {
   int rc = 0;
   if (e.dirty && (rc = rebuild(s, e))) return rc;
   for (int k = 0; k < s->cfg.round_steps; k++) {
-    cudaGraphExec_t& g = e.graphs[e.cur * 2 + e.rslot];
+    const int nb = (int)e.h_list.size();
+    if (shz::amr_step_wants_tuning(e.L, nb, nb, 0)) {
+      long long c = 0;
+      if ((rc = enqueue_step(s, e, true, &c))) return rc;
+      e.launches += c;
+      e.cur ^= 1;
+      e.rslot ^= 1;
+      continue;
+    }
+    const int gi = e.cur * 2 + e.rslot;
+    cudaGraphExec_t& g = e.graphs[gi];
     if (!g) {
       cudaGraph_t graph;
       SV_CUDA(s, cudaStreamBeginCapture(e.stream, cudaStreamCaptureModeThreadLocal));
-      rc = enqueue_step(s, e);
+      long long c = 0;
+      rc = enqueue_step(s, e, false, &c);
+      e.graph_launches[gi] = c;
       const cudaError_t ce = cudaStreamEndCapture(e.stream, &graph);
       if (rc) return rc;
       if (ce != cudaSuccess) return fail(s, SHZ_E_CUDA, "capture: %s", cudaGetErrorString(ce));
@@ -360,7 +378,7 @@ int launch_round(shz_server* s, Engine& e) {
       if (ie != cudaSuccess) return fail(s, SHZ_E_CUDA, "instantiate: %s", cudaGetErrorString(ie));
     }
     SV_CUDA(s, cudaGraphLaunch(g, e.stream));
-    e.launches += 3;
+    e.launches += e.graph_launches[gi];
     e.cur ^= 1;
     e.rslot ^= 1;
   }

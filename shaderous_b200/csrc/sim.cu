@@ -20,6 +20,7 @@
 #include "../../include/shaderous_b200.h"
 #include "problems.h"
 #include "sweep.h"
+#include "tune.h"
 
 struct shz_sim {
   shz_config cfg;
@@ -161,11 +162,64 @@ int refresh_rate(shz_sim* s) {
   return 0;
 }
 
+// The autotuner's key of this grid's sweep, and its tuned z depth (0: the default).
+shz::tune::Key sweep_key(const shz_sim* s) {
+  return shz::tune::Key{shz::tune::K_UNIFORM_SWEEP, s->ndim, s->cfg.recon,
+                        (s->cfg.isentropic != 0 && s->cfg.recon != SHZ_RECON_PPM) ? 1 : 0,
+                        shz::tune::size_class((long long)s->ncell)};
+}
+int sweep_tz(const shz_sim* s) {
+  shz::tune::Choice c;
+  return (s->ndim == 3 && shz::tune::lookup(sweep_key(s), &c)) ? c.tz : 0;
+}
+bool wants_tuning(const shz_sim* s) { return s->ndim == 3 && shz::tune::needs(sweep_key(s)); }
+
+// One step whose sweep is run once per candidate z depth, timed, the fastest kept. The sweep
+// reads one parity and writes the other (and folds the same rate maximum), so the step's result
+// is that of a single launch. A clock held at its stop time is not tuned on (the sweep would
+// only copy the state).
+int tuned_step(shz_sim* s) {
+  CUDA_OR_FAIL(s, shz::launch_clock(s->clk, s->rates, s->slot, s->stream));
+  s->launches += 1;
+  shz::DevClock h;
+  CUDA_OR_FAIL(s, cudaMemcpyAsync(&h, s->clk, sizeof h, cudaMemcpyDeviceToHost, s->stream));
+  CUDA_OR_FAIL(s, cudaStreamSynchronize(s->stream));
+  auto launch = [&](const shz::tune::Choice& c) {
+    return shz::launch_sweep(s->kp, s->ndim, s->cfg.recon, s->cfg.isentropic != 0, s->u1[s->cur], s->u2[s->cur],
+                             s->u1[1 - s->cur], s->u2[1 - s->cur], s->clk, s->rates + (s->slot ^ 1), s->stream, c.tz);
+  };
+  if (h.held) {
+    CUDA_OR_FAIL(s, launch(shz::tune::Choice{}));
+    s->launches += 1;
+  } else {
+    std::vector<shz::tune::Choice> cands;
+    for (int tz : {shz::SWEEP_TZ_DEFAULT, 32, 128, 256}) {
+      if (tz != shz::SWEEP_TZ_DEFAULT && tz > s->cfg.n[2]) continue;
+      shz::tune::Choice c;
+      c.tz = tz;
+      cands.push_back(c);
+    }
+    const int reps = 2;
+    shz::tune::Choice best;
+    CUDA_OR_FAIL(s, shz::tune::choose(sweep_key(s), cands, launch, s->stream, reps, &best));
+    s->launches += (long long)cands.size() * (1 + reps);
+  }
+  s->cur ^= 1;
+  s->slot ^= 1;
+  return 0;
+}
+
 int enqueue_steps(shz_sim* s, int n) {
   for (int i = 0; i < n; i++) {
+    if (wants_tuning(s)) {
+      const int rc = tuned_step(s);
+      if (rc) return rc;
+      continue;
+    }
     CUDA_OR_FAIL(s, shz::launch_clock(s->clk, s->rates, s->slot, s->stream));
     CUDA_OR_FAIL(s, shz::launch_sweep(s->kp, s->ndim, s->cfg.recon, s->cfg.isentropic != 0, s->u1[s->cur], s->u2[s->cur],
-                                      s->u1[1 - s->cur], s->u2[1 - s->cur], s->clk, s->rates + (s->slot ^ 1), s->stream));
+                                      s->u1[1 - s->cur], s->u2[1 - s->cur], s->clk, s->rates + (s->slot ^ 1), s->stream,
+                                      sweep_tz(s)));
     s->launches += 2;
     s->cur ^= 1;
     s->slot ^= 1;
@@ -479,11 +533,19 @@ int shz_profile(shz_sim* s, int32_t n, shz_profile_result* out) {
   int rc = 0;
   CUDA_OR_FAIL(s, cudaEventRecord(ev[0], s->stream));
   for (int i = 0; i < n && rc == 0; i++) {
+    if (wants_tuning(s)) {
+      // (a step that tunes the sweep counts whole, tuning included, as sweep time)
+      CUDA_OR_FAIL(s, cudaEventRecord(ev[1 + 2 * i], s->stream));
+      rc = tuned_step(s);
+      if (rc == 0) CUDA_OR_FAIL(s, cudaEventRecord(ev[2 + 2 * i], s->stream));
+      continue;
+    }
     cudaError_t e = shz::launch_clock(s->clk, s->rates, s->slot, s->stream);
     if (e == cudaSuccess) e = cudaEventRecord(ev[1 + 2 * i], s->stream);
     if (e == cudaSuccess)
       e = shz::launch_sweep(s->kp, s->ndim, s->cfg.recon, s->cfg.isentropic != 0, s->u1[s->cur], s->u2[s->cur],
-                            s->u1[1 - s->cur], s->u2[1 - s->cur], s->clk, s->rates + (s->slot ^ 1), s->stream);
+                            s->u1[1 - s->cur], s->u2[1 - s->cur], s->clk, s->rates + (s->slot ^ 1), s->stream,
+                            sweep_tz(s));
     if (e == cudaSuccess) e = cudaEventRecord(ev[2 + 2 * i], s->stream);
     if (e != cudaSuccess) rc = fail(s, SHZ_E_CUDA, "profile step %d: %s", i, cudaGetErrorString(e));
     s->launches += 2;

@@ -12,7 +12,7 @@
 // switch, writes the new state, and folds the new state's signal rate into the next step's
 // maximum (warp shuffles, then one atomicMax per CTA on the float's bits).
 //
-// Decomposition: a CTA owns a TX x TY column of cells and marches it along z through TZ planes
+// Decomposition: a CTA owns a TX x TY column of cells and marches it along z through tz planes
 // (2.5D). Its threads are the (TX+2) x (TY+2) cells of the column plus one ring of halo cells;
 // each thread keeps the primitives of its own column for the planes the predictor reads along
 // z in registers, so z-neighbours and z-faces never touch shared memory. Per plane, the
@@ -43,7 +43,6 @@ struct Geo {
   static constexpr int ZH = (RECON == R_PPM) ? 2 : 1;  // planes each way the predictor reads along z
   static constexpr int TX = (DIM == 1) ? 126 : 16;
   static constexpr int TY = (DIM == 1) ? 1 : 16;
-  static constexpr int TZ = (DIM == 3) ? 64 : 1;
   static constexpr int PX = TX + 2;
   static constexpr int PY = (DIM >= 2) ? TY + 2 : 1;
   static constexpr int NT = PX * PY;
@@ -121,7 +120,7 @@ __device__ __forceinline__ float rate_guard(float r) { return (r == r) ? r : __i
 template <int DIM, int RECON, bool ISEN>
 __global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, RECON>::MAXREG))
     sweep_kernel(const KParams P, const float4* __restrict__ u1, const float4* __restrict__ u2, float4* __restrict__ o1,
-                 float4* __restrict__ o2, const DevClock* __restrict__ clk, unsigned* __restrict__ rate_out) {
+                 float4* __restrict__ o2, const DevClock* __restrict__ clk, unsigned* __restrict__ rate_out, int tz) {
   using G = Geo<DIM, RECON>;
   constexpr int H = G::H, ZH = G::ZH, PX = G::PX, PN = G::PN, WN = G::WN, WC = G::WC;
   extern __shared__ __align__(16) float smem[];
@@ -151,8 +150,8 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, REC
 
   // A step held at the stop time (dt = 0) leaves the state as it is (clock.wgsl:120-125).
   if (clk->held) {
-    const int zb = (DIM == 3) ? blockIdx.z * G::TZ : 0;
-    const int ze = (DIM == 3) ? min(zb + G::TZ, nz) : 1;
+    const int zb = (DIM == 3) ? blockIdx.z * tz : 0;
+    const int ze = (DIM == 3) ? min(zb + tz, nz) : 1;
     for (int idx = tid; idx < G::TX * G::TY; idx += G::NT) {
       const int cx = x0 + idx % G::TX, cy = (DIM >= 2) ? y0 + idx / G::TX : 0;
       if (cx >= nx || cy >= ny) continue;
@@ -182,8 +181,8 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, REC
   if (DIM >= 2 && yg_lo && gy == -1 && col_t) { g_src = tid + PX; g_axis = 1; g_flip = P.bc_lo[1] == 2; }
   if (DIM >= 2 && yg_hi && gy == ny && col_t) { g_src = tid - PX; g_axis = 1; g_flip = P.bc_hi[1] == 2; }
 
-  const int z0 = (DIM == 3) ? blockIdx.z * G::TZ : 0;
-  const int z1 = (DIM == 3) ? min(z0 + G::TZ, nz) : 1;
+  const int z0 = (DIM == 3) ? blockIdx.z * tz : 0;
+  const int z1 = (DIM == 3) ? min(z0 + tz, nz) : 1;
   // plane -> its slot of the ring (planes may be negative near the lower boundary)
   auto ring = [&](int plane) -> float* {
     return sW + (((plane % G::NBUF) + G::NBUF) % G::NBUF) * WC * WN;
@@ -546,7 +545,7 @@ __global__ void diag_final_kernel(const double* __restrict__ part, int nblocks, 
 
 template <int DIM, int RECON, bool ISEN>
 static cudaError_t launch_sweep_t(const KParams& P, const float4* u1, const float4* u2, float4* o1, float4* o2,
-                                  const DevClock* clk, unsigned* rate_out, cudaStream_t s) {
+                                  const DevClock* clk, unsigned* rate_out, int tz, cudaStream_t s) {
   using G = Geo<DIM, RECON>;
   static bool configured = false;
   if (!configured) {
@@ -560,41 +559,42 @@ static cudaError_t launch_sweep_t(const KParams& P, const float4* u1, const floa
     configured = true;
   }
   dim3 grid((P.n[0] + G::TX - 1) / G::TX, DIM >= 2 ? (P.n[1] + G::TY - 1) / G::TY : 1,
-            DIM == 3 ? (P.n[2] + G::TZ - 1) / G::TZ : 1);
-  sweep_kernel<DIM, RECON, ISEN><<<grid, G::NT, G::SMEM_BYTES, s>>>(P, u1, u2, o1, o2, clk, rate_out);
+            DIM == 3 ? (P.n[2] + tz - 1) / tz : 1);
+  sweep_kernel<DIM, RECON, ISEN><<<grid, G::NT, G::SMEM_BYTES, s>>>(P, u1, u2, o1, o2, clk, rate_out, tz);
   return cudaGetLastError();
 }
 
 template <int DIM, int RECON>
 static cudaError_t launch_sweep_r(const KParams& P, bool isen, const float4* u1, const float4* u2, float4* o1, float4* o2,
-                                  const DevClock* clk, unsigned* rate_out, cudaStream_t s) {
+                                  const DevClock* clk, unsigned* rate_out, int tz, cudaStream_t s) {
   if constexpr (RECON == R_PPM) {
-    return launch_sweep_t<DIM, RECON, false>(P, u1, u2, o1, o2, clk, rate_out, s);
+    return launch_sweep_t<DIM, RECON, false>(P, u1, u2, o1, o2, clk, rate_out, tz, s);
   } else {
-    return isen ? launch_sweep_t<DIM, RECON, true>(P, u1, u2, o1, o2, clk, rate_out, s)
-                : launch_sweep_t<DIM, RECON, false>(P, u1, u2, o1, o2, clk, rate_out, s);
+    return isen ? launch_sweep_t<DIM, RECON, true>(P, u1, u2, o1, o2, clk, rate_out, tz, s)
+                : launch_sweep_t<DIM, RECON, false>(P, u1, u2, o1, o2, clk, rate_out, tz, s);
   }
 }
 
 template <int DIM>
 static cudaError_t launch_sweep_d(const KParams& P, int recon, bool isen, const float4* u1, const float4* u2, float4* o1,
-                                  float4* o2, const DevClock* clk, unsigned* rate_out, cudaStream_t s) {
+                                  float4* o2, const DevClock* clk, unsigned* rate_out, int tz, cudaStream_t s) {
   switch (recon) {
-    case R_MINMOD: return launch_sweep_r<DIM, R_MINMOD>(P, isen, u1, u2, o1, o2, clk, rate_out, s);
-    case R_MC: return launch_sweep_r<DIM, R_MC>(P, isen, u1, u2, o1, o2, clk, rate_out, s);
-    case R_VANLEER: return launch_sweep_r<DIM, R_VANLEER>(P, isen, u1, u2, o1, o2, clk, rate_out, s);
-    case R_KOREN: return launch_sweep_r<DIM, R_KOREN>(P, isen, u1, u2, o1, o2, clk, rate_out, s);
-    case R_PPM: return launch_sweep_r<DIM, R_PPM>(P, isen, u1, u2, o1, o2, clk, rate_out, s);
+    case R_MINMOD: return launch_sweep_r<DIM, R_MINMOD>(P, isen, u1, u2, o1, o2, clk, rate_out, tz, s);
+    case R_MC: return launch_sweep_r<DIM, R_MC>(P, isen, u1, u2, o1, o2, clk, rate_out, tz, s);
+    case R_VANLEER: return launch_sweep_r<DIM, R_VANLEER>(P, isen, u1, u2, o1, o2, clk, rate_out, tz, s);
+    case R_KOREN: return launch_sweep_r<DIM, R_KOREN>(P, isen, u1, u2, o1, o2, clk, rate_out, tz, s);
+    case R_PPM: return launch_sweep_r<DIM, R_PPM>(P, isen, u1, u2, o1, o2, clk, rate_out, tz, s);
     default: return cudaErrorInvalidValue;
   }
 }
 
 cudaError_t launch_sweep(const KParams& P, int ndim, int recon, bool isen, const float4* u1, const float4* u2, float4* o1,
-                         float4* o2, const DevClock* clk, unsigned* rate_out, cudaStream_t s) {
+                         float4* o2, const DevClock* clk, unsigned* rate_out, cudaStream_t s, int tz) {
+  if (tz <= 0) tz = SWEEP_TZ_DEFAULT;
   switch (ndim) {
-    case 1: return launch_sweep_d<1>(P, recon, isen, u1, u2, o1, o2, clk, rate_out, s);
-    case 2: return launch_sweep_d<2>(P, recon, isen, u1, u2, o1, o2, clk, rate_out, s);
-    case 3: return launch_sweep_d<3>(P, recon, isen, u1, u2, o1, o2, clk, rate_out, s);
+    case 1: return launch_sweep_d<1>(P, recon, isen, u1, u2, o1, o2, clk, rate_out, 1, s);
+    case 2: return launch_sweep_d<2>(P, recon, isen, u1, u2, o1, o2, clk, rate_out, 1, s);
+    case 3: return launch_sweep_d<3>(P, recon, isen, u1, u2, o1, o2, clk, rate_out, tz, s);
     default: return cudaErrorInvalidValue;
   }
 }
