@@ -11,7 +11,7 @@
  *  - Every function returns 0 on success or a negative SHZ_E* code; shz_last_error() gives the
  *    message of the last failure on a handle (UTF-8, owned by the handle).
  *  - Host buffers belong to the caller; device memory belongs to the handle. No device pointer
- *    escapes except through shz_state_device(), documented there.
+ *    escapes except through shz_state_device() and the slab functions below, documented there.
  *  - A handle is not re-entrant: callers serialise calls on one handle, as the reference's API
  *    serialises every call (src/ui/api.ts:1414-1416). Different handles may be used from
  *    different threads; each owns one CUDA stream.
@@ -43,6 +43,11 @@ extern "C" {
 #define SHZ_BC_PERIODIC 0
 #define SHZ_BC_OUTFLOW 1
 #define SHZ_BC_REFLECT 2
+/* z faces only: one slab of a grid split along z over several handles (one per GPU). The handle
+ * stores the face's ghost planes (shz_halo_depth) beyond the slab; the caller fills them with the
+ * neighbouring slab's planes before every step (shz_halo_device). No counterpart in the reference,
+ * which runs one grid on one GPU (docs/architecture.md:695-700). */
+#define SHZ_BC_HALO 3
 
 /* Reconstructions: the reference's limiters (src/reference/hydro.ts:30-46) plus PPM. */
 #define SHZ_RECON_MINMOD 0
@@ -186,6 +191,32 @@ int shz_sync(shz_sim* sim);
 /* Device pointers of the current state (two float4 arrays, layout above), valid until the next
  * step or destroy; for callers that keep data on the device (benchmarks, interop). */
 int shz_state_device(shz_sim* sim, void** u1, void** u2);
+
+/*
+ * A grid split into z-slabs, one handle per GPU (SHZ_BC_HALO faces). Before every step the
+ * caller, on the handle's stream:
+ *   1. copies each halo face's `inner` planes into the neighbouring slab's `ghost` planes of the
+ *      facing side (and receives its own ghosts likewise): NCCL send/recv between GPUs;
+ *   2. replaces the rate word with its maximum over all slabs (an all-reduce of uint32 max: the
+ *      word holds a non-negative float's bits), so that every slab takes the same dt;
+ * then calls shz_step(sim, 1). The pointers change parity every step: query them each time.
+ * No counterpart in the reference (single GPU).
+ */
+/* Load planes k0 .. k0 + nz - 1 of a built-in problem sampled on the whole grid `grid` (nx, ny
+ * and dx as the slab's) into the slab; the clock goes to 0. */
+int shz_reset_problem_slab(shz_sim* sim, const shz_config* grid, const shz_problem* prob, int32_t k0);
+/* Stored ghost planes of a halo face: 3 with PPM, else 2. */
+int shz_halo_depth(const shz_sim* sim, int32_t* planes);
+/* Face `side` (0 lower z, 1 upper z) of the current state: its inner planes (the slab's own
+ * planes next to the face) and its ghost planes (stored beyond it), each `bytes` long in u1 and
+ * in u2 (depth x nx x ny float4, x fastest). */
+int shz_halo_device(shz_sim* sim, int32_t side, void** inner_u1, void** inner_u2, void** ghost_u1, void** ghost_u2,
+                    size_t* bytes);
+/* The device word the next step's clock reads its rate from (uint32 bits of the largest
+ * rate / dx over this slab after its last step, or after shz_set_state / shz_reset_problem). */
+int shz_rate_device(shz_sim* sim, void** rate);
+/* The handle's CUDA stream (a cudaStream_t), to order the caller's transfers with the steps. */
+int shz_stream(shz_sim* sim, void** stream);
 
 /* Per-pass timing of `n` steps with CUDA events on the handle's stream, as the reference's
  * Sim.profile(reps) (src/sim.ts:3541) and its per-pass timestamps (src/gpu/timing.ts:232):

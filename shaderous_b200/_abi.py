@@ -165,6 +165,12 @@ SIGNATURES = [
     ("shz_sync", C.c_int, [C.c_void_p]),
     ("shz_state_device", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
     ("shz_profile", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(shz_profile_result)]),
+    ("shz_reset_problem_slab", C.c_int, [C.c_void_p, C.POINTER(shz_config), C.POINTER(shz_problem), C.c_int32]),
+    ("shz_halo_depth", C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
+    ("shz_halo_device", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                                  C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_size_t)]),
+    ("shz_rate_device", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    ("shz_stream", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     ("shz_kernel_launches", C.c_int64, [C.c_void_p]),
     ("shz_version", C.c_char_p, []),
     ("shz_tune_enable", C.c_int, [C.c_int32]),

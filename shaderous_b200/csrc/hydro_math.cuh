@@ -273,6 +273,13 @@ __device__ __forceinline__ float signal_rate(const float4 a, const float4 b, con
 // hydro.ts:216-220 bcAxis: the source index of a possibly out-of-range index and the sign of
 // the velocity along that axis. Indices beyond the reach of the scheme are clamped into range
 // (they feed no output).
+// Boundary codes: 0 periodic, 1 outflow, 2 reflect (the reference's), and 3 halo: a z face of one
+// slab of a larger grid, whose ghost planes are stored beyond the slab and filled by the caller
+// with the neighbouring slab's planes.
+constexpr int BC_HALO = 3;
+// Whether a face's ghosts take the adjacent inner cell's half step (outflow and reflect).
+__host__ __device__ __forceinline__ bool bc_inner(int code) { return code == 1 || code == 2; }
+
 __device__ __forceinline__ int bc_map(int i, int n, int lo, int hi, float& f) {
   f = 1.f;
   if (i < 0) {

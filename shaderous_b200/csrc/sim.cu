@@ -27,8 +27,11 @@ struct shz_sim {
   int ndim = 1;
   size_t ncell = 0;
   shz::KParams kp;
-  float4* u1[2] = {nullptr, nullptr};
+  float4* u1[2] = {nullptr, nullptr};  // first interior plane of each parity
   float4* u2[2] = {nullptr, nullptr};
+  float4* a1[2] = {nullptr, nullptr};  // the allocations: halo planes below, the grid, halo planes above
+  float4* a2[2] = {nullptr, nullptr};
+  int halo_lo = 0, halo_hi = 0;        // stored ghost planes below and above (z faces of code 3)
   int cur = 0;
   shz::DevClock* clk = nullptr;
   unsigned* rates = nullptr;  // two slots
@@ -83,17 +86,28 @@ struct DeviceScope {
 };
 
 int ndim_of(const shz_config& c) { return c.n[2] > 1 ? 3 : (c.n[1] > 1 ? 2 : 1); }
+// Ghost planes a halo face stores: the z march reads 1 + 2 planes beyond the slab with PPM's
+// five-cell stencil, 1 + 1 with the three-cell limiters.
+int halo_planes(const shz_config& c) { return c.recon == SHZ_RECON_PPM ? 3 : 2; }
 
 int validate(const shz_config& c, std::string& why) {
   char b[256];
   for (int a = 0; a < 3; a++) {
     if (c.n[a] < 1) { snprintf(b, sizeof b, "n[%d] = %d: every axis needs at least one cell", a, c.n[a]); why = b; return -1; }
-    if (c.bc_lo[a] < 0 || c.bc_lo[a] > 2 || c.bc_hi[a] < 0 || c.bc_hi[a] > 2) {
-      snprintf(b, sizeof b, "axis %d: boundary codes are 0 periodic, 1 outflow, 2 reflect", a); why = b; return -1;
+    const int top = a == 2 ? 3 : 2;
+    if (c.bc_lo[a] < 0 || c.bc_lo[a] > top || c.bc_hi[a] < 0 || c.bc_hi[a] > top) {
+      snprintf(b, sizeof b, "axis %d: boundary codes are 0 periodic, 1 outflow, 2 reflect (and 3 halo on z)", a);
+      why = b;
+      return -1;
     }
   }
   if (c.n[1] == 1 && c.n[2] > 1) { why = "a collapsed y axis with z cells: collapse z first (2D grids are x-y)"; return -1; }
   const int nd = ndim_of(c);
+  if ((c.bc_lo[2] == 3 || c.bc_hi[2] == 3) && nd != 3) { why = "halo faces (code 3) are z faces of a 3D slab"; return -1; }
+  if ((c.bc_lo[2] == 3) != (c.bc_hi[2] == 3) && (c.bc_lo[2] == 0 || c.bc_hi[2] == 0)) {
+    why = "a periodic z face needs a periodic partner: use halo faces on both sides of a slab of a periodic grid";
+    return -1;
+  }
   const int need = shz::sweep_min_cells(c.recon);
   for (int a = 0; a < nd; a++)
     if (c.n[a] < need) { snprintf(b, sizeof b, "axis %d has %d cells; this reconstruction needs %d", a, c.n[a], need); why = b; return -1; }
@@ -284,6 +298,11 @@ int shz_create(const shz_config* cfg, shz_sim** out) {
   s->ncell = (size_t)cfg->n[0] * cfg->n[1] * cfg->n[2];
   fill_kparams(s);
   const size_t bytes = s->ncell * sizeof(float4);
+  const size_t plane = (size_t)cfg->n[0] * cfg->n[1];
+  const int hz = halo_planes(*cfg);
+  s->halo_lo = cfg->bc_lo[2] == 3 ? hz : 0;
+  s->halo_hi = cfg->bc_hi[2] == 3 ? hz : 0;
+  const size_t abytes = bytes + (size_t)(s->halo_lo + s->halo_hi) * plane * sizeof(float4);
   auto bail = [&](int code) {
     std::string m = s->err;
     shz_destroy(s);
@@ -292,11 +311,17 @@ int shz_create(const shz_config* cfg, shz_sim** out) {
   e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) { fail(s, SHZ_E_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e)); return bail(SHZ_E_CUDA); }
   for (int p = 0; p < 2; p++) {
-    if (cudaMalloc(&s->u1[p], bytes) != cudaSuccess || cudaMalloc(&s->u2[p], bytes) != cudaSuccess) {
+    if (cudaMalloc(&s->a1[p], abytes) != cudaSuccess || cudaMalloc(&s->a2[p], abytes) != cudaSuccess) {
       cudaGetLastError();
-      fail(s, SHZ_E_OOM, "device state of %zu cells (%.2f GB) does not fit", s->ncell, 4.0 * bytes / 1e9);
+      fail(s, SHZ_E_OOM, "device state of %zu cells (%.2f GB) does not fit", s->ncell, 4.0 * abytes / 1e9);
       return bail(SHZ_E_OOM);
     }
+    s->u1[p] = s->a1[p] + (size_t)s->halo_lo * plane;
+    s->u2[p] = s->a2[p] + (size_t)s->halo_lo * plane;
+    // (ghost planes start as zeros until the caller fills them: a state of zeros is a vacuum,
+    // which the floors keep finite)
+    cudaMemsetAsync(s->a1[p], 0, abytes, s->stream);
+    cudaMemsetAsync(s->a2[p], 0, abytes, s->stream);
   }
   const int dblocks = shz::diag_blocks(s->ncell);
   if (cudaMalloc(&s->clk, sizeof(shz::DevClock)) != cudaSuccess || cudaMalloc(&s->rates, 2 * sizeof(unsigned)) != cudaSuccess ||
@@ -306,8 +331,6 @@ int shz_create(const shz_config* cfg, shz_sim** out) {
     fail(s, SHZ_E_OOM, "clock / reduction buffers do not fit");
     return bail(SHZ_E_OOM);
   }
-  cudaMemsetAsync(s->u1[0], 0, bytes, s->stream);
-  cudaMemsetAsync(s->u2[0], 0, bytes, s->stream);
   cudaMemsetAsync(s->rates, 0, 2 * sizeof(unsigned), s->stream);
   if (write_clock(s, 0.0, 0) != 0) return bail(SHZ_E_CUDA);
   *out = s;
@@ -319,8 +342,8 @@ void shz_destroy(shz_sim* s) {
   DeviceScope ds_(s->device);
   if (s->stream) cudaStreamSynchronize(s->stream);
   for (int p = 0; p < 2; p++) {
-    if (s->u1[p]) cudaFree(s->u1[p]);
-    if (s->u2[p]) cudaFree(s->u2[p]);
+    if (s->a1[p]) cudaFree(s->a1[p]);
+    if (s->a2[p]) cudaFree(s->a2[p]);
   }
   if (s->clk) cudaFree(s->clk);
   if (s->rates) cudaFree(s->rates);
@@ -330,9 +353,12 @@ void shz_destroy(shz_sim* s) {
   delete s;
 }
 
-int shz_reset_problem(shz_sim* s, const shz_problem* prob) {
-  if (!s || !prob) return SHZ_E_CONFIG;
-  DeviceScope ds_(s->device);
+}  // extern "C"
+
+namespace {
+// The handle's planes as planes kofs.. of `prob` sampled on the grid `grid` (the handle's own
+// grid with kofs 0, or the whole grid a slab belongs to); then the clock to 0 and the rate.
+int reset_planes(shz_sim* s, const shz_config& grid, const shz_problem* prob, int kofs) {
   if (!shz::problem_known(prob->kind)) return fail(s, SHZ_E_CONFIG, "unknown problem kind %d", prob->kind);
   const int nx = s->cfg.n[0], ny = s->cfg.n[1], nz = s->cfg.n[2];
   const size_t plane = (size_t)nx * ny;
@@ -351,7 +377,7 @@ int shz_reset_problem(shz_sim* s, const shz_problem* prob) {
   for (int k0 = 0; k0 < nz && rc == 0; k0 += kstep) {
     const int k1 = std::min(nz, k0 + kstep);
     const size_t cnt = (size_t)(k1 - k0) * plane;
-    shz::problem_prims(s->cfg, *prob, k0, k1, w.data());
+    shz::problem_prims(grid, *prob, kofs + k0, kofs + k1, w.data());
     shz::prims_to_state(w.data(), s->cfg.gamma, (int64_t)cnt, h1, h2);
     cudaError_t e1 = cudaMemcpyAsync(s->u1[s->cur] + (size_t)k0 * plane, h1, cnt * sizeof(float4), cudaMemcpyHostToDevice, s->stream);
     cudaError_t e2 = cudaMemcpyAsync(s->u2[s->cur] + (size_t)k0 * plane, h2, cnt * sizeof(float4), cudaMemcpyHostToDevice, s->stream);
@@ -364,6 +390,26 @@ int shz_reset_problem(shz_sim* s, const shz_problem* prob) {
   if (rc) return rc;
   if ((rc = write_clock(s, 0.0, 0))) return rc;
   return refresh_rate(s);
+}
+}  // namespace
+
+extern "C" {
+
+int shz_reset_problem(shz_sim* s, const shz_problem* prob) {
+  if (!s || !prob) return SHZ_E_CONFIG;
+  DeviceScope ds_(s->device);
+  return reset_planes(s, s->cfg, prob, 0);
+}
+
+int shz_reset_problem_slab(shz_sim* s, const shz_config* grid, const shz_problem* prob, int32_t k0) {
+  if (!s || !grid || !prob) return SHZ_E_CONFIG;
+  DeviceScope ds_(s->device);
+  if (grid->n[0] != s->cfg.n[0] || grid->n[1] != s->cfg.n[1] || grid->dx != s->cfg.dx)
+    return fail(s, SHZ_E_CONFIG, "the whole grid must have the slab's nx, ny and dx");
+  if (k0 < 0 || (int64_t)k0 + s->cfg.n[2] > grid->n[2])
+    return fail(s, SHZ_E_CONFIG, "planes %d..%d are not planes of the whole grid (nz %d)", k0, k0 + s->cfg.n[2] - 1,
+                grid->n[2]);
+  return reset_planes(s, *grid, prob, k0);
 }
 
 int shz_set_state(shz_sim* s, const float* u1, const float* u2, size_t ncell) {
@@ -521,6 +567,43 @@ int shz_state_device(shz_sim* s, void** u1, void** u2) {
   DeviceScope ds_(s->device);
   *u1 = s->u1[s->cur];
   *u2 = s->u2[s->cur];
+  return 0;
+}
+
+int shz_halo_depth(const shz_sim* s, int32_t* planes) {
+  if (!s || !planes) return SHZ_E_CONFIG;
+  *planes = halo_planes(s->cfg);
+  return 0;
+}
+
+int shz_halo_device(shz_sim* s, int32_t side, void** inner_u1, void** inner_u2, void** ghost_u1, void** ghost_u2,
+                    size_t* bytes) {
+  if (!s || (side != 0 && side != 1) || !inner_u1 || !inner_u2 || !ghost_u1 || !ghost_u2 || !bytes) return SHZ_E_CONFIG;
+  const int depth = side == 0 ? s->halo_lo : s->halo_hi;
+  if (depth == 0) return fail(s, SHZ_E_CONFIG, "z face %d is not a halo face (code 3)", side);
+  const size_t plane = (size_t)s->cfg.n[0] * s->cfg.n[1];
+  const size_t nz = (size_t)s->cfg.n[2];
+  if (nz < (size_t)depth) return fail(s, SHZ_E_CONFIG, "the slab has fewer planes than its halo");
+  // inner: the `depth` planes next to the face; ghost: the `depth` stored planes beyond it
+  const size_t in0 = side == 0 ? 0 : (nz - depth) * plane;
+  const ptrdiff_t g0 = side == 0 ? -(ptrdiff_t)(depth * plane) : (ptrdiff_t)(nz * plane);
+  *inner_u1 = s->u1[s->cur] + in0;
+  *inner_u2 = s->u2[s->cur] + in0;
+  *ghost_u1 = s->u1[s->cur] + g0;
+  *ghost_u2 = s->u2[s->cur] + g0;
+  *bytes = (size_t)depth * plane * sizeof(float4);
+  return 0;
+}
+
+int shz_rate_device(shz_sim* s, void** rate) {
+  if (!s || !rate) return SHZ_E_CONFIG;
+  *rate = s->rates + s->slot;
+  return 0;
+}
+
+int shz_stream(shz_sim* s, void** stream) {
+  if (!s || !stream) return SHZ_E_CONFIG;
+  *stream = (void*)s->stream;
   return 0;
 }
 

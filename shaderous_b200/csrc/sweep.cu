@@ -68,14 +68,16 @@ __device__ __forceinline__ void load_w_plane(const KParams& P, const float4* __r
                                              int x0, int y0, int plane, float* __restrict__ sWb) {
   using G = Geo<DIM, RECON>;
   float fz = 1.f;
-  const int gz = (DIM == 3) ? bc_map(plane, P.n[2], P.bc_lo[2], P.bc_hi[2], fz) : 0;
-  const size_t zoff = (size_t)gz * P.n[1] * P.n[0];
+  // (a halo face's ghost planes are stored beyond the slab: read as they are)
+  const bool zhalo = (DIM == 3) && ((plane < 0 && P.bc_lo[2] == BC_HALO) || (plane >= P.n[2] && P.bc_hi[2] == BC_HALO));
+  const int gz = (DIM == 3) ? (zhalo ? plane : bc_map(plane, P.n[2], P.bc_lo[2], P.bc_hi[2], fz)) : 0;
+  const ptrdiff_t zoff = (ptrdiff_t)gz * P.n[1] * P.n[0];
   for (int idx = threadIdx.x; idx < G::WN; idx += G::NT) {
     const int lx = idx % G::WX, ly = idx / G::WX;
     float fx, fy = 1.f;
     const int gx = bc_map(x0 - G::H + lx, P.n[0], P.bc_lo[0], P.bc_hi[0], fx);
     const int gy = (DIM >= 2) ? bc_map(y0 - G::H + ly, P.n[1], P.bc_lo[1], P.bc_hi[1], fy) : 0;
-    const size_t o = zoff + (size_t)gy * P.n[0] + gx;
+    const ptrdiff_t o = zoff + (ptrdiff_t)gy * P.n[0] + gx;
     const float4 a = __ldg(u1 + o), b = __ldg(u2 + o);
     float w[6];
     prim6_from_cons(a, b, P, fx, fy, fz, w);
@@ -215,8 +217,8 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, REC
     if constexpr (DIM == 3) {
       // The z ghost planes (outflow / reflect) need only their edges toward the domain, at the
       // ghost position; their half-step state is that of the adjacent inner plane.
-      const bool zg_lo = j == -1 && P.bc_lo[2] != 0;
-      const bool zg_hi = j == nz && P.bc_hi[2] != 0;
+      const bool zg_lo = j == -1 && bc_inner(P.bc_lo[2]);
+      const bool zg_hi = j == nz && bc_inner(P.bc_hi[2]);
       if (zg_lo || zg_hi) {
         float c[7], m[7], p[7], m2[7], p2[7], su[6], sd[6];
         read_w<DIM, RECON>(sWj, wx, wy, c);
@@ -316,7 +318,7 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, REC
     }
     if constexpr (DIM == 3) {
       // plane 0 stands in for the lower z ghost: its face state toward plane 0
-      if (j == 0 && P.bc_lo[2] != 0) {
+      if (j == 0 && bc_inner(P.bc_lo[2])) {
         Pred g = pr;
         if (P.bc_lo[2] == 2) g.q[3] = -g.q[3];
         face_state(g, gsu, 1.f, zhi_prev);

@@ -243,6 +243,33 @@ class Sim:
         self._ok(self._lib.shz_state_device(self._h, C.byref(a), C.byref(b)))
         return a.value, b.value
 
+    # -- slabs of a grid split along z (SHZ_BC_HALO faces) -----------------------------------------
+    def reset_slab(self, grid: Config, prob: Problem, k0: int) -> None:
+        """Load planes k0.. of `prob` sampled on the whole grid `grid`; the clock goes to 0."""
+        self._ok(self._lib.shz_reset_problem_slab(self._h, C.byref(grid.to_c()), C.byref(prob.to_c()), int(k0)))
+
+    def halo_depth(self) -> int:
+        d = C.c_int32()
+        self._ok(self._lib.shz_halo_depth(self._h, C.byref(d)))
+        return d.value
+
+    def halo_device(self, side: int) -> tuple[int, int, int, int, int]:
+        """(inner u1, inner u2, ghost u1, ghost u2, bytes) of z face `side` of the current state."""
+        p = [C.c_void_p() for _ in range(4)]
+        b = C.c_size_t()
+        self._ok(self._lib.shz_halo_device(self._h, int(side), *[C.byref(x) for x in p], C.byref(b)))
+        return p[0].value, p[1].value, p[2].value, p[3].value, b.value
+
+    def rate_device(self) -> int:
+        p = C.c_void_p()
+        self._ok(self._lib.shz_rate_device(self._h, C.byref(p)))
+        return p.value
+
+    def stream_handle(self) -> int:
+        p = C.c_void_p()
+        self._ok(self._lib.shz_stream(self._h, C.byref(p)))
+        return p.value or 0
+
     def profile(self, n: int) -> dict:
         """Device time of n steps and of their sweeps alone, by CUDA events on the handle's
         stream (the reference's Sim.profile, src/sim.ts:3541)."""
