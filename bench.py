@@ -7,8 +7,10 @@ gamma = 5/3), PPM + HLLC, float32 state, CFL 0.4 — the configuration the headl
 host in float64 and rounded once to float32.
 
   value   zone-updates/s of `--steps` steps with the state resident in HBM, timed with CUDA events
-          on the library's stream (max over ranks; N ranks run N replicas: the single-grid step is
-          not sharded, each GPU advances its own grid).
+          on the library's stream. With N > 1 ranks (torchrun), weak scaling: one periodic grid of
+          512 x 512 x 512N cells split into z-slabs of 512^3, one per GPU, with NCCL halo exchange
+          and a max all-reduce of the rate before every step (shaderous_b200.dist); the time is the
+          slowest rank's.
   e2e     the same metric through the C ABI with host buffers: upload of the state from pinned
           host memory, the configuration's full run of 200 steps with the clock read back between
           batches (shz_run), download of the final state.
@@ -60,6 +62,8 @@ def parse():
     ap.add_argument("--section", choices=["all", "amr", "serving"], default="all",
                     help="amr / serving: only that measurement, printed as its own JSON line")
     ap.add_argument("--amr-variant", choices=["both", "spec", "developed"], default="both")
+    ap.add_argument("--slabs", action="store_true",
+                    help="the z-slab driver also at N = 1 (one periodic slab exchanging with itself)")
     return ap.parse_args()
 
 
@@ -264,6 +268,98 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def headline(args, world, value, total_ms, sweep_ms, ncell, launches, clocks, e2e_value, e2e_s, config):
+    """The JSON line: the metric, the sweep's roofline (ncell cells per GPU), e2e, launches, clocks."""
+    sweep_avg_s = sweep_ms / args.steps / 1000.0
+    peak, peak_kind = measured_peaks()
+    achieved = BYTES_PER_ZU * ncell / sweep_avg_s / 1e9
+    tr = profile_traffic(args.recon)
+    state_bytes = 2 * ncell * 16
+    e2e_steps = args.e2e_steps
+    return {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic", "config": config,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": (tr * ncell) if tr else None, "kernel": "sweep_kernel",
+                     "algorithmic_bytes_per_zu": BYTES_PER_ZU, "peak_source": f"{peak_kind} hbm_gbs",
+                     "sweep_ms_per_step": sweep_ms / args.steps},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": state_bytes / e2e_steps,
+                "d2h_bytes_per_step": (state_bytes + 64 * math.ceil(math.log2(e2e_steps + 1))) / e2e_steps,
+                "steps": e2e_steps, "seconds": e2e_s},
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+
+
+def run_slabs(args, rank, world, local):
+    """N GPUs, weak scaling: one periodic Taylor-Green grid of n x n x (n N) cells on
+    [0,2pi]^2 x [0,2pi N] (the vortex repeated N times along z), split into N z-slabs of n^3, one
+    per rank (shaderous_b200.dist.SlabSim): before every step NCCL send/recv fills each slab's halo
+    planes and a max all-reduce of the rate gives every slab the same dt."""
+    import torch
+    import torch.distributed as dist
+
+    from shaderous_b200.dist import SlabSim, max_over_ranks
+
+    cfg, prob = workload(args.n, args.recon)
+    cfg.n = (args.n, args.n, args.n * world)
+    cfg.device = local
+    dev = f"cuda:{local}"
+    sl = SlabSim(cfg, device=local)
+    sl.reset(prob)
+    ncell_local = sl.sim.ncell
+    total_cells = ncell_local * world
+
+    sl.step(max(args.warmup, 1))  # warm-up (the first step tunes the sweep's launch shape)
+    sl.sync()
+    dist.barrier()
+    launches0 = sl.sim.kernel_launches
+    visible = [v for v in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if v.strip()]
+    gpu_index = visible[local] if local < len(visible) else local
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(gpu_index) as clocks:
+        torch.cuda.synchronize()
+        e0.record(sl.stream)
+        sl.step(args.steps)
+        e1.record(sl.stream)
+        e1.synchronize()
+    step_ms = max_over_ranks(e0.elapsed_time(e1), device=dev)
+    launches = sl.sim.kernel_launches - launches0
+    value = total_cells * args.steps / (step_ms / 1000.0)
+    # the sweep alone (clock + sweep launches, no exchange) for the kernel's roofline
+    prof = sl.sim.profile(args.steps)
+    sweep_ms = max_over_ranks(prof["sweep_ms"], device=dev)
+
+    # end to end: each rank's slab from pinned host memory, steps with exchanges, back to the host
+    u1_0, u2_0 = sl.read_state()
+    h_in1 = torch.from_numpy(u1_0).pin_memory()
+    h_in2 = torch.from_numpy(u2_0).pin_memory()
+    h_out1 = torch.empty_like(h_in1).pin_memory()
+    h_out2 = torch.empty_like(h_in2).pin_memory()
+    del u1_0, u2_0
+    lib = sl.sim._lib
+    dist.barrier()
+    t0 = time.perf_counter()
+    sl.sim._ok(lib.shz_set_state(sl.sim._h, h_in1.data_ptr(), h_in2.data_ptr(), ncell_local))
+    sl.step(args.e2e_steps)
+    sl.sim._ok(lib.shz_get_state(sl.sim._h, h_out1.data_ptr(), h_out2.data_ptr(), ncell_local))
+    e2e_s = max_over_ranks(time.perf_counter() - t0, device=dev)
+    if not np.isfinite(h_out1[:: max(1, ncell_local // 4096)].numpy()).all():
+        raise RuntimeError("non-finite state after the end-to-end run")
+    sl.destroy()
+    return {"value": value, "total_ms": step_ms, "sweep_ms": sweep_ms, "launches": launches, "clocks": clocks.summary(),
+            "ncell": ncell_local, "total_cells": total_cells,
+            "e2e_value": total_cells * args.e2e_steps / e2e_s, "e2e_s": e2e_s,
+            "config": {"workload": f"taylor-green {args.n}x{args.n}x{args.n * world} periodic [0,2pi]^2 x [0,2pi*{world}]"
+                                   f" (the vortex repeated along z), rho 1, p0 100, gamma 5/3, {args.recon}+hllc, cfl 0.4",
+                       "cells": total_cells, "cells_per_gpu": ncell_local,
+                       "parallelism": f"z-slabs x{world}: NCCL send/recv halo planes + max all-reduce of the rate per step",
+                       "l2": f"inputs larger than L2 ({2 * ncell_local * 16 / 1e9:.2f} GB state per GPU vs "
+                             f"{L2_BYTES / 1e6:.0f} MB L2)"}}
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -287,17 +383,26 @@ def main():
     import torch
 
     dist = None
-    if world > 1:
+    if world > 1 or args.slabs:
         import datetime
 
         import torch.distributed as dist
 
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        os.environ.setdefault("MASTER_PORT", "29511")
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    import ctypes as C
+        dist.init_process_group("nccl", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    if world > 1 or args.slabs:
+        r = run_slabs(args, rank, world, local)
+        dist.barrier()
+        dist.destroy_process_group()
+        if rank == 0:
+            print(json.dumps(headline(args, world, r["value"], r["total_ms"], r["sweep_ms"], r["ncell"], r["launches"],
+                                      r["clocks"], r["e2e_value"], r["e2e_s"], r["config"])), flush=True)
+        return
 
     from shaderous_b200 import Sim, problem_prims, prims_to_state
-    from shaderous_b200 import _abi
 
     cfg, prob = workload(args.n, args.recon)
     cfg.device = local
@@ -324,10 +429,6 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms, sweep_ms = float(t[0]), float(t[1])
     value = ncell * args.steps * world / (total_ms / 1000.0)
-    sweep_avg_s = sweep_ms / args.steps / 1000.0
-    peak, peak_kind = measured_peaks()
-    achieved = BYTES_PER_ZU * ncell / sweep_avg_s / 1e9
-    tr = profile_traffic(args.recon)
 
     # end to end through the C ABI with pinned host buffers
     u1_0, u2_0 = prims_to_state(problem_prims(cfg, prob), cfg.gamma)
@@ -351,7 +452,6 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t[0])
     e2e_value = ncell * e2e_steps * world / e2e_s
-    state_bytes = 2 * ncell * 16
     if not np.isfinite(h_out1[:: max(1, ncell // 4096)].numpy()).all():
         raise RuntimeError("non-finite state after the end-to-end run")
 
@@ -372,24 +472,11 @@ def main():
         dist.destroy_process_group()
     if rank != 0:
         return
-    line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"taylor-green {args.n}^3 periodic [0,2pi]^3, rho 1, p0 100, gamma 5/3, "
-                               f"{args.recon}+hllc, cfl 0.4",
-                   "cells": ncell, "parallelism": f"replicas x{world}" if world > 1 else "single grid",
-                   "l2": f"inputs larger than L2 ({2 * ncell * 16 / 1e9:.2f} GB state vs {L2_BYTES / 1e6:.0f} MB L2)"},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": (tr * ncell) if tr else None, "kernel": "sweep_kernel",
-                     "algorithmic_bytes_per_zu": BYTES_PER_ZU, "peak_source": f"{peak_kind} hbm_gbs",
-                     "sweep_ms_per_step": sweep_ms / args.steps},
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": state_bytes / e2e_steps,
-                "d2h_bytes_per_step": (state_bytes + 64 * math.ceil(math.log2(e2e_steps + 1))) / e2e_steps,
-                "steps": e2e_steps, "seconds": e2e_s},
-        "gpu_launches": launches,
-        "clocks": clocks.summary(),
-    }
+    config = {"workload": f"taylor-green {args.n}^3 periodic [0,2pi]^3, rho 1, p0 100, gamma 5/3, "
+                          f"{args.recon}+hllc, cfl 0.4",
+              "cells": ncell, "parallelism": "single grid",
+              "l2": f"inputs larger than L2 ({2 * ncell * 16 / 1e9:.2f} GB state vs {L2_BYTES / 1e6:.0f} MB L2)"}
+    line = headline(args, world, value, total_ms, sweep_ms, ncell, launches, clocks.summary(), e2e_value, e2e_s, config)
     if cpu:
         line["cpu_baseline"] = cpu
     if amr:
