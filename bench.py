@@ -62,12 +62,15 @@ def parse():
     ap.add_argument("--section", choices=["all", "amr", "serving"], default="all",
                     help="amr / serving: only that measurement, printed as its own JSON line")
     ap.add_argument("--amr-variant", choices=["both", "spec", "developed"], default="both")
+    ap.add_argument("--amr-cap", type=int, default=26000, help="block slots of the AMR runs")
+    ap.add_argument("--profile-window", action="store_true",
+                    help="AMR section: bracket one step after the warm-up with cudaProfilerStart/Stop")
     ap.add_argument("--slabs", action="store_true",
                     help="the z-slab driver also at N = 1 (one periodic slab exchanging with itself)")
     return ap.parse_args()
 
 
-def amr_sedov(levels=4, nr=8, radius_cells=3.5, steps=24, cap=26000, grown=False):
+def amr_sedov(levels=4, nr=8, radius_cells=3.5, steps=24, cap=26000, grown=False, profile_window=False):
     """3D Sedov blast on the block grid: 16^3-cell blocks, levels 0-levels above nr^3 roots (finest
     nr * 16 << levels cells per side), E = 1 spread over the finest cells within radius_cells of
     the centre, Löhner refinement above 0.1 (below 0.05 merges), a refinement check every 8 steps.
@@ -88,6 +91,16 @@ def amr_sedov(levels=4, nr=8, radius_cells=3.5, steps=24, cap=26000, grown=False
         a.reset(prob)
         t_init = time.perf_counter() - t0
         a.profile(8)  # warm-up, including one refinement check
+        if profile_window:
+            # one graph-replayed step between cudaProfilerStart/Stop, for `ncu --profile-from-start off`
+            import torch
+
+            torch.cuda.synchronize()
+            torch.cuda.profiler.start()
+            a.step(1)
+            a.diagnostics()
+            torch.cuda.synchronize()
+            torch.cuda.profiler.stop()
         n0 = len(a.leaves()[0])
         l0 = a.kernel_launches
         prof = a.profile(steps)
@@ -372,9 +385,10 @@ def main():
         out = {}
         if args.section == "amr":
             if args.amr_variant in ("both", "spec"):
-                out["spec"] = amr_sedov(steps=max(args.steps, 8))
+                out["spec"] = amr_sedov(steps=max(args.steps, 8), cap=args.amr_cap, profile_window=args.profile_window)
             if args.amr_variant in ("both", "developed"):
-                out["developed"] = amr_sedov(steps=max(args.steps, 8), grown=True)
+                out["developed"] = amr_sedov(steps=max(args.steps, 8), grown=True, cap=args.amr_cap,
+                                             profile_window=args.profile_window)
         else:
             out = serving(args.serve_requests)
         print(json.dumps({"section": args.section, "result": out}), flush=True)

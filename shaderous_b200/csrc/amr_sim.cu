@@ -250,9 +250,10 @@ int step_once(shz_amr* a) {
 // The refinement indicators of the current state: a fresh assemble, then the Löhner pass.
 int compute_flags(shz_amr* a) {
   AMR_CUDA(a, cudaMemsetAsync(a->rates + 2, 0, 2 * sizeof(unsigned), a->stream));
-  AMR_CUDA(a, shz::amr_launch_assemble(a->L, a->cfg.two_pass ? a->d_all : a->d_leaves,
-                                       a->cfg.two_pass ? n_all(a) : n_leaves(a), a->u1[a->cur], a->u2[a->cur],
-                                       a->rates + 2, 0, a->stream));
+  long long n = 0;
+  AMR_CUDA(a, shz::amr_assemble_tuned(a->L, a->cfg.two_pass ? a->d_all : a->d_leaves,
+                                      a->cfg.two_pass ? n_all(a) : n_leaves(a), a->u1[a->cur], a->u2[a->cur],
+                                      a->rates + 2, 0, a->stream, false, &n));
   AMR_CUDA(a, cudaMemsetAsync(a->d_flags, 0, sizeof(float) * a->cfg.cap, a->stream));
   AMR_CUDA(a, shz::amr_launch_flag(a->L, a->d_leaves, n_leaves(a), a->d_flags, a->stream));
   a->launches += 2;
