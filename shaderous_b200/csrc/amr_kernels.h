@@ -23,6 +23,9 @@ struct AmrLaunch {
   // Fine-flux buffer of the fused sweep: 2 float4 per face cell (16^(ndim-1) cells) per matched
   // face; a leaf's row holds its first entry in word 27 (-1: none).
   float4* fbuf = nullptr;
+  // Device error word the kernels set when a bounded wait runs out (tma::ERR_*); read and cleared
+  // by the host.
+  int* err = nullptr;
 };
 
 // rates: two 32-bit maxima per grid; the assemble folds the leaves' rate / dx into slot rslot.

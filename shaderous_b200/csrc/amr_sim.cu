@@ -42,6 +42,7 @@ struct shz_amr {
   unsigned* rates = nullptr;  // slots 0, 1: the steps'; 2, 3: the refinement check's
   double *diag_part = nullptr, *diag_out = nullptr;
   int* d_ghost = nullptr;
+  int* d_err = nullptr;  // the kernels' error word
   // faces matched to refined neighbours (fused sweep): (leaf slot, face, entry) triples and the
   // buffer of their mean fine fluxes, grown with the mesh
   int* d_flist = nullptr;
@@ -142,6 +143,7 @@ int upload_tables(shz_amr* a) {
     a->fine_cap = want;
   }
   a->L.fbuf = a->fbuf;
+  a->L.err = a->d_err;
   if (a->nfine > 0)
     AMR_CUDA(a, cudaMemcpyAsync(a->d_flist, a->h_flist.data(), a->h_flist.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
                                 a->stream));
@@ -154,10 +156,22 @@ int upload_tables(shz_amr* a) {
   return 0;
 }
 
+// The kernels' error word: a bounded wait inside a kernel that ran out (tma::ERR_*) fails the call.
+int check_err(shz_amr* a) {
+  int e = 0;
+  AMR_CUDA(a, cudaMemcpyAsync(&e, a->d_err, sizeof e, cudaMemcpyDeviceToHost, a->stream));
+  AMR_CUDA(a, cudaStreamSynchronize(a->stream));
+  if (e) {
+    cudaMemsetAsync(a->d_err, 0, sizeof(int), a->stream);
+    return fail(a, SHZ_E_TIMEOUT, "a kernel's bounded wait for a bulk copy ran out (code %d); the state is not valid", e);
+  }
+  return 0;
+}
+
 int read_clock(shz_amr* a, shz::DevClock* h) {
   AMR_CUDA(a, cudaMemcpyAsync(h, a->clk, sizeof *h, cudaMemcpyDeviceToHost, a->stream));
   AMR_CUDA(a, cudaStreamSynchronize(a->stream));
-  return 0;
+  return check_err(a);
 }
 
 int write_clock(shz_amr* a, double t, long long steps) {
@@ -466,6 +480,8 @@ int shz_amr_create(const shz_amr_config* cfg, shz_amr** out) {
   ok = ok && cudaMalloc(&a->diag_part, (size_t)shz::amr_diag_blocks(c.cap) * 9 * sizeof(double)) == cudaSuccess;
   ok = ok && cudaMalloc(&a->diag_out, 9 * sizeof(double)) == cudaSuccess;
   ok = ok && cudaMalloc(&a->d_ghost, (size_t)a->WN * 5 * sizeof(int)) == cudaSuccess;
+  ok = ok && cudaMalloc(&a->d_err, sizeof(int)) == cudaSuccess;
+  if (ok) ok = cudaMemset(a->d_err, 0, sizeof(int)) == cudaSuccess;
   if (!ok) {
     cudaGetLastError();
     char buf[160];
@@ -501,7 +517,7 @@ void shz_amr_destroy(shz_amr* a) {
     cudaFree(a->u2[p]);
   }
   void* bufs[] = {a->w1, a->w2, a->p1, a->p2, a->d_bt, a->d_all, a->d_leaves, a->d_rg, a->d_flags, a->d_gp,
-                  a->clk, a->rates, a->diag_part, a->diag_out, a->d_ghost, a->d_flist, a->fbuf};
+                  a->clk, a->rates, a->diag_part, a->diag_out, a->d_ghost, a->d_flist, a->fbuf, a->d_err};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (a->stream) cudaStreamDestroy(a->stream);
@@ -733,6 +749,7 @@ int shz_amr_profile(shz_amr* a, int32_t n, shz_profile_result* out) {
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (rc) return rc;
+  if ((rc = check_err(a))) return rc;
   out->steps = n;
   out->total_ms = ms;
   out->sweep_ms = ms;

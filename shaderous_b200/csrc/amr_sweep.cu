@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "amr_device.cuh"
+#include "tma.cuh"
 
 namespace shz {
 namespace amrk {
@@ -32,9 +33,15 @@ constexpr int SNT = SX * SX;      // 324 threads
 constexpr int SPN = SX * SX;      // predictor region per plane
 constexpr int SWN = PAD * PAD;    // primitive texels per plane
 
-__device__ __forceinline__ void read_w6(const float* __restrict__ plane, int x, int y, float* w) {
-#pragma unroll
-  for (int c = 0; c < 6; c++) w[c] = plane[c * SWN + (y + NG) * PAD + (x + NG)];
+
+// The seven primitives of texel l of a block's atlas (the sound speed as the atlas holds it).
+template <int DIM>
+__device__ __forceinline__ void load_w7(const float4* __restrict__ w1, const float4* __restrict__ w2, int slot, const int* l,
+                                        float* w) {
+  const size_t o = (size_t)slot * BG<DIM>::WN + wtex<DIM>(l);
+  const float4 a = __ldg(w1 + o), b = __ldg(w2 + o);
+  w[0] = a.x; w[1] = a.y; w[2] = a.z; w[3] = a.w;
+  w[4] = b.x; w[5] = b.y; w[6] = b.z;
 }
 
 template <int DIM>
@@ -78,8 +85,7 @@ __device__ __forceinline__ void predict_texel(const KParams& P, const int* __res
   }
   float c[7], sua[DIM][6], sda[DIM][6];
   float conv = 0.f, jump = 0.f;
-  load_w6<DIM>(w1, w2, slot, l, c);
-  with_cs(c, P);
+  load_w7<DIM>(w1, w2, slot, l, c);
 #pragma unroll
   for (int a = 0; a < DIM; a++) {
     float m[7], p[7];
@@ -101,8 +107,7 @@ __device__ __forceinline__ void predict_texel(const KParams& P, const int* __res
     int lm[3] = {l0[0], l0[1], l0[2]}, lp[3] = {l0[0], l0[1], l0[2]};
     lm[axis] -= 1;
     lp[axis] += 1;
-    load_w6<DIM>(w1, w2, slot, l0, g);
-    with_cs(g, P);
+    load_w7<DIM>(w1, w2, slot, l0, g);
     load_w6<DIM>(w1, w2, slot, lm, m);
     load_w6<DIM>(w1, w2, slot, lp, p);
     axis_edges<R, ISEN>(m, m, g, p, p, P.inv_gamma, su, sd);
@@ -200,21 +205,34 @@ __global__ void __launch_bounds__(NT) amr_fine_flux(const KParams* __restrict__ 
   }
 }
 
-// Shared memory of the block sweep, in floats.
-constexpr int SW_RING = 3 * 6 * SWN;  // three planes of primitives
+// Shared memory of the block sweep, in floats. The primitive planes are a ring of four, each the
+// plane's w1 texels then its w2 texels (float4, as in the atlas), filled by bulk copies (TMA): the
+// march reads planes j - 1, j, j + 1 while plane j + 2 is in flight.
+constexpr int RING = 4;
+constexpr int SW_PLANE = 2 * 4 * SWN;    // floats of one staged plane (w1 and w2)
+constexpr int SW_RING = RING * SW_PLANE;
 constexpr int SW_FACE = 2 * 7 * SPN;  // x and y upper face states of a plane
 constexpr int SW_FLUX = 2 * 8 * SPN;  // x and y lower-face fluxes of a plane (also the half-step exchange)
 constexpr int SW_KEEP = 8 * SPN;      // z boundary ghosts: a plane's half steps or the ghost's increments
 constexpr size_t SWEEP_SMEM = (size_t)(SW_RING + SW_FACE + SW_FLUX + SW_KEEP) * sizeof(float);
+constexpr uint32_t PLANE_BYTES = SWN * sizeof(float4);  // one of w1 / w2 of a plane: 6400 B
+
+// Texel (x, y) of a staged plane: its seven primitives (the sound speed as the atlas holds it).
+__device__ __forceinline__ void read_w7(const float4* __restrict__ plane, int x, int y, float* w) {
+  const int t = (y + NG) * PAD + (x + NG);
+  const float4 a = plane[t], b = plane[SWN + t];
+  w[0] = a.x; w[1] = a.y; w[2] = a.z; w[3] = a.w;
+  w[4] = b.x; w[5] = b.y; w[6] = b.z;
+}
 
 template <int DIM, int R, bool ISEN>
 __global__ void __maxnreg__(80)
     amr_sweep(const KParams* __restrict__ gp, const int* __restrict__ bt, const int* __restrict__ list, int n,
               const float4* __restrict__ u1, const float4* __restrict__ u2, const float4* __restrict__ w1,
               const float4* __restrict__ w2, float4* __restrict__ o1, float4* __restrict__ o2,
-              const DevClock* __restrict__ clks, const float4* __restrict__ fbuf) {
+              const DevClock* __restrict__ clks, const float4* __restrict__ fbuf, int* __restrict__ err) {
   constexpr int FC = DIM == 3 ? BS * BS : BS;  // cells of a face
-  extern __shared__ __align__(16) float smem[];
+  extern __shared__ __align__(128) float smem[];
   float* sW = smem;
   float* sFace = sW + SW_RING;
   float* sFlux = sFace + SW_FACE;
@@ -227,7 +245,18 @@ __global__ void __maxnreg__(80)
   const bool row_t = ty >= 1 && ty <= BS;
   const bool col_t = tx >= 1 && tx <= BS;
   const bool tile_t = row_t && col_t;
-  auto ring = [&](int plane) -> float* { return sW + ((plane + 6) % 3) * 6 * SWN; };
+  auto ring = [&](int plane) -> const float4* {
+    return reinterpret_cast<const float4*>(sW + (size_t)((plane + 8) & (RING - 1)) * SW_PLANE);
+  };
+  // One mbarrier per ring slot; the phase each thread expects next, per slot (uniform across the
+  // CTA: every thread waits for every plane once); slots with a copy in flight.
+  __shared__ __align__(8) uint64_t sBar[RING];
+  uint32_t phase = 0, pending = 0;
+  if (tid == 0) {
+    for (int s = 0; s < RING; s++) tma::mbar_init(&sBar[s], 1);
+    tma::fence_mbar_init();
+  }
+  __syncthreads();
 
   for (int i = blockIdx.x; i < n; i += gridDim.x) {
     const int slot = __ldg(list + i);
@@ -287,55 +316,79 @@ __global__ void __maxnreg__(80)
     float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     float ph_prev = 0.f;
 
-    auto load_plane = [&](int pl) {
-      float* dst = ring(pl);
-      const size_t zb = (size_t)slot * BG<DIM>::WN + (DIM == 3 ? (size_t)(pl + NG) * SWN : 0);
-      for (int t = tid; t < SWN; t += SNT) {
-        const float4 a = __ldg(w1 + zb + t), b = __ldg(w2 + zb + t);
-        dst[0 * SWN + t] = a.x;
-        dst[1 * SWN + t] = a.y;
-        dst[2 * SWN + t] = a.z;
-        dst[3 * SWN + t] = a.w;
-        dst[4 * SWN + t] = b.x;
-        dst[5 * SWN + t] = b.y;
+    // Plane pl (-2 .. 17) of this block's atlas into its ring slot: issued by one thread, after a
+    // barrier that follows every thread's last read of the slot (the plane four before).
+    auto issue = [&](int pl) {
+      const int s = (pl + 8) & (RING - 1);
+      if (tid == 0) {
+        const size_t zb = (size_t)slot * BG<DIM>::WN + (DIM == 3 ? (size_t)(pl + NG) * SWN : 0);
+        float4* dst = reinterpret_cast<float4*>(sW + (size_t)s * SW_PLANE);
+        tma::fence_proxy_async();
+        tma::mbar_expect_tx(&sBar[s], 2 * PLANE_BYTES);
+        tma::bulk_g2s(dst, w1 + zb, PLANE_BYTES, &sBar[s]);
+        tma::bulk_g2s(dst + SWN, w2 + zb, PLANE_BYTES, &sBar[s]);
       }
+      pending |= 1u << s;
+    };
+    // Wait for plane pl; CTA-uniformly false if the copy did not complete in time.
+    auto arrived = [&](int pl) -> bool {
+      const int s = (pl + 8) & (RING - 1);
+      const bool ok = tma::mbar_wait(&sBar[s], (phase >> s) & 1u, tma::WAIT_LIMIT);
+      phase ^= 1u << s;
+      pending &= ~(1u << s);
+      return !__syncthreads_or(!ok);
+    };
+    // A copy that never completed: record it, let the others land (bounded), leave.
+    auto give_up = [&]() {
+      if (tid == 0 && err) atomicExch(err, tma::ERR_TMA_TIMEOUT);
+      for (int s = 0; s < RING; s++)
+        if (pending & (1u << s)) tma::mbar_wait(&sBar[s], (phase >> s) & 1u, tma::WAIT_LIMIT);
     };
     if constexpr (DIM == 3) {
-      load_plane(-2);
-      load_plane(-1);
+      issue(-2);
+      issue(-1);
+      issue(0);
+      if (!arrived(-2) || !arrived(-1)) {
+        give_up();
+        return;
+      }
+    } else {
+      issue(0);
     }
     // 3D: planes -1 .. 16, the first and last the z ghosts; 2D: the one plane.
     const int jb = DIM == 3 ? -1 : 0, je = DIM == 3 ? BS : 0;
     for (int j = jb; j <= je; j++) {
-      load_plane(DIM == 3 ? j + 1 : 0);
-      __syncthreads();
-      const float* pj = ring(DIM == 3 ? j : 0);
+      if (DIM == 3 && j + 2 <= BS + 1) issue(j + 2);
+      if (!arrived(DIM == 3 ? j + 1 : 0)) {
+        give_up();
+        return;
+      }
+      const float4* pj = ring(DIM == 3 ? j : 0);
       const bool zghost = DIM == 3 && (j == -1 || j == BS);
       const int znb = j == -1 ? zlo_nb : zhi_nb;  // (meaningful on the z ghost planes)
 
       // the predictor at plane j
       float c[7];
-      read_w6(pj, lx, ly, c);
-      with_cs(c, P);
+      read_w7(pj, lx, ly, c);
       float su[DIM][6], sd[DIM][6];
       float conv = 0.f, jump = 0.f;
       {
         float m[7], p[7];
-        read_w6(pj, lx - 1, ly, m);
-        read_w6(pj, lx + 1, ly, p);
+        read_w7(pj, lx - 1, ly, m);
+        read_w7(pj, lx + 1, ly, p);
         axis_edges<R, ISEN>(m, m, c, p, p, P.inv_gamma, su[0], sd[0]);
         conv += p[1] - m[1];
         jump = fmaxf(jump, fabsf(p[4] - m[4]) / fminf(p[4], m[4]));
         if constexpr (DIM >= 2) {
-          read_w6(pj, lx, ly - 1, m);
-          read_w6(pj, lx, ly + 1, p);
+          read_w7(pj, lx, ly - 1, m);
+          read_w7(pj, lx, ly + 1, p);
           axis_edges<R, ISEN>(m, m, c, p, p, P.inv_gamma, su[1], sd[1]);
           conv += p[2] - m[2];
           jump = fmaxf(jump, fabsf(p[4] - m[4]) / fminf(p[4], m[4]));
         }
         if constexpr (DIM == 3) {
-          read_w6(ring(j - 1), lx, ly, m);
-          read_w6(ring(j + 1), lx, ly, p);
+          read_w7(ring(j - 1), lx, ly, m);
+          read_w7(ring(j + 1), lx, ly, p);
           axis_edges<R, ISEN>(m, m, c, p, p, P.inv_gamma, su[2], sd[2]);
           conv += p[3] - m[3];
           jump = fmaxf(jump, fabsf(p[4] - m[4]) / fminf(p[4], m[4]));
@@ -519,7 +572,8 @@ cudaError_t sweep_one(const AmrLaunch& L, const int* list, int n, const float4* 
     return e;
   }();
   if (attr != cudaSuccess) return attr;
-  k<<<grid_for(n, per_sm), amrk::SNT, amrk::SWEEP_SMEM, s>>>(L.gp, L.bt, list, n, u1, u2, L.w1, L.w2, o1, o2, clks, L.fbuf);
+  k<<<grid_for(n, per_sm), amrk::SNT, amrk::SWEEP_SMEM, s>>>(L.gp, L.bt, list, n, u1, u2, L.w1, L.w2, o1, o2, clks, L.fbuf,
+                                                             L.err);
   return cudaGetLastError();
 }
 }  // namespace

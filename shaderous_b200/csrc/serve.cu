@@ -63,6 +63,7 @@ struct Engine {
   shz::DevClock* d_clk = nullptr;
   unsigned* d_rates = nullptr;
   double *d_part = nullptr, *d_out = nullptr;
+  int* d_err = nullptr;  // the kernels' error word
   std::vector<int> free_slots, free_g;
   std::vector<Grid*> active;
   std::vector<int32_t> h_bt, h_list;
@@ -153,6 +154,8 @@ int engine_init(shz_server* s, Engine& e, int ndim, double budget) {
   }
   SV_CUDA(s, cudaMalloc(&e.w1, cap * e.WN * sizeof(float4)));
   SV_CUDA(s, cudaMalloc(&e.w2, cap * e.WN * sizeof(float4)));
+  SV_CUDA(s, cudaMalloc(&e.d_err, sizeof(int)));
+  SV_CUDA(s, cudaMemset(e.d_err, 0, sizeof(int)));
   SV_CUDA(s, cudaMalloc(&e.d_bt, cap * 32 * sizeof(int)));
   SV_CUDA(s, cudaMalloc(&e.d_list, cap * sizeof(int)));
   SV_CUDA(s, cudaMalloc(&e.d_glist, cap * sizeof(int)));
@@ -179,6 +182,7 @@ int engine_init(shz_server* s, Engine& e, int ndim, double budget) {
   e.L.bt = e.d_bt;
   e.L.w1 = e.w1;
   e.L.w2 = e.w2;
+  e.L.err = e.d_err;
   e.L.p1 = nullptr;  // (the fused sweep keeps no half-step atlas)
   e.L.p2 = nullptr;
   return 0;
@@ -191,7 +195,7 @@ void engine_free(Engine& e) {
     cudaFree(e.u1[p]);
     cudaFree(e.u2[p]);
   }
-  void* b[] = {e.w1, e.w2, e.d_bt, e.d_list, e.d_glist, e.d_gp, e.d_clk, e.d_rates, e.d_part, e.d_out};
+  void* b[] = {e.w1, e.w2, e.d_err, e.d_bt, e.d_list, e.d_glist, e.d_gp, e.d_clk, e.d_rates, e.d_part, e.d_out};
   for (void* x : b)
     if (x) cudaFree(x);
   if (e.stream) cudaStreamDestroy(e.stream);
@@ -464,8 +468,16 @@ int round_once(shz_server* s) {
       stage_grid(s, *G);
       break;
     }
-  for (Engine& e : s->e)
-    if (e.stream) SV_CUDA(s, cudaStreamSynchronize(e.stream));
+  for (Engine& e : s->e) {
+    if (!e.stream) continue;
+    SV_CUDA(s, cudaStreamSynchronize(e.stream));
+    int err = 0;
+    SV_CUDA(s, cudaMemcpy(&err, e.d_err, sizeof err, cudaMemcpyDeviceToHost));
+    if (err) {
+      cudaMemset(e.d_err, 0, sizeof(int));
+      return fail(s, SHZ_E_TIMEOUT, "a kernel's bounded wait for a bulk copy ran out (code %d)", err);
+    }
+  }
   s->rounds++;
   for (Engine& e : s->e) {
     std::vector<Grid*> done;
