@@ -32,6 +32,8 @@ struct shz_sim {
   float4* a1[2] = {nullptr, nullptr};  // the allocations: halo planes below, the grid, halo planes above
   float4* a2[2] = {nullptr, nullptr};
   int halo_lo = 0, halo_hi = 0;        // stored ghost planes below and above (z faces of code 3)
+  shz::SweepMaps maps[2];              // 3D: tensor maps of each parity for the sweep's TMA staging
+  int* d_err = nullptr;                // the kernels' error word (a bounded wait that ran out)
   int cur = 0;
   shz::DevClock* clk = nullptr;
   unsigned* rates = nullptr;  // two slots
@@ -163,10 +165,22 @@ int write_clock(shz_sim* s, double t, long long steps) {
   return 0;
 }
 
+// The kernels' error word: a bounded wait inside the sweep that ran out fails the call.
+int check_err(shz_sim* s) {
+  int e = 0;
+  CUDA_OR_FAIL(s, cudaMemcpyAsync(&e, s->d_err, sizeof e, cudaMemcpyDeviceToHost, s->stream));
+  CUDA_OR_FAIL(s, cudaStreamSynchronize(s->stream));
+  if (e) {
+    cudaMemsetAsync(s->d_err, 0, sizeof(int), s->stream);
+    return fail(s, SHZ_E_TIMEOUT, "the sweep's bounded wait for a bulk copy ran out (code %d); the state is not valid", e);
+  }
+  return 0;
+}
+
 int read_clock(shz_sim* s, shz::DevClock* h) {
   CUDA_OR_FAIL(s, cudaMemcpyAsync(h, s->clk, sizeof *h, cudaMemcpyDeviceToHost, s->stream));
   CUDA_OR_FAIL(s, cudaStreamSynchronize(s->stream));
-  return 0;
+  return check_err(s);
 }
 
 // The rate maximum of the current state into the slot the next clock kernel reads.
@@ -200,7 +214,7 @@ int tuned_step(shz_sim* s) {
   CUDA_OR_FAIL(s, cudaStreamSynchronize(s->stream));
   auto launch = [&](const shz::tune::Choice& c) {
     return shz::launch_sweep(s->kp, s->ndim, s->cfg.recon, s->cfg.isentropic != 0, s->u1[s->cur], s->u2[s->cur],
-                             s->u1[1 - s->cur], s->u2[1 - s->cur], s->clk, s->rates + (s->slot ^ 1), s->stream, c.tz);
+                             s->u1[1 - s->cur], s->u2[1 - s->cur], s->clk, s->rates + (s->slot ^ 1), s->stream, c.tz, &s->maps[s->cur], s->d_err);
   };
   if (h.held) {
     CUDA_OR_FAIL(s, launch(shz::tune::Choice{}));
@@ -233,7 +247,7 @@ int enqueue_steps(shz_sim* s, int n) {
     CUDA_OR_FAIL(s, shz::launch_clock(s->clk, s->rates, s->slot, s->stream));
     CUDA_OR_FAIL(s, shz::launch_sweep(s->kp, s->ndim, s->cfg.recon, s->cfg.isentropic != 0, s->u1[s->cur], s->u2[s->cur],
                                       s->u1[1 - s->cur], s->u2[1 - s->cur], s->clk, s->rates + (s->slot ^ 1), s->stream,
-                                      sweep_tz(s)));
+                                      sweep_tz(s), &s->maps[s->cur], s->d_err));
     s->launches += 2;
     s->cur ^= 1;
     s->slot ^= 1;
@@ -318,13 +332,17 @@ int shz_create(const shz_config* cfg, shz_sim** out) {
     }
     s->u1[p] = s->a1[p] + (size_t)s->halo_lo * plane;
     s->u2[p] = s->a2[p] + (size_t)s->halo_lo * plane;
+    if (s->ndim == 3)
+      shz::encode_sweep_maps(&s->maps[p], s->a1[p], s->a2[p], cfg->n[0], cfg->n[1],
+                             cfg->n[2] + s->halo_lo + s->halo_hi, s->halo_lo, cfg->recon);
     // (ghost planes start as zeros until the caller fills them: a state of zeros is a vacuum,
     // which the floors keep finite)
     cudaMemsetAsync(s->a1[p], 0, abytes, s->stream);
     cudaMemsetAsync(s->a2[p], 0, abytes, s->stream);
   }
   const int dblocks = shz::diag_blocks(s->ncell);
-  if (cudaMalloc(&s->clk, sizeof(shz::DevClock)) != cudaSuccess || cudaMalloc(&s->rates, 2 * sizeof(unsigned)) != cudaSuccess ||
+  if (cudaMalloc(&s->d_err, sizeof(int)) != cudaSuccess || cudaMemset(s->d_err, 0, sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&s->clk, sizeof(shz::DevClock)) != cudaSuccess || cudaMalloc(&s->rates, 2 * sizeof(unsigned)) != cudaSuccess ||
       cudaMalloc(&s->diag_part, (size_t)dblocks * shz::DIAG_VALUES * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&s->diag_out, shz::DIAG_VALUES * sizeof(double)) != cudaSuccess) {
     cudaGetLastError();
@@ -345,6 +363,7 @@ void shz_destroy(shz_sim* s) {
     if (s->a1[p]) cudaFree(s->a1[p]);
     if (s->a2[p]) cudaFree(s->a2[p]);
   }
+  if (s->d_err) cudaFree(s->d_err);
   if (s->clk) cudaFree(s->clk);
   if (s->rates) cudaFree(s->rates);
   if (s->diag_part) cudaFree(s->diag_part);
@@ -628,7 +647,7 @@ int shz_profile(shz_sim* s, int32_t n, shz_profile_result* out) {
     if (e == cudaSuccess)
       e = shz::launch_sweep(s->kp, s->ndim, s->cfg.recon, s->cfg.isentropic != 0, s->u1[s->cur], s->u2[s->cur],
                             s->u1[1 - s->cur], s->u2[1 - s->cur], s->clk, s->rates + (s->slot ^ 1), s->stream,
-                            sweep_tz(s));
+                            sweep_tz(s), &s->maps[s->cur], s->d_err);
     if (e == cudaSuccess) e = cudaEventRecord(ev[2 + 2 * i], s->stream);
     if (e != cudaSuccess) rc = fail(s, SHZ_E_CUDA, "profile step %d: %s", i, cudaGetErrorString(e));
     s->launches += 2;
@@ -638,6 +657,7 @@ int shz_profile(shz_sim* s, int32_t n, shz_profile_result* out) {
   if (rc == 0) {
     cudaError_t e = cudaEventSynchronize(ev[2 * (size_t)n]);
     if (e != cudaSuccess) rc = fail(s, SHZ_E_CUDA, "profile sync: %s", cudaGetErrorString(e));
+    if (rc == 0) rc = check_err(s);
   }
   if (rc == 0) {
     float tot = 0.f;

@@ -34,6 +34,7 @@
 #include "hydro_cell.cuh"
 #include "hydro_math.cuh"
 #include "sweep.h"
+#include "tma.cuh"
 
 namespace shz {
 
@@ -57,7 +58,12 @@ struct Geo {
   // four sub-partitions, each with a 16K-register file: two 11-warp CTAs put 6 warps on one,
   // and 6 x 32 x 80 <= 16384.
   static constexpr int MAXREG = (DIM == 1) ? 64 : 80;
-  static constexpr size_t SMEM_FLOATS = (size_t)NBUF * WC * WN + (size_t)NF * 7 * PN + (size_t)NF * 8 * PN + 32;
+  static constexpr size_t BASE_FLOATS = (size_t)NBUF * WC * WN + (size_t)NF * 7 * PN + (size_t)NF * 8 * PN + 32;
+  // 3D: a staging area for one plane's conserved state, u1 box then u2 box (float4, x fastest),
+  // filled by a tiled TMA copy; both boxes start on 128-byte boundaries.
+  static constexpr size_t STAGE_OFS = (BASE_FLOATS + 31) / 32 * 32;
+  static constexpr size_t STAGE_BOX = ((size_t)4 * WN + 31) / 32 * 32;
+  static constexpr size_t SMEM_FLOATS = (DIM == 3) ? STAGE_OFS + 2 * STAGE_BOX : BASE_FLOATS;
   static constexpr size_t SMEM_BYTES = SMEM_FLOATS * sizeof(float);
 };
 
@@ -122,10 +128,12 @@ __device__ __forceinline__ float rate_guard(float r) { return (r == r) ? r : __i
 template <int DIM, int RECON, bool ISEN>
 __global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, RECON>::MAXREG))
     sweep_kernel(const KParams P, const float4* __restrict__ u1, const float4* __restrict__ u2, float4* __restrict__ o1,
-                 float4* __restrict__ o2, const DevClock* __restrict__ clk, unsigned* __restrict__ rate_out, int tz) {
+                 float4* __restrict__ o2, const DevClock* __restrict__ clk, unsigned* __restrict__ rate_out, int tz,
+                 const __grid_constant__ CUtensorMap tm1, const __grid_constant__ CUtensorMap tm2, int zofs, int use_tma,
+                 int* __restrict__ err) {
   using G = Geo<DIM, RECON>;
   constexpr int H = G::H, ZH = G::ZH, PX = G::PX, PN = G::PN, WN = G::WN, WC = G::WC;
-  extern __shared__ __align__(16) float smem[];
+  extern __shared__ __align__(128) float smem[];
   float* sW = smem;
   float* sFace = sW + G::NBUF * WC * WN;
   float* sFlux = sFace + G::NF * 7 * PN;
@@ -200,9 +208,41 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, REC
 #pragma unroll
   for (int v = 0; v < 7; v++) zhi_prev[v] = 0.f;
 
+  // 3D columns whose stencil region lies inside the grid in x and y stage each plane's state with
+  // one tiled TMA copy per array (boxes of WX x WY float4 at (x0 - H, y0 - H), the plane mapped
+  // through the z boundary) while the previous plane is computed; columns at an x or y face keep
+  // the per-cell loads through the boundary mapping.
+  // (the staging boxes must start on 128-byte boundaries of shared memory; checked, not assumed)
+  const bool tma_tile = (DIM == 3) && use_tma && x0 - H >= 0 && x0 - H + G::WX <= nx && y0 - H >= 0 &&
+                        y0 - H + G::WY <= ny && (tma::smem_u32(smem + G::STAGE_OFS) & 127u) == 0;
+  __shared__ __align__(8) uint64_t sBarU;
+  const float4* stage1 = reinterpret_cast<const float4*>(smem + G::STAGE_OFS);
+  const float4* stage2 = reinterpret_cast<const float4*>(smem + G::STAGE_OFS + G::STAGE_BOX);
+  uint32_t uphase = 0;
+  float stage_fz = 1.f;  // velocity sign of the staged plane (a mirrored z ghost)
+  auto issue_plane = [&](int pl) {
+    float fz = 1.f;
+    const bool zhalo = (pl < 0 && P.bc_lo[2] == BC_HALO) || (pl >= nz && P.bc_hi[2] == BC_HALO);
+    const int gz = zhalo ? pl : bc_map(pl, nz, P.bc_lo[2], P.bc_hi[2], fz);
+    stage_fz = fz;
+    if (tid == 0) {
+      tma::fence_proxy_async();
+      tma::mbar_expect_tx(&sBarU, (uint32_t)(2 * WN * sizeof(float4)));
+      tma::tile3d_g2s(smem + G::STAGE_OFS, &tm1, 4 * (x0 - H), y0 - H, gz + zofs, &sBarU);
+      tma::tile3d_g2s(smem + G::STAGE_OFS + G::STAGE_BOX, &tm2, 4 * (x0 - H), y0 - H, gz + zofs, &sBarU);
+    }
+  };
   if constexpr (DIM == 3) {
+    if (tma_tile) {
+      if (tid == 0) {
+        tma::mbar_init(&sBarU, 1);
+        tma::fence_mbar_init();
+      }
+      __syncthreads();
+    }
     // the planes below the first that the predictor reads along z
     for (int pl = z0 - 1 - ZH; pl <= z0 - 2 + ZH; pl++) load_w_plane<DIM, RECON>(P, u1, u2, x0, y0, pl, ring(pl));
+    if (tma_tile) issue_plane(z0 - 1 + ZH);
   }
 
   const int jb = (DIM == 3) ? z0 - 1 : 0;
@@ -210,8 +250,27 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, REC
   for (int j = jb; j <= je; j++) {
     // 1. primitives of plane j + ZH (the plane itself when there is no march)
     const int lp = (DIM == 3) ? j + ZH : 0;
-    load_w_plane<DIM, RECON>(P, u1, u2, x0, y0, lp, ring(lp));
-    __syncthreads();
+    if (tma_tile) {
+      const bool ok = tma::mbar_wait(&sBarU, uphase, tma::WAIT_LIMIT);
+      uphase ^= 1u;
+      if (__syncthreads_or(!ok)) {
+        if (tid == 0 && err) atomicExch(err, tma::ERR_TMA_TIMEOUT);
+        return;
+      }
+      float* dst = ring(lp);
+      for (int idx = tid; idx < WN; idx += G::NT) {
+        float w[6];
+        prim6_from_cons(stage1[idx], stage2[idx], P, 1.f, 1.f, stage_fz, w);
+#pragma unroll
+        for (int c = 0; c < 6; c++) dst[c * WN + idx] = w[c];
+      }
+      __syncthreads();
+      // the staging area is free again: the next plane's copy overlaps this plane's work
+      if (j + 1 <= je) issue_plane(j + 1 + ZH);
+    } else {
+      load_w_plane<DIM, RECON>(P, u1, u2, x0, y0, lp, ring(lp));
+      __syncthreads();
+    }
     const float* sWj = ring((DIM == 3) ? j : 0);
 
     if constexpr (DIM == 3) {
@@ -547,7 +606,8 @@ __global__ void diag_final_kernel(const double* __restrict__ part, int nblocks, 
 
 template <int DIM, int RECON, bool ISEN>
 static cudaError_t launch_sweep_t(const KParams& P, const float4* u1, const float4* u2, float4* o1, float4* o2,
-                                  const DevClock* clk, unsigned* rate_out, int tz, cudaStream_t s) {
+                                  const DevClock* clk, unsigned* rate_out, int tz, const SweepMaps* maps, int* err,
+                                  cudaStream_t s) {
   using G = Geo<DIM, RECON>;
   static bool configured = false;
   if (!configured) {
@@ -562,41 +622,48 @@ static cudaError_t launch_sweep_t(const KParams& P, const float4* u1, const floa
   }
   dim3 grid((P.n[0] + G::TX - 1) / G::TX, DIM >= 2 ? (P.n[1] + G::TY - 1) / G::TY : 1,
             DIM == 3 ? (P.n[2] + tz - 1) / tz : 1);
-  sweep_kernel<DIM, RECON, ISEN><<<grid, G::NT, G::SMEM_BYTES, s>>>(P, u1, u2, o1, o2, clk, rate_out, tz);
+  static const CUtensorMap none{};
+  const bool tma = DIM == 3 && maps && maps->valid;
+  sweep_kernel<DIM, RECON, ISEN><<<grid, G::NT, G::SMEM_BYTES, s>>>(P, u1, u2, o1, o2, clk, rate_out, tz,
+                                                                    tma ? maps->u1 : none, tma ? maps->u2 : none,
+                                                                    tma ? maps->zofs : 0, tma ? 1 : 0, err);
   return cudaGetLastError();
 }
 
 template <int DIM, int RECON>
 static cudaError_t launch_sweep_r(const KParams& P, bool isen, const float4* u1, const float4* u2, float4* o1, float4* o2,
-                                  const DevClock* clk, unsigned* rate_out, int tz, cudaStream_t s) {
+                                  const DevClock* clk, unsigned* rate_out, int tz, const SweepMaps* maps, int* err,
+                                  cudaStream_t s) {
   if constexpr (RECON == R_PPM) {
-    return launch_sweep_t<DIM, RECON, false>(P, u1, u2, o1, o2, clk, rate_out, tz, s);
+    return launch_sweep_t<DIM, RECON, false>(P, u1, u2, o1, o2, clk, rate_out, tz, maps, err, s);
   } else {
-    return isen ? launch_sweep_t<DIM, RECON, true>(P, u1, u2, o1, o2, clk, rate_out, tz, s)
-                : launch_sweep_t<DIM, RECON, false>(P, u1, u2, o1, o2, clk, rate_out, tz, s);
+    return isen ? launch_sweep_t<DIM, RECON, true>(P, u1, u2, o1, o2, clk, rate_out, tz, maps, err, s)
+                : launch_sweep_t<DIM, RECON, false>(P, u1, u2, o1, o2, clk, rate_out, tz, maps, err, s);
   }
 }
 
 template <int DIM>
 static cudaError_t launch_sweep_d(const KParams& P, int recon, bool isen, const float4* u1, const float4* u2, float4* o1,
-                                  float4* o2, const DevClock* clk, unsigned* rate_out, int tz, cudaStream_t s) {
+                                  float4* o2, const DevClock* clk, unsigned* rate_out, int tz, const SweepMaps* maps,
+                                  int* err, cudaStream_t s) {
   switch (recon) {
-    case R_MINMOD: return launch_sweep_r<DIM, R_MINMOD>(P, isen, u1, u2, o1, o2, clk, rate_out, tz, s);
-    case R_MC: return launch_sweep_r<DIM, R_MC>(P, isen, u1, u2, o1, o2, clk, rate_out, tz, s);
-    case R_VANLEER: return launch_sweep_r<DIM, R_VANLEER>(P, isen, u1, u2, o1, o2, clk, rate_out, tz, s);
-    case R_KOREN: return launch_sweep_r<DIM, R_KOREN>(P, isen, u1, u2, o1, o2, clk, rate_out, tz, s);
-    case R_PPM: return launch_sweep_r<DIM, R_PPM>(P, isen, u1, u2, o1, o2, clk, rate_out, tz, s);
+    case R_MINMOD: return launch_sweep_r<DIM, R_MINMOD>(P, isen, u1, u2, o1, o2, clk, rate_out, tz, maps, err, s);
+    case R_MC: return launch_sweep_r<DIM, R_MC>(P, isen, u1, u2, o1, o2, clk, rate_out, tz, maps, err, s);
+    case R_VANLEER: return launch_sweep_r<DIM, R_VANLEER>(P, isen, u1, u2, o1, o2, clk, rate_out, tz, maps, err, s);
+    case R_KOREN: return launch_sweep_r<DIM, R_KOREN>(P, isen, u1, u2, o1, o2, clk, rate_out, tz, maps, err, s);
+    case R_PPM: return launch_sweep_r<DIM, R_PPM>(P, isen, u1, u2, o1, o2, clk, rate_out, tz, maps, err, s);
     default: return cudaErrorInvalidValue;
   }
 }
 
 cudaError_t launch_sweep(const KParams& P, int ndim, int recon, bool isen, const float4* u1, const float4* u2, float4* o1,
-                         float4* o2, const DevClock* clk, unsigned* rate_out, cudaStream_t s, int tz) {
+                         float4* o2, const DevClock* clk, unsigned* rate_out, cudaStream_t s, int tz,
+                         const SweepMaps* maps, int* err) {
   if (tz <= 0) tz = SWEEP_TZ_DEFAULT;
   switch (ndim) {
-    case 1: return launch_sweep_d<1>(P, recon, isen, u1, u2, o1, o2, clk, rate_out, 1, s);
-    case 2: return launch_sweep_d<2>(P, recon, isen, u1, u2, o1, o2, clk, rate_out, 1, s);
-    case 3: return launch_sweep_d<3>(P, recon, isen, u1, u2, o1, o2, clk, rate_out, tz, s);
+    case 1: return launch_sweep_d<1>(P, recon, isen, u1, u2, o1, o2, clk, rate_out, 1, nullptr, err, s);
+    case 2: return launch_sweep_d<2>(P, recon, isen, u1, u2, o1, o2, clk, rate_out, 1, nullptr, err, s);
+    case 3: return launch_sweep_d<3>(P, recon, isen, u1, u2, o1, o2, clk, rate_out, tz, maps, err, s);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -638,6 +705,45 @@ cudaError_t launch_diag(const KParams& P, const float4* u1, const float4* u2, si
   diag_partial_kernel<<<blocks, 256, 0, s>>>(P, u1, u2, ncell, part);
   diag_final_kernel<<<1, 32, 0, s>>>(part, blocks, out);
   return cudaGetLastError();
+}
+
+// Tensor maps of a 3D state for the sweep's staging: each array as a 3D tensor of floats
+// (4 nx, ny, planes), box (4 WX, WY, 1) of the reconstruction's stencil region. `base` is the start
+// of the allocation (halo planes included); the sweep adds zofs to a plane's index.
+bool encode_sweep_maps(SweepMaps* m, const float4* base1, const float4* base2, int nx, int ny, int planes, int zofs,
+                       int recon) {
+  m->valid = false;
+  using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*, const cuuint64_t*,
+                              const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                              CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  static Encode encode = [] {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      fn = nullptr;
+    return reinterpret_cast<Encode>(fn);
+  }();
+  if (!encode) return false;
+  const int wx = (recon == R_PPM ? Geo<3, R_PPM>::WX : Geo<3, R_MINMOD>::WX);
+  const int wy = (recon == R_PPM ? Geo<3, R_PPM>::WY : Geo<3, R_MINMOD>::WY);
+  if (nx < wx || ny < wy) return false;
+  const cuuint64_t dims[3] = {(cuuint64_t)4 * nx, (cuuint64_t)ny, (cuuint64_t)planes};
+  const cuuint64_t strides[2] = {(cuuint64_t)nx * sizeof(float4), (cuuint64_t)nx * ny * sizeof(float4)};
+  const cuuint32_t box[3] = {(cuuint32_t)(4 * wx), (cuuint32_t)wy, 1u};
+  const cuuint32_t estr[3] = {1u, 1u, 1u};
+  const float4* bases[2] = {base1, base2};
+  CUtensorMap* maps[2] = {&m->u1, &m->u2};
+  for (int i = 0; i < 2; i++) {
+    if (((uintptr_t)bases[i] & 15u) != 0) return false;
+    if (encode(maps[i], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void*)bases[i], dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return false;
+  }
+  m->zofs = zofs;
+  m->valid = true;
+  return true;
 }
 
 }  // namespace shz
