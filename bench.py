@@ -158,13 +158,25 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def profile_traffic(recon: str):
-    """Per-cell DRAM traffic of the sweep kernel from the committed ncu summary, if present."""
+def profile_figure(recon: str, key: str):
+    """A per-cell figure of the sweep kernel from the committed ncu summary, if present."""
     f = ROOT / "profiles" / f"sweep_3d_{recon}.md"
     if not f.exists():
         return None
-    m = re.search(r"dram_bytes_per_cell:\s*([0-9.]+)", f.read_text())
+    m = re.search(key + r":\s*([0-9.]+)", f.read_text())
     return float(m.group(1)) if m else None
+
+
+def profile_traffic(recon: str):
+    return profile_figure(recon, "dram_bytes_per_cell")
+
+
+# The B200's issue and FP32 ceilings at its maximum SM clock (148 SMs x 4 schedulers, one warp
+# instruction each per cycle; 128 FP32 lanes per SM, an FMA counting 2): no measured figure exists
+# for these, so they are the nominal ones.
+SM_COUNT, SM_MHZ = 148, 1965.0
+ISSUE_PEAK = SM_COUNT * 4 * SM_MHZ * 1e6          # warp instructions / s
+FP32_PEAK = SM_COUNT * 128 * 2 * SM_MHZ * 1e6     # FLOP / s
 
 
 class ClockSampler:
@@ -248,6 +260,42 @@ def cpu_sample(recon: str, min_seconds: float = 10.0, max_steps: int = 40):
                       f"src/reference/hydro.ts), {threads} threads, {dt:.1f} s"}
 
 
+def cpu_extra() -> list:
+    """Short samples of the oracle on the reference's own CPU test cases and on one thread: Sod 512
+    to t = 0.2, KH 256^2, Sedov 64^3 (all host threads) and TGV 128^3 PPM on one thread."""
+    from oracle.oracle import RefHydro
+    from shaderous_b200 import Config, Problem, problem_prims
+
+    threads = os.cpu_count() or 1
+    out = []
+
+    def sample(name, cfg, prob, limiter, nthreads, steps=None, t_end=None):
+        h = RefHydro(n=cfg.n, dx=cfg.dx, gamma=cfg.gamma, bc_lo=cfg.bc_lo, bc_hi=cfg.bc_hi, cfl=cfg.cfl,
+                     limiter=limiter, isentropic=cfg.isentropic and limiter != "ppm", threads=nthreads)
+        h.init_prims(problem_prims(cfg, prob))
+        t0 = time.perf_counter()
+        if t_end is not None:
+            h.run(t_end)
+        else:
+            for _ in range(steps):
+                h.step()
+        dt = time.perf_counter() - t0
+        out.append({"case": name, "value": cfg.ncell * h.steps / dt, "unit": UNIT, "cores": nthreads, "steps": h.steps,
+                    "seconds": dt})
+
+    sample("sod 512 minmod+hllc to t=0.2", Config(n=(512, 1, 1), gamma=1.4, bc_lo=(1, 0, 0), bc_hi=(1, 0, 0), cfl=0.4,
+                                                   recon="minmod", p_floor=1e-12),
+           Problem("sod", a=(1, 0, 1, 0.125, 0, 0.1)), "minmod", 1, t_end=0.2)
+    sample("kh 256^2 mc+hllc, 20 steps", Config(n=(256, 256, 1), gamma=1.4, cfl=0.4, recon="mc"),
+           Problem("kh", a=(2.0, 1.0, 0.5, 2.5, 0.01, 1e-3), seed=7), "mc", threads, steps=20)
+    sample("sedov 64^3 koren+hllc, 10 steps", Config(n=(64, 64, 64), gamma=5 / 3, cfl=0.5, recon="koren",
+                                                      bc_lo=(1, 1, 1), bc_hi=(1, 1, 1), p_floor=1e-12),
+           Problem("sedov", a=(1.0, 1e-5, 1.0, 3.5)), "koren", threads, steps=10)
+    cfg, prob = workload(128, "ppm")
+    sample("tgv 128^3 ppm+hllc, 2 steps, one thread", cfg, prob, "ppm", 1, steps=2)
+    return out
+
+
 def run_reference(args, rank, world):
     """The reference arm: the CPU oracle on the host's cores, one bounded sample step per bench step."""
     if rank != 0:
@@ -302,7 +350,27 @@ def headline(args, world, value, total_ms, sweep_ms, ncell, launches, clocks, e2
                 "steps": e2e_steps, "seconds": e2e_s},
         "gpu_launches": launches,
         "clocks": clocks,
+        **extra_rooflines(args, ncell * args.steps / (sweep_ms / 1000.0)),
     }
+
+
+def extra_rooflines(args, zu_per_s_gpu: float) -> dict:
+    """The sweep's issue and FP32 rooflines: warp instructions and executed FP32 FLOP per cell from
+    the committed ncu capture, times this run's zone-updates/s of the sweep on one GPU, against the
+    nominal ceilings."""
+    out = {}
+    inst = profile_figure(args.recon, "warp_inst_per_cell")
+    flop = profile_figure(args.recon, "fp32_flop_per_cell")
+    if inst:
+        a = inst * zu_per_s_gpu
+        out["roofline_issue"] = {"bound": "issue", "achieved": a, "peak": ISSUE_PEAK, "unit": "warp instructions/s",
+                                 "frac": a / ISSUE_PEAK, "per_zu": inst, "peak_source": "nominal (148 SMs x 4 x 1965 MHz)"}
+    if flop:
+        a = flop * zu_per_s_gpu
+        out["roofline_fp32"] = {"bound": "fp32", "achieved": a / 1e12, "peak": FP32_PEAK / 1e12, "unit": "TFLOP/s",
+                                "frac": a / FP32_PEAK, "per_zu": flop,
+                                "peak_source": "nominal (148 SMs x 128 lanes x 2 x 1965 MHz); executed FADD + FMUL + 2 FFMA"}
+    return out
 
 
 def run_slabs(args, rank, world, local):
@@ -481,6 +549,9 @@ def main():
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_sample(args.recon)
+        cpu["extra"] = cpu_extra()
+        cpu["reference_js"] = ("src/reference/hydro.ts itself: unavailable on this box (no JavaScript runtime); "
+                               "these are its C++ float64 restatement")
     if dist:
         dist.barrier()
         dist.destroy_process_group()
