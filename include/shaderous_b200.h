@@ -129,6 +129,20 @@ typedef struct shz_diag {
 #define SHZ_PROB_BLAST 5     /* pressure sphere: rho_in a[0], p_in a[1], rho_out a[2], p_out a[3], radius (box units) a[4] */
 #define SHZ_PROB_GAUSS 6     /* gaussian pulse in 3D: rho = a[0] + exp(-r2/a[1]), v = (a[2],a[3],a[4]) , p = a[5] + 0.5 exp(-r2/a[6]) */
 
+/* The rest of the reference's Diagnostics channels (hydro/diagnostics.wgsl channels 6, 9-23;
+ * src/sim.ts:1808-1862): the totals above, the [min, max] over the cells of density,
+ * temperature ((gamma - 1) e_int / rho), scalar (rho s / rho), pressure and speed (`ranges`, in
+ * the reference's FIELDS order), and the centre of mass from the box centre (`com`). The
+ * gravitational, Jeans and burning channels are zero: no gravity or burning on this path. */
+typedef struct shz_diag_ext {
+  shz_diag base;
+  double range[5][2];
+  double com[3];
+  double e_grav;
+  double jeans_unresolved;
+  double nuclear_heating;
+} shz_diag_ext;
+
 typedef struct shz_problem {
   int32_t kind;    /* SHZ_PROB_* */
   int32_t axis;    /* SOD: normal axis */
@@ -187,6 +201,9 @@ int shz_set_t_end(shz_sim* sim, double t_end);
 
 /* Wait for the handle's queued work. */
 int shz_sync(shz_sim* sim);
+
+/* Totals and the extended channels (shz_diag_ext), as Simulation.diagnostics() returns them. */
+int shz_diagnostics_ext(shz_sim* sim, shz_diag_ext* out);
 
 /* Device pointers of the current state (two float4 arrays, layout above), valid until the next
  * step or destroy; for callers that keep data on the device (benchmarks, interop). */
@@ -300,6 +317,8 @@ int shz_amr_step(shz_amr* a, int32_t n);
 int shz_amr_run(shz_amr* a, const shz_run_opts* opts, shz_run_result* res);
 int shz_amr_diagnostics(shz_amr* a, shz_diag* out);
 int shz_amr_clock(shz_amr* a, double* t, double* dt, int64_t* steps);
+/* Totals and the extended channels over the leaves (shz_diag_ext). */
+int shz_amr_diagnostics_ext(shz_amr* a, shz_diag_ext* out);
 /* Run the refinement check now (flag, adapt, regrid); *changed = 1 if the mesh changed. */
 int shz_amr_regrid(shz_amr* a, int32_t* changed);
 /* The leaves, coarsest first (lists().leaves): slots, levels and block coordinates (3 per leaf). */

@@ -81,6 +81,11 @@ class shz_diag(C.Structure):
     ]
 
 
+class shz_diag_ext(C.Structure):
+    _fields_ = [("base", shz_diag), ("range", (C.c_double * 2) * 5), ("com", C.c_double * 3), ("e_grav", C.c_double),
+                ("jeans_unresolved", C.c_double), ("nuclear_heating", C.c_double)]
+
+
 class shz_problem(C.Structure):
     _fields_ = [("kind", C.c_int32), ("axis", C.c_int32), ("seed", C.c_uint64), ("a", C.c_double * 8)]
 
@@ -159,6 +164,7 @@ SIGNATURES = [
     ("shz_step", C.c_int, [C.c_void_p, C.c_int32]),
     ("shz_run", C.c_int, [C.c_void_p, C.POINTER(shz_run_opts), C.POINTER(shz_run_result)]),
     ("shz_diagnostics", C.c_int, [C.c_void_p, C.POINTER(shz_diag)]),
+    ("shz_diagnostics_ext", C.c_int, [C.c_void_p, C.POINTER(shz_diag_ext)]),
     ("shz_clock", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     ("shz_set_clock", C.c_int, [C.c_void_p, C.c_double, C.c_int64]),
     ("shz_set_t_end", C.c_int, [C.c_void_p, C.c_double]),
@@ -200,6 +206,7 @@ SIGNATURES = [
     ("shz_amr_step", C.c_int, [C.c_void_p, C.c_int32]),
     ("shz_amr_run", C.c_int, [C.c_void_p, C.POINTER(shz_run_opts), C.POINTER(shz_run_result)]),
     ("shz_amr_diagnostics", C.c_int, [C.c_void_p, C.POINTER(shz_diag)]),
+    ("shz_amr_diagnostics_ext", C.c_int, [C.c_void_p, C.POINTER(shz_diag_ext)]),
     ("shz_amr_clock", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     ("shz_amr_regrid", C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     ("shz_amr_leaves", C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.c_void_p, C.c_void_p, C.c_void_p]),

@@ -103,6 +103,13 @@ class AmrSim:
         self._ok(self._lib.shz_amr_diagnostics(self._h, C.byref(d)))
         return Diagnostics(d.t, d.dt, d.steps, d.mass, tuple(d.momentum), d.e_kin, d.e_int, d.e_tot, d.max_mach, d.floored)
 
+    def diagnostics_ext(self):
+        from .sim import DiagnosticsExt
+
+        d = _abi.shz_diag_ext()
+        self._ok(self._lib.shz_amr_diagnostics_ext(self._h, C.byref(d)))
+        return DiagnosticsExt.from_c(d)
+
     def leaves(self):
         """(slots, levels, coords (n, 3)) of the leaves, coarsest first."""
         cap = self.cfg.cap

@@ -17,6 +17,7 @@
 #include <cstdint>
 
 #include "amr_device.cuh"
+#include "diag_ext.cuh"
 
 namespace shz {
 namespace amrk {
@@ -242,6 +243,33 @@ __global__ void __launch_bounds__(NT) amr_diag(const KParams* __restrict__ gp, c
   }
 }
 
+// The extended channels (diag_ext.cuh) over the leaves: cell centres from the box centre, each
+// block's cells of its own level's size (amr/grid.wgsl:172-177 blk_pos); a 2D grid in z = 0.
+template <int DIM>
+__global__ void __launch_bounds__(NT) amr_diag_ext(const KParams* __restrict__ gp, const int* __restrict__ bt,
+                                                   const int* __restrict__ list, int n, const float4* __restrict__ u1,
+                                                   const float4* __restrict__ u2, double* __restrict__ part) {
+  dext::Ext e;
+  e.init();
+  for (int i = blockIdx.x; i < n; i += gridDim.x) {
+    const int slot = __ldg(list + i);
+    const KParams& P = gp[bt_at(bt, slot, GRID_WORD)];
+    const double dx = P.dx / ldexp(1.0, bt_at(bt, slot, 0));
+    const double dv = DIM == 3 ? dx * dx * dx : dx * dx;
+    const double half = 0.5 * P.n[0] * BS * P.dx;  // half the box: n[0] root blocks of BS cells
+    const int c0 = bt_at(bt, slot, 1), c1 = bt_at(bt, slot, 2), c2 = bt_at(bt, slot, 3);
+    for (int t = threadIdx.x; t < BG<DIM>::CB; t += NT) {
+      const int l0 = t % BS, l1 = (t / BS) % BS, l2 = DIM == 3 ? t / (BS * BS) : 0;
+      const double x = (c0 * BS + l0 + 0.5) * dx - half;
+      const double y = (c1 * BS + l1 + 0.5) * dx - half;
+      const double z = DIM == 3 ? (c2 * BS + l2 + 0.5) * dx - half : 0.0;
+      const size_t o = (size_t)slot * BG<DIM>::CB + t;
+      e.cell(__ldg(u1 + o), __ldg(u2 + o), P, dv, x, y, z);
+    }
+  }
+  dext::block_reduce(e, part + (size_t)blockIdx.x * dext::N);
+}
+
 __global__ void amr_diag_final(const double* __restrict__ part, int nblocks, double* __restrict__ out) {
   const int v = threadIdx.x;
   if (v >= 9) return;
@@ -361,6 +389,15 @@ cudaError_t amr_launch_diag(const AmrLaunch& L, const int* list, int n, const fl
   if (L.ndim == 3) amrk::amr_diag<3><<<g, amrk::NT, 0, s>>>(L.gp, L.bt, list, n, u1, u2, part);
   else amrk::amr_diag<2><<<g, amrk::NT, 0, s>>>(L.gp, L.bt, list, n, u1, u2, part);
   amrk::amr_diag_final<<<1, 32, 0, s>>>(part, g, out);
+  return cudaGetLastError();
+}
+
+cudaError_t amr_launch_diag_ext(const AmrLaunch& L, const int* list, int n, const float4* u1, const float4* u2,
+                                double* part, double* out, cudaStream_t s) {
+  const int g = amr_diag_blocks(n);
+  if (L.ndim == 3) amrk::amr_diag_ext<3><<<g, amrk::NT, 0, s>>>(L.gp, L.bt, list, n, u1, u2, part);
+  else amrk::amr_diag_ext<2><<<g, amrk::NT, 0, s>>>(L.gp, L.bt, list, n, u1, u2, part);
+  dext::final_kernel<<<1, 32, 0, s>>>(part, g, out);
   return cudaGetLastError();
 }
 

@@ -51,6 +51,10 @@ cudaError_t amr_launch_regrid(const AmrLaunch& L, const int* rg, const int* list
 int amr_diag_blocks(int n);
 cudaError_t amr_launch_diag(const AmrLaunch& L, const int* list, int n, const float4* u1, const float4* u2, double* part,
                             double* out, cudaStream_t s);
+// The extended diagnostics channels (diag_ext.cuh, 13 values) over the leaves in list; part holds
+// amr_diag_blocks(n) x 13 doubles.
+cudaError_t amr_launch_diag_ext(const AmrLaunch& L, const int* list, int n, const float4* u1, const float4* u2,
+                                double* part, double* out, cudaStream_t s);
 cudaError_t amr_launch_ghost_map(const AmrLaunch& L, int slot, int* out, cudaStream_t s);
 
 }  // namespace shz

@@ -477,8 +477,9 @@ int shz_amr_create(const shz_amr_config* cfg, shz_amr** out) {
   ok = ok && cudaMalloc(&a->clk, sizeof(shz::DevClock)) == cudaSuccess;
   ok = ok && cudaMalloc(&a->rates, 4 * sizeof(unsigned)) == cudaSuccess;
   ok = ok && cudaMalloc(&a->d_gp, sizeof(shz::KParams)) == cudaSuccess;
-  ok = ok && cudaMalloc(&a->diag_part, (size_t)shz::amr_diag_blocks(c.cap) * 9 * sizeof(double)) == cudaSuccess;
-  ok = ok && cudaMalloc(&a->diag_out, 9 * sizeof(double)) == cudaSuccess;
+  // (room for the 9 totals or the 13 extended channels per block)
+  ok = ok && cudaMalloc(&a->diag_part, (size_t)shz::amr_diag_blocks(c.cap) * 16 * sizeof(double)) == cudaSuccess;
+  ok = ok && cudaMalloc(&a->diag_out, 16 * sizeof(double)) == cudaSuccess;
   ok = ok && cudaMalloc(&a->d_ghost, (size_t)a->WN * 5 * sizeof(int)) == cudaSuccess;
   ok = ok && cudaMalloc(&a->d_err, sizeof(int)) == cudaSuccess;
   if (ok) ok = cudaMemset(a->d_err, 0, sizeof(int)) == cudaSuccess;
@@ -677,6 +678,28 @@ int shz_amr_diagnostics(shz_amr* a, shz_diag* d) {
   d->e_tot = v[6];
   d->floored = v[7];
   d->max_mach = v[8];
+  return 0;
+}
+
+int shz_amr_diagnostics_ext(shz_amr* a, shz_diag_ext* d) {
+  if (!a || !d) return SHZ_E_CONFIG;
+  int rc = shz_amr_diagnostics(a, &d->base);
+  if (rc) return rc;
+  Dev dv(a->device);
+  AMR_CUDA(a, shz::amr_launch_diag_ext(a->L, a->d_leaves, n_leaves(a), a->u1[a->cur], a->u2[a->cur], a->diag_part,
+                                       a->diag_out, a->stream));
+  a->launches += 2;
+  double v[shz::DIAG_EXT_VALUES];
+  AMR_CUDA(a, cudaMemcpyAsync(v, a->diag_out, sizeof v, cudaMemcpyDeviceToHost, a->stream));
+  AMR_CUDA(a, cudaStreamSynchronize(a->stream));
+  for (int i = 0; i < 5; i++) {
+    d->range[i][0] = v[i];
+    d->range[i][1] = v[5 + i];
+  }
+  for (int i = 0; i < 3; i++) d->com[i] = d->base.mass > 0 ? v[10 + i] / d->base.mass : 0.0;
+  d->e_grav = 0.0;
+  d->jeans_unresolved = 0.0;
+  d->nuclear_heating = 0.0;
   return 0;
 }
 

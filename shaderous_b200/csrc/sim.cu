@@ -343,8 +343,8 @@ int shz_create(const shz_config* cfg, shz_sim** out) {
   const int dblocks = shz::diag_blocks(s->ncell);
   if (cudaMalloc(&s->d_err, sizeof(int)) != cudaSuccess || cudaMemset(s->d_err, 0, sizeof(int)) != cudaSuccess ||
       cudaMalloc(&s->clk, sizeof(shz::DevClock)) != cudaSuccess || cudaMalloc(&s->rates, 2 * sizeof(unsigned)) != cudaSuccess ||
-      cudaMalloc(&s->diag_part, (size_t)dblocks * shz::DIAG_VALUES * sizeof(double)) != cudaSuccess ||
-      cudaMalloc(&s->diag_out, shz::DIAG_VALUES * sizeof(double)) != cudaSuccess) {
+      cudaMalloc(&s->diag_part, (size_t)dblocks * 16 * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&s->diag_out, 16 * sizeof(double)) != cudaSuccess) {  // the totals or the extended channels
     cudaGetLastError();
     fail(s, SHZ_E_OOM, "clock / reduction buffers do not fit");
     return bail(SHZ_E_OOM);
@@ -578,6 +578,28 @@ int shz_diagnostics(shz_sim* s, shz_diag* d) {
   d->e_tot = v[6];
   d->floored = v[7];
   d->max_mach = v[8];
+  return 0;
+}
+
+int shz_diagnostics_ext(shz_sim* s, shz_diag_ext* d) {
+  if (!s || !d) return SHZ_E_CONFIG;
+  int rc = shz_diagnostics(s, &d->base);
+  if (rc) return rc;
+  DeviceScope ds_(s->device);
+  CUDA_OR_FAIL(s, shz::launch_diag_ext(s->kp, s->u1[s->cur], s->u2[s->cur], s->ncell, s->diag_part, s->diag_out,
+                                       s->stream));
+  s->launches += 2;
+  double v[shz::DIAG_EXT_VALUES];
+  CUDA_OR_FAIL(s, cudaMemcpyAsync(v, s->diag_out, sizeof v, cudaMemcpyDeviceToHost, s->stream));
+  CUDA_OR_FAIL(s, cudaStreamSynchronize(s->stream));
+  for (int i = 0; i < 5; i++) {
+    d->range[i][0] = v[i];
+    d->range[i][1] = v[5 + i];
+  }
+  for (int i = 0; i < 3; i++) d->com[i] = d->base.mass > 0 ? v[10 + i] / d->base.mass : 0.0;
+  d->e_grav = 0.0;
+  d->jeans_unresolved = 0.0;
+  d->nuclear_heating = 0.0;
   return 0;
 }
 

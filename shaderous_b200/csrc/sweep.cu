@@ -33,6 +33,7 @@
 
 #include "hydro_cell.cuh"
 #include "hydro_math.cuh"
+#include "diag_ext.cuh"
 #include "sweep.h"
 #include "tma.cuh"
 
@@ -601,8 +602,34 @@ __global__ void diag_final_kernel(const double* __restrict__ part, int nblocks, 
   out[i] = (i == 8) ? mx : s.value();
 }
 
+// The extended channels (diag_ext.cuh) of a uniform grid: cell centres from the box centre, as
+// diagnostics.wgsl:52-56 has them (a 2D grid in the plane z = 0, a 1D one on the x axis).
+__global__ void diag_ext_partial_kernel(const KParams P, const float4* __restrict__ u1, const float4* __restrict__ u2,
+                                        size_t ncell, double* __restrict__ part) {
+  dext::Ext e;
+  e.init();
+  const int nx = P.n[0], ny = P.n[1], nz = P.n[2];
+  const double dx = P.dx, dv = P.dv;
+  for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < ncell; o += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(o % nx), j = (int)((o / nx) % ny), k = (int)(o / ((size_t)nx * ny));
+    const double x = (i + 0.5 - 0.5 * nx) * dx;
+    const double y = ny > 1 ? (j + 0.5 - 0.5 * ny) * dx : 0.0;
+    const double z = nz > 1 ? (k + 0.5 - 0.5 * nz) * dx : 0.0;
+    e.cell(__ldg(u1 + o), __ldg(u2 + o), P, dv, x, y, z);
+  }
+  dext::block_reduce(e, part + (size_t)blockIdx.x * dext::N);
+}
+
 // ---------------------------------------------------------------------------------------------
 // Host launchers.
+
+cudaError_t launch_diag_ext(const KParams& P, const float4* u1, const float4* u2, size_t ncell, double* part, double* out,
+                            cudaStream_t s) {
+  const int g = diag_blocks(ncell);
+  diag_ext_partial_kernel<<<g, 256, 0, s>>>(P, u1, u2, ncell, part);
+  dext::final_kernel<<<1, 32, 0, s>>>(part, g, out);
+  return cudaGetLastError();
+}
 
 template <int DIM, int RECON, bool ISEN>
 static cudaError_t launch_sweep_t(const KParams& P, const float4* u1, const float4* u2, float4* o1, float4* o2,

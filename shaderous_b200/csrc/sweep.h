@@ -34,6 +34,11 @@ cudaError_t launch_clock(DevClock* clk, unsigned* rates, int slot, cudaStream_t 
 int diag_blocks(size_t ncell);
 cudaError_t launch_diag(const KParams& P, const float4* u1, const float4* u2, size_t ncell, double* part, double* out,
                         cudaStream_t s);
+// The extended diagnostics channels (diag_ext.cuh, 13 values) of a state; part holds
+// diag_blocks(ncell) x 13 doubles.
+constexpr int DIAG_EXT_VALUES = 13;
+cudaError_t launch_diag_ext(const KParams& P, const float4* u1, const float4* u2, size_t ncell, double* part, double* out,
+                            cudaStream_t s);
 size_t sweep_smem_bytes(int ndim, int recon);
 int sweep_min_cells(int recon);
 

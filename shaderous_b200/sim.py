@@ -56,6 +56,28 @@ class Diagnostics:
 
 
 @dataclass
+class DiagnosticsExt:
+    """The totals and the reference's other Diagnostics channels (src/sim.ts:1810-1862): ranges
+    as [min, max] of density, temperature, scalar, pressure and speed (FIELDS order), the centre
+    of mass from the box centre; gravity, Jeans and burning channels (zero on this path)."""
+
+    totals: Diagnostics
+    ranges: dict
+    com: tuple
+    e_grav: float
+    jeans_unresolved: float
+    nuclear_heating: float
+
+    @staticmethod
+    def from_c(d) -> "DiagnosticsExt":
+        b = d.base
+        tot = Diagnostics(b.t, b.dt, b.steps, b.mass, tuple(b.momentum), b.e_kin, b.e_int, b.e_tot, b.max_mach, b.floored)
+        names = ("rho", "temperature", "scalar", "pressure", "speed")
+        return DiagnosticsExt(tot, {k: (d.range[i][0], d.range[i][1]) for i, k in enumerate(names)}, tuple(d.com),
+                              d.e_grav, d.jeans_unresolved, d.nuclear_heating)
+
+
+@dataclass
 class Config:
     """The hot-path subset of SimConfig (src/sim.ts:48-265), defaults from configFor (:645-742)."""
 
@@ -237,6 +259,11 @@ class Sim:
         d = _abi.shz_diag()
         self._ok(self._lib.shz_diagnostics(self._h, C.byref(d)))
         return Diagnostics(d.t, d.dt, d.steps, d.mass, tuple(d.momentum), d.e_kin, d.e_int, d.e_tot, d.max_mach, d.floored)
+
+    def diagnostics_ext(self) -> DiagnosticsExt:
+        d = _abi.shz_diag_ext()
+        self._ok(self._lib.shz_diagnostics_ext(self._h, C.byref(d)))
+        return DiagnosticsExt.from_c(d)
 
     def state_device(self) -> tuple[int, int]:
         a, b = C.c_void_p(), C.c_void_p()
