@@ -58,8 +58,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-amr", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-comparable", action="store_true",
+                    help="skip the configurations the reference publishes throughputs for")
     ap.add_argument("--serve-requests", type=int, default=200)
-    ap.add_argument("--section", choices=["all", "amr", "serving"], default="all",
+    ap.add_argument("--section", choices=["all", "amr", "serving", "comparable"], default="all",
                     help="amr / serving: only that measurement, printed as its own JSON line")
     ap.add_argument("--amr-variant", choices=["both", "spec", "developed"], default="both")
     ap.add_argument("--amr-cap", type=int, default=26000, help="block slots of the AMR runs")
@@ -113,6 +115,40 @@ def amr_sedov(levels=4, nr=8, radius_cells=3.5, steps=24, cap=26000, grown=False
             "finest_cells_per_side": nr * 16 << levels, "radius_finest_cells": 0.2 * (nr * 16 << levels) if grown else radius_cells,
             "init_s": t_init, "gpu_launches": launches,
             "note": "time includes the refinement checks (flag, host adapt, regrid) every 8 steps"}
+
+
+# The reference's published throughputs (WebGPU, zone-updates/s) for the same
+# configurations, for context: other hardware and another implementation.
+PUBLISHED = {
+    "kh_2d_1024": {"H200 NVL": 2.339e9, "RTX 3080": 1.633e9},
+    "kh_2d_2048": {"H200 NVL": 2.743e9, "H100": 2.602e9, "A100": 1.736e9, "RTX 3080": 1.849e9},
+    "sedov_3d_256": {"H200 NVL": 1.670e9, "H100": 1.571e9, "A100": 1.196e9, "RTX 3080": 1.386e9},
+}
+
+
+def comparable(steps=40):
+    """The configurations the reference publishes throughputs for, with its default scheme
+    (koren + isentropic density + HLLC, CFL 0.8 unless stated): 2D Kelvin-Helmholtz at 1024^2 and
+    2048^2 and the 3D Sedov blast on a uniform 256^3 grid. Device time of `steps` steps after a
+    warm-up, CUDA events on the library's stream."""
+    from shaderous_b200 import Config, Problem, Sim
+
+    out = {}
+    cases = [
+        ("kh_2d_1024", Config(n=(1024, 1024, 1), gamma=1.4, recon="koren"), Problem("kh", a=(2, 1, 0.5, 2.5, 0.01, 1e-3), seed=1)),
+        ("kh_2d_2048", Config(n=(2048, 2048, 1), gamma=1.4, recon="koren"), Problem("kh", a=(2, 1, 0.5, 2.5, 0.01, 1e-3), seed=1)),
+        ("sedov_3d_256", Config(n=(256, 256, 256), gamma=5 / 3, recon="koren", bc_lo=(1, 1, 1), bc_hi=(1, 1, 1),
+                                p_floor=1e-12), Problem("sedov", a=(1.0, 1e-5, 1.0, 3.5))),
+    ]
+    for name, cfg, prob in cases:
+        with Sim(cfg) as s:
+            s.reset(prob)
+            s.profile(5)  # warm-up (tunes)
+            prof = s.profile(steps)
+        v = cfg.ncell * steps / (prof["total_ms"] / 1000.0)
+        out[name] = {"value": v, "unit": UNIT, "ms_per_step": prof["total_ms"] / steps, "steps": steps,
+                     "scheme": "koren+isentropic+hllc, cfl 0.8", "published_reference": PUBLISHED[name]}
+    return out
 
 
 def serving(n_requests=200, seed=2024, budget=150e9):
@@ -457,6 +493,8 @@ def main():
             if args.amr_variant in ("both", "developed"):
                 out["developed"] = amr_sedov(steps=max(args.steps, 8), grown=True, cap=args.amr_cap,
                                              profile_window=args.profile_window)
+        elif args.section == "comparable":
+            out = comparable()
         else:
             out = serving(args.serve_requests)
         print(json.dumps({"section": args.section, "result": out}), flush=True)
@@ -546,6 +584,7 @@ def main():
                                      "grown blast (about 20k blocks) that the spec's run reaches later")
     if rank == 0 and not args.no_serving:
         serve = serving(args.serve_requests)
+    comp = comparable() if rank == 0 and not args.no_comparable else None
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_sample(args.recon)
@@ -568,6 +607,8 @@ def main():
         line["amr_sedov"] = amr
     if serve:
         line["serving"] = serve
+    if comp:
+        line["comparable"] = comp
     print(json.dumps(line), flush=True)
 
 

@@ -263,14 +263,15 @@ __device__ __forceinline__ Cons prolong_child(const Cons& uc, const Slopes& s, c
   return u;
 }
 
-// amr/assemble.wgsl:47-75 from_coarse: a ghost beyond a face whose neighbour is one level
-// coarser, prolonged from the coarse leaf `cs` with slopes from that leaf's neighbours.
+// The coarse cell under texel l of block `slot`, in the coarser leaf `cs`: its state and the
+// prolongation's limited slopes (amr/assemble.wgsl:47-75, amr/cons.wgsl:78-106), and the texel's
+// parity within it. Every fine texel over one coarse cell gets the same state and slopes.
 template <int DIM, int R>
-__device__ __forceinline__ Cons from_coarse(const int* __restrict__ bt, const float4* __restrict__ u1,
+__device__ __forceinline__ void coarse_cell(const int* __restrict__ bt, const float4* __restrict__ u1,
                                             const float4* __restrict__ u2, int nr, int slot, const int* l, int cs,
-                                            float rho_floor) {  // nr: root blocks per side of the block's grid
+                                            float rho_floor, Cons& uc, Slopes& sl, int* par) {
   const int nc = nr * BS << bt_at(bt, cs, 0);
-  int gf[3], lc[3], par[3];
+  int gf[3], lc[3];
 #pragma unroll
   for (int a = 0; a < 3; a++) {
     gf[a] = a < DIM ? bt_at(bt, slot, 1 + a) * BS + l[a] : 0;
@@ -279,7 +280,7 @@ __device__ __forceinline__ Cons from_coarse(const int* __restrict__ bt, const fl
     lc[a] = a < DIM ? gc - bt_at(bt, cs, 1 + a) * BS : 0;
     par[a] = a < DIM ? (gf[a] & 1) : 0;
   }
-  Cons uc, m[3], p[3];
+  Cons m[3], p[3];
   bool mok[3] = {false, false, false}, pok[3] = {false, false, false};
   if (!u_near<DIM>(bt, u1, u2, cs, lc, uc)) uc = Cons{make_float4(1.f, 0.f, 0.f, 0.f), make_float4(1.f, 1.f, 0.f, 0.f)};
 #pragma unroll
@@ -290,7 +291,19 @@ __device__ __forceinline__ Cons from_coarse(const int* __restrict__ bt, const fl
     at[a] += 2;
     pok[a] = u_near<DIM>(bt, u1, u2, cs, at, p[a]);
   }
-  const Slopes sl = prolong_slopes<DIM, R>(uc, m, mok, p, pok, rho_floor);
+  sl = prolong_slopes<DIM, R>(uc, m, mok, p, pok, rho_floor);
+}
+
+// amr/assemble.wgsl:47-75 from_coarse: a ghost beyond a face whose neighbour is one level
+// coarser, prolonged from the coarse leaf `cs` with slopes from that leaf's neighbours.
+template <int DIM, int R>
+__device__ __forceinline__ Cons from_coarse(const int* __restrict__ bt, const float4* __restrict__ u1,
+                                            const float4* __restrict__ u2, int nr, int slot, const int* l, int cs,
+                                            float rho_floor) {  // nr: root blocks per side of the block's grid
+  Cons uc;
+  Slopes sl;
+  int par[3];
+  coarse_cell<DIM, R>(bt, u1, u2, nr, slot, l, cs, rho_floor, uc, sl, par);
   return prolong_child(uc, sl, par);
 }
 

@@ -22,16 +22,55 @@
 namespace shz {
 namespace amrk {
 
+// The coarse-cell table of the assemble: for each face of a block whose neighbour is one level
+// coarser, the state and prolongation slopes of the coarse cells its ghosts lie over (8 x 8 in
+// 3D, 8 in 2D; the two ghost layers are one coarse layer), 33 floats each: uc, three slopes, the
+// common scale-back factor. Every fine ghost over a coarse cell reads the same entry.
+constexpr int TAB_VALS = 33;
+template <int DIM>
+struct Tab {
+  static constexpr int CPF = DIM == 3 ? 64 : 8;  // coarse cells per face
+  static constexpr size_t BYTES = (size_t)2 * DIM * CPF * TAB_VALS * sizeof(float);
+};
+
+__device__ __forceinline__ void tab_store(float* e, const Cons& uc, const Slopes& sl) {
+  const float4 v[8] = {uc.a, uc.b, sl.s[0].a, sl.s[0].b, sl.s[1].a, sl.s[1].b, sl.s[2].a, sl.s[2].b};
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    e[4 * k] = v[k].x;
+    e[4 * k + 1] = v[k].y;
+    e[4 * k + 2] = v[k].z;
+    e[4 * k + 3] = v[k].w;
+  }
+  e[32] = sl.f;
+}
+__device__ __forceinline__ void tab_load(const float* e, Cons& uc, Slopes& sl) {
+  float4 v[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) v[k] = make_float4(e[4 * k], e[4 * k + 1], e[4 * k + 2], e[4 * k + 3]);
+  uc = Cons{v[0], v[1]};
+  sl.s[0] = Cons{v[2], v[3]};
+  sl.s[1] = Cons{v[4], v[5]};
+  sl.s[2] = Cons{v[6], v[7]};
+  sl.f = e[32];
+}
+
 // 1. Primitives of every block in the list with two ghost layers; the rate / dx maximum over the
 // leaves' own cells (assemble.wgsl:78-154; PER_DX in clock.wgsl). MINB: the CTAs per SM the
 // register budget is planned for (the autotuner's variant): more CTAs hide the gather's latency,
-// fewer registers spill on the prolongation path of coarse ghosts.
+// fewer registers spill on the prolongation path of coarse ghosts. Ghosts beyond a coarser
+// block's face take their coarse cell's state and slopes from the block's table (built first,
+// once per coarse cell); with per_texel (the two-pass mode, the reference's structure) each
+// ghost forms them itself. Both give the same numbers.
 template <int DIM, int R, int MINB>
 __global__ void __launch_bounds__(NT, MINB) amr_assemble(const KParams* __restrict__ gp, const int* __restrict__ bt,
                                                    const int* __restrict__ list, int n, const float4* __restrict__ u1,
                                                    const float4* __restrict__ u2, float4* __restrict__ w1,
-                                                   float4* __restrict__ w2, unsigned* __restrict__ rates, int rslot) {
+                                                   float4* __restrict__ w2, unsigned* __restrict__ rates, int rslot,
+                                                   int per_texel) {
+  using T = Tab<DIM>;
   __shared__ float sRed[NT / 32];
+  extern __shared__ __align__(16) float sTab[];
   for (int i = blockIdx.x; i < n; i += gridDim.x) {
     float rmax = 0.f;
     const int slot = __ldg(list + i);
@@ -40,21 +79,62 @@ __global__ void __launch_bounds__(NT, MINB) amr_assemble(const KParams* __restri
     const int nr = P.n[0];
     const bool leaf = leaf_of(bt, slot);
     const float inv_dx = (float)(ldexp(1.0, bt_at(bt, slot, 0)) / P.dx);
+    unsigned cmask = 0;
+    if (!per_texel)
+#pragma unroll
+      for (int f = 0; f < 2 * DIM; f++)
+        if (bt_at(bt, slot, 6 + f) == -1) cmask |= 1u << f;
+    if (cmask) {
+      // the table of this block's coarse faces (the previous block's reads of it ended at the
+      // barriers of its rate maximum)
+      const int nf = __popc(cmask);
+      for (int idx = threadIdx.x; idx < nf * T::CPF; idx += NT) {
+        const int k = idx / T::CPF, c = idx % T::CPF;
+        unsigned mk = cmask;
+        for (int q = 0; q < k; q++) mk &= mk - 1;
+        const int f = __ffs(mk) - 1;
+        const int a = f >> 1;
+        int m[3] = {0, 0, 0};
+        m[a] = (f & 1) ? BS : -1;
+        if (DIM == 3) {
+          m[(a + 1) % 3] = 2 * (c % 8);
+          m[(a + 2) % 3] = 2 * (c / 8);
+        } else {
+          m[1 - a] = 2 * c;
+        }
+        Cons uc;
+        Slopes sl;
+        int par[3];
+        coarse_cell<DIM, R>(bt, u1, u2, nr, slot, m, bt_at(bt, slot, 20 + f), P.rho_floor, uc, sl, par);
+        tab_store(sTab + (size_t)(f * T::CPF + c) * TAB_VALS, uc, sl);
+      }
+      __syncthreads();
+    }
     for (int t = threadIdx.x; t < BG<DIM>::WN; t += NT) {
       int l[3] = {t % PAD - NG, (t / PAD) % PAD - NG, DIM == 3 ? t / (PAD * PAD) - NG : 0};
       const Src s = ghost_src_any<DIM>(bt, slot, l);
       Cons u;
       if (s.kind == 0) {
         u = u_at<DIM>(bt, u1, u2, s.slot, s.l);
-        u.a.y *= s.flip[0];
-        u.a.z *= s.flip[1];
-        u.a.w *= s.flip[2];
+      } else if (cmask && s.from == slot) {
+        // a ghost of this block's own coarse face: its coarse cell from the table
+        int a = 0;
+#pragma unroll
+        for (int q = 0; q < DIM; q++)
+          if (s.l[q] < 0 || s.l[q] >= BS) a = q;
+        const int f = 2 * a + (s.l[a] >= BS ? 1 : 0);
+        const int c = DIM == 3 ? (s.l[(a + 1) % 3] >> 1) + 8 * (s.l[(a + 2) % 3] >> 1) : (s.l[1 - a] >> 1);
+        Cons uc;
+        Slopes sl;
+        tab_load(sTab + (size_t)(f * T::CPF + c) * TAB_VALS, uc, sl);
+        const int par[3] = {s.l[0] & 1, s.l[1] & 1, DIM == 3 ? (s.l[2] & 1) : 0};
+        u = prolong_child(uc, sl, par);
       } else {
         u = from_coarse<DIM, R>(bt, u1, u2, nr, s.from, s.l, s.slot, P.rho_floor);
-        u.a.y *= s.flip[0];
-        u.a.z *= s.flip[1];
-        u.a.w *= s.flip[2];
       }
+      u.a.y *= s.flip[0];
+      u.a.z *= s.flip[1];
+      u.a.w *= s.flip[2];
       float w[7];
       prim_from_cons(u.a, u.b, P, 1.f, 1.f, 1.f, w);
       const size_t o = (size_t)slot * BG<DIM>::WN + t;
@@ -62,7 +142,7 @@ __global__ void __launch_bounds__(NT, MINB) amr_assemble(const KParams* __restri
       w2[o] = make_float4(w[4], w[5], w[6], 0.f);
       bool inside = leaf;
 #pragma unroll
-      for (int a = 0; a < DIM; a++) inside = inside && l[a] >= 0 && l[a] < BS;
+      for (int q = 0; q < DIM; q++) inside = inside && l[q] >= 0 && l[q] < BS;
       if (inside) rmax = fmaxf(rmax, rate_guard_f(fabsf(w[1]) + fabsf(w[2]) + fabsf(w[3]) + P.signal * w[6]) * inv_dx);
     }
     const float m = block_max(rmax, sRed);
@@ -303,14 +383,27 @@ __global__ void amr_ghost_map(const int* __restrict__ bt, int slot, int* __restr
 // Host launchers.
 
 namespace {
+template <int DIM, int R, int MINB>
+cudaError_t assemble_t(const AmrLaunch& L, int g, const int* list, int n, const float4* u1, const float4* u2,
+                       unsigned* rates, int rslot, cudaStream_t s) {
+  auto k = amrk::amr_assemble<DIM, R, MINB>;
+  // (set once per instantiation; not a stream operation)
+  static const cudaError_t attr =
+      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)amrk::Tab<DIM>::BYTES);
+  if (attr != cudaSuccess) return attr;
+  const size_t smem = L.per_texel ? 0 : amrk::Tab<DIM>::BYTES;
+  k<<<g, amrk::NT, smem, s>>>(L.gp, L.bt, list, n, u1, u2, L.w1, L.w2, rates, rslot, L.per_texel ? 1 : 0);
+  return cudaGetLastError();
+}
 template <int MINB>
-void assemble_v(const AmrLaunch& L, int g, const int* list, int n, const float4* u1, const float4* u2, unsigned* rates,
-                int rslot, cudaStream_t s) {
+cudaError_t assemble_v(const AmrLaunch& L, int g, const int* list, int n, const float4* u1, const float4* u2,
+                       unsigned* rates, int rslot, cudaStream_t s) {
   if (L.ndim == 3) {
-    SHZ_RECON_SWITCH(L.recon, false, (amrk::amr_assemble<3, R, MINB><<<g, amrk::NT, 0, s>>>(L.gp, L.bt, list, n, u1, u2, L.w1, L.w2, rates, rslot)))
+    SHZ_RECON_SWITCH(L.recon, false, return (assemble_t<3, R, MINB>(L, g, list, n, u1, u2, rates, rslot, s)))
   } else {
-    SHZ_RECON_SWITCH(L.recon, false, (amrk::amr_assemble<2, R, MINB><<<g, amrk::NT, 0, s>>>(L.gp, L.bt, list, n, u1, u2, L.w1, L.w2, rates, rslot)))
+    SHZ_RECON_SWITCH(L.recon, false, return (assemble_t<2, R, MINB>(L, g, list, n, u1, u2, rates, rslot, s)))
   }
+  return cudaSuccess;
 }
 }  // namespace
 
@@ -319,11 +412,10 @@ cudaError_t amr_launch_assemble(const AmrLaunch& L, const int* list, int n, cons
   if (n <= 0) return cudaSuccess;
   const int g = grid_for(n, c && c->per_sm > 0 ? c->per_sm : 4);
   switch (c ? c->variant : 0) {
-    case 1: assemble_v<2>(L, g, list, n, u1, u2, rates, rslot, s); break;
-    case 2: assemble_v<3>(L, g, list, n, u1, u2, rates, rslot, s); break;
-    default: assemble_v<1>(L, g, list, n, u1, u2, rates, rslot, s); break;
+    case 1: return assemble_v<2>(L, g, list, n, u1, u2, rates, rslot, s);
+    case 2: return assemble_v<3>(L, g, list, n, u1, u2, rates, rslot, s);
+    default: return assemble_v<1>(L, g, list, n, u1, u2, rates, rslot, s);
   }
-  return cudaGetLastError();
 }
 
 cudaError_t amr_launch_flag(const AmrLaunch& L, const int* list, int n, float* flags, cudaStream_t s) {

@@ -26,6 +26,9 @@ struct AmrLaunch {
   // Device error word the kernels set when a bounded wait runs out (tma::ERR_*); read and cleared
   // by the host.
   int* err = nullptr;
+  // The assemble forms every coarse ghost's prolongation itself, as the reference does (the two-pass
+  // mode), instead of from its per-block table of coarse cells; the numbers are the same.
+  bool per_texel = false;
 };
 
 // rates: two 32-bit maxima per grid; the assemble folds the leaves' rate / dx into slot rslot.

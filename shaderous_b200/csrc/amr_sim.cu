@@ -451,6 +451,7 @@ int shz_amr_create(const shz_amr_config* cfg, shz_amr** out) {
   a->L.ndim = c.ndim;
   a->L.recon = c.hydro.recon;
   a->L.isen = c.hydro.isentropic != 0;
+  a->L.per_texel = c.two_pass != 0;
   auto bail = [&](int code, const char* what) {
     g_create_err = what;
     shz_amr_destroy(a);
