@@ -426,6 +426,12 @@ typedef struct shz_tune_entry {
 int shz_tune_enable(int32_t on);
 /* Forget every choice. */
 void shz_tune_reset(void);
+
+/* A check of the kernels' bounded waits on `device`: one CTA waits on an mbarrier phase that
+ * nothing completes, with a short limit, and reports through its error word as a sweep whose bulk
+ * copy never lands would (then the handle's calls return SHZ_E_TIMEOUT). *code is the kernel's
+ * error code: 1 (the timeout) when the path works. No counterpart in the reference. */
+int shz_selftest_wait_timeout(int32_t device, int32_t* code);
 /* Copy up to `max` entries of the table; *n = entries in the table. */
 int shz_tune_entries(shz_tune_entry* out, int32_t max, int32_t* n);
 

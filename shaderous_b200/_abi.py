@@ -182,6 +182,7 @@ SIGNATURES = [
     ("shz_tune_enable", C.c_int, [C.c_int32]),
     ("shz_tune_reset", None, []),
     ("shz_tune_entries", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]),
+    ("shz_selftest_wait_timeout", C.c_int, [C.c_int32, C.POINTER(C.c_int32)]),
     ("shz_tree_create", C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_int32),
                                   C.POINTER(C.c_int32), C.c_int32, C.POINTER(C.c_void_p)]),
     ("shz_tree_destroy", None, [C.c_void_p]),

@@ -138,3 +138,47 @@ int shz_tune_entries(shz_tune_entry* out, int32_t max, int32_t* n) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// A check of the kernels' bounded-wait path, without any fault: one CTA waits on an mbarrier
+// phase that nothing completes, with a short limit, and must come back with the timeout code in
+// its error word, as a copy that never lands would make the sweeps do.
+#include "tma.cuh"
+
+namespace {
+__global__ void wait_timeout_kernel(int* err, uint32_t limit) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    shz::tma::mbar_init(&bar, 1);
+    shz::tma::fence_mbar_init();
+  }
+  __syncthreads();
+  // phase 0 never completes: no thread arrives on it
+  const bool ok = shz::tma::mbar_wait(&bar, 0u, limit);
+  if (__syncthreads_or(!ok)) {
+    if (threadIdx.x == 0) atomicExch(err, shz::tma::ERR_TMA_TIMEOUT);
+    return;
+  }
+  if (threadIdx.x == 0) atomicExch(err, -1);  // (cannot happen: the phase has no arrivals)
+}
+}  // namespace
+
+extern "C" int shz_selftest_wait_timeout(int32_t device, int32_t* code) {
+  if (!code) return SHZ_E_CONFIG;
+  int prev = -1;
+  cudaGetDevice(&prev);
+  if (cudaSetDevice(device) != cudaSuccess) return SHZ_E_NODEV;
+  int* d = nullptr;
+  int rc = SHZ_OK;
+  if (cudaMalloc(&d, sizeof(int)) != cudaSuccess || cudaMemset(d, 0, sizeof(int)) != cudaSuccess) rc = SHZ_E_CUDA;
+  if (rc == SHZ_OK) {
+    wait_timeout_kernel<<<1, 64>>>(d, 1000u);
+    if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) rc = SHZ_E_CUDA;
+  }
+  int h = 0;
+  if (rc == SHZ_OK && cudaMemcpy(&h, d, sizeof h, cudaMemcpyDeviceToHost) != cudaSuccess) rc = SHZ_E_CUDA;
+  if (d) cudaFree(d);
+  if (prev >= 0) cudaSetDevice(prev);
+  *code = h;
+  return rc;
+}

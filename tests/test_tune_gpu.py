@@ -56,3 +56,16 @@ def test_amr_tuning_is_exact():
     assert {"amr_assemble", "amr_sweep", "amr_fine_flux"} <= kinds
     for e in tune.entries():
         assert e["ms"] <= e["default_ms"]
+
+
+def test_bounded_wait_reports_timeout():
+    """The bounded-wait path of the TMA-staged sweeps, run for real without a fault: a wait on an
+    mbarrier phase nothing completes gives up after its limit and sets the timeout code."""
+    import ctypes as C
+
+    from shaderous_b200 import _abi
+
+    lib = _abi.load()
+    code = C.c_int32(0)
+    assert lib.shz_selftest_wait_timeout(0, C.byref(code)) == 0
+    assert code.value == 1
