@@ -303,6 +303,12 @@ typedef struct shz_amr_config {
                            primitives); 1: the reference's two passes, predict into a half-step
                            atlas then update (amr_sim.ts:2709-2946), which costs that atlas's
                            memory; both give the same state to rounding */
+  int32_t time_bins;    /* per-block timesteps (SimConfig.timeBins, amr_sim.ts:1002-1010): 0 off,
+                           else up to 5 bins, time advancing in cycles of 2^time_bins substeps of
+                           the fastest block's step (amr/bins_*.wgsl); run with the two-pass
+                           kernels, which keep each block's half step for its slower neighbours */
+  int32_t time_bins_always; /* 1: never pause the cycles when they save too little
+                               (SimConfig.timeBinsAlways, amr_sim.ts:2992-3020) */
 } shz_amr_config;
 typedef struct shz_amr shz_amr;
 
@@ -336,6 +342,15 @@ int shz_amr_flags(shz_amr* a, float* out);
 int shz_amr_ghost_map(shz_amr* a, int32_t slot, int32_t* out);
 int shz_amr_profile(shz_amr* a, int32_t n, shz_profile_result* out);
 int64_t shz_amr_kernel_launches(const shz_amr* a);
+/* Per-block timesteps. The bin table of the last cycle (AmrSim.readBins, amr_sim.ts:4283): cap + 1
+ * ints, [0] the substep last taken, [1 + slot] the block's bin; and, if rates is not null, the
+ * blocks' own signal rates per unit cell size that the cycle's bins were formed from (cap floats,
+ * leaves only). Both are zero before the first cycle. */
+int shz_amr_bins(shz_amr* a, int32_t* bins, float* rates);
+/* The work of the cycles so far (AmrSim.binWork, amr_sim.ts:1663): cycles taken, block updates
+ * made (deposits included) and the updates single steps would have made; *paused: single steps
+ * left before the cycles resume (the start of a run, or a pause when they saved too little). */
+int shz_amr_bin_work(shz_amr* a, int64_t* cycles, int64_t* updates, int64_t* single, int32_t* paused);
 
 /*
  * Serving: independent hydro runs ("requests") of uneven sizes kept resident in HBM and advanced

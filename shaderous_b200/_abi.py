@@ -102,6 +102,8 @@ class shz_amr_config(C.Structure):
         ("refine_lo", C.c_double),
         ("regrid_every", C.c_int32),
         ("two_pass", C.c_int32),
+        ("time_bins", C.c_int32),
+        ("time_bins_always", C.c_int32),
     ]
 
 
@@ -217,6 +219,9 @@ SIGNATURES = [
     ("shz_amr_ghost_map", C.c_int, [C.c_void_p, C.c_int32, C.c_void_p]),
     ("shz_amr_profile", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(shz_profile_result)]),
     ("shz_amr_kernel_launches", C.c_int64, [C.c_void_p]),
+    ("shz_amr_bins", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("shz_amr_bin_work", C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                   C.POINTER(C.c_int32)]),
     ("shz_server_create", C.c_int, [C.POINTER(shz_server_config), C.POINTER(C.c_void_p)]),
     ("shz_server_destroy", None, [C.c_void_p]),
     ("shz_server_error", C.c_char_p, [C.c_void_p]),

@@ -28,6 +28,8 @@ class AmrConfig:
     refine_lo: float = 0.05
     regrid_every: int = 8
     two_pass: bool = False  # predict into a half-step atlas, then update (the reference's passes)
+    time_bins: int = 0  # per-block timesteps: cycles of 2^time_bins substeps (0: one timestep)
+    time_bins_always: bool = False  # never pause the cycles when they save too little
 
     def to_c(self) -> _abi.shz_amr_config:
         c = _abi.shz_amr_config()
@@ -35,6 +37,8 @@ class AmrConfig:
         c.ndim, c.nr, c.max_level, c.cap = self.ndim, self.nr, self.max_level, self.cap
         c.box, c.refine_hi, c.refine_lo, c.regrid_every = self.box, self.refine_hi, self.refine_lo, self.regrid_every
         c.two_pass = 1 if self.two_pass else 0
+        c.time_bins = int(self.time_bins)
+        c.time_bins_always = 1 if self.time_bins_always else 0
         return c
 
     @property
@@ -154,6 +158,21 @@ class AmrSim:
     @property
     def kernel_launches(self) -> int:
         return int(self._lib.shz_amr_kernel_launches(self._h))
+
+    def bins(self):
+        """The last cycle's bin table (cap + 1 ints: the substep, then each slot's bin) and the
+        blocks' own rates per unit cell size it was formed from (AmrSim.readBins)."""
+        b = np.zeros(self.cfg.cap + 1, np.int32)
+        r = np.zeros(self.cfg.cap, np.float32)
+        self._ok(self._lib.shz_amr_bins(self._h, b.ctypes.data, r.ctypes.data))
+        return b, r
+
+    def bin_work(self) -> dict:
+        """Cycles taken, block updates made and what single steps would have made (AmrSim.binWork),
+        and the single steps left before the cycles resume."""
+        cy, up, si, pa = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int32()
+        self._ok(self._lib.shz_amr_bin_work(self._h, C.byref(cy), C.byref(up), C.byref(si), C.byref(pa)))
+        return {"cycles": cy.value, "updates": up.value, "single": si.value, "paused": pa.value}
 
     def uniform_level(self, level: int = 0):
         """Leaves all at one level assembled into a uniform (nz, ny, nx, 4) pair of arrays."""

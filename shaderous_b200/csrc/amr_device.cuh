@@ -332,6 +332,37 @@ __device__ __forceinline__ void load_w(const float4* __restrict__ w1, const floa
   w[4] = b.x; w[5] = b.y; w[6] = b.z;
 }
 
+// Per-block timesteps (amr/bins_on.wgsl). Time advances in cycles of 2^K substeps of the fastest
+// block's step; a block in bin k steps 2^k substeps at a time, starting on substeps that are
+// multiples of 2^k. The bin table holds [0] the substep being taken and [1 + slot] each block's
+// bin; a null table is one timestep for every block (amr/bins_off.wgsl).
+__device__ __forceinline__ int blk_bin(const int* __restrict__ bins, int slot) {
+  return bins ? __ldg(bins + 1 + slot) : 0;
+}
+// The block starts a step on this substep.
+__device__ __forceinline__ bool blk_active(const int* __restrict__ bins, int slot) {
+  if (!bins) return true;
+  return (__ldg(bins) & ((1 << __ldg(bins + 1 + slot)) - 1)) == 0;
+}
+// A leaf part way through a longer step (amr/mid_on.wgsl mid_block): its stored state is already
+// that of the end of its step, and its neighbours take its half-step prediction instead.
+__device__ __forceinline__ bool mid_block(const int* __restrict__ bt, const int* __restrict__ bins, int slot) {
+  return bins && leaf_of(bt, slot) && !blk_active(bins, slot);
+}
+// The conserved state at cell l (interior or first ghost layer) of block `slot` at the middle of
+// its step, from the half-step atlas its prediction wrote when the step began
+// (amr/mid_on.wgsl:18-31 mid_cons; ideal gas, e = p / (gamma - 1)).
+template <int DIM>
+__device__ __forceinline__ Cons mid_cons(const KParams& P, const float4* __restrict__ p1, const float4* __restrict__ p2,
+                                         int slot, const int* l) {
+  const size_t o = (size_t)slot * BG<DIM>::PN + ptex<DIM>(l);
+  const float4 a = __ldg(p1 + o), b = __ldg(p2 + o);
+  const float rho = a.x;
+  const float eint = b.x * P.inv_gm1;
+  return Cons{make_float4(rho, rho * a.y, rho * a.z, rho * a.w),
+              make_float4(eint + 0.5f * rho * (a.y * a.y + a.z * a.z + a.w * a.w), eint, rho * b.y, 0.f)};
+}
+
 }  // namespace amrk
 
 // Persistent work-list grids: `per_sm` CTAs on each of the 148 SMs, or one per block when fewer.

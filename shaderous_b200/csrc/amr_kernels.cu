@@ -441,7 +441,8 @@ cudaError_t amr_launch_regrid(const AmrLaunch& L, const int* rg, const int* list
 // The clocks of many grids at once, one thread each: as clock_kernel (sweep.cu), reading grid
 // g's rate from rates[2 g + rslot] and clearing the other slot for the next step; a grid that
 // has taken max_steps steps holds.
-__global__ void clock_multi_kernel(DevClock* __restrict__ clks, unsigned* __restrict__ rates, int rslot, int ngrids) {
+__global__ void clock_multi_kernel(DevClock* __restrict__ clks, unsigned* __restrict__ rates, int rslot, int ngrids,
+                                   int cycle) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= ngrids) return;
   DevClock& c = clks[g];
@@ -455,7 +456,7 @@ __global__ void clock_multi_kernel(DevClock* __restrict__ clks, unsigned* __rest
   if (te < HUGE_VAL) {
     const double rem = te - t;
     if (rem <= 1e-12 * fabs(te)) dt = 0.0;
-    else dt = fmin(dt, rem);
+    else dt = fmin(dt, rem / cycle);
   }
   if (c.bad || c.steps >= c.max_steps) dt = 0.0;
   c.dt = dt;
@@ -467,9 +468,9 @@ __global__ void clock_multi_kernel(DevClock* __restrict__ clks, unsigned* __rest
   }
 }
 
-cudaError_t launch_clock_multi(DevClock* clks, unsigned* rates, int rslot, int ngrids, cudaStream_t s) {
+cudaError_t launch_clock_multi(DevClock* clks, unsigned* rates, int rslot, int ngrids, cudaStream_t s, int cycle) {
   if (ngrids <= 0) return cudaSuccess;
-  clock_multi_kernel<<<(ngrids + 127) / 128, 128, 0, s>>>(clks, rates, rslot, ngrids);
+  clock_multi_kernel<<<(ngrids + 127) / 128, 128, 0, s>>>(clks, rates, rslot, ngrids, cycle < 1 ? 1 : cycle);
   return cudaGetLastError();
 }
 

@@ -35,11 +35,29 @@ struct AmrLaunch {
 // c: the autotuner's choice (null: the default shape), as for the fine-flux pass and the sweep.
 cudaError_t amr_launch_assemble(const AmrLaunch& L, const int* list, int n, const float4* u1, const float4* u2,
                                 unsigned* rates, int rslot, cudaStream_t s, const tune::Choice* c = nullptr);
-// The clocks of `ngrids` grids at once (one thread each): dt from each grid's rate slot.
-cudaError_t launch_clock_multi(DevClock* clks, unsigned* rates, int rslot, int ngrids, cudaStream_t s);
-cudaError_t amr_launch_predict(const AmrLaunch& L, const int* list, int n, const DevClock* clks, cudaStream_t s);
+// The clocks of `ngrids` grids at once (one thread each): dt from each grid's rate slot. With
+// cycle > 1 (per-block timesteps) the step is repeated for a cycle of that many substeps, and is
+// kept short enough for the cycle to end by the stop time.
+cudaError_t launch_clock_multi(DevClock* clks, unsigned* rates, int rslot, int ngrids, cudaStream_t s, int cycle = 1);
+// The two passes (amr_twopass.cu); bins: the per-block timesteps' bin table (null: one timestep).
+// With bins the update writes in place: o1, o2 are u1, u2.
+cudaError_t amr_launch_predict(const AmrLaunch& L, const int* list, int n, const DevClock* clks, cudaStream_t s,
+                               const int* bins = nullptr);
 cudaError_t amr_launch_update(const AmrLaunch& L, const int* list, int n, const float4* u1, const float4* u2, float4* o1,
-                              float4* o2, const DevClock* clks, cudaStream_t s);
+                              float4* o2, const DevClock* clks, cudaStream_t s, const int* bins = nullptr);
+// Per-block timesteps (amr_bins.cu).
+// The assemble of the blocks in list for a substep: as amr_launch_assemble's per-texel form, with
+// the ghosts of neighbours part way through a longer step taken from their half-step atlas; each
+// leaf's own rate / dx also goes to brate[slot] (if not null).
+cudaError_t amr_launch_assemble_bins(const AmrLaunch& L, const int* list, int n, const float4* u1, const float4* u2,
+                                     const int* bins, unsigned* rates, int rslot, float* brate, cudaStream_t s);
+// The bins of a cycle over the blocks in list (all of them): the first guess from each leaf's rate
+// and the clock's dt into `a`, then the dilation sweep into `b` and `sweeps` (odd) relaxation
+// sweeps alternating b -> a, a -> b, ..., so that the result is in `a`.
+cudaError_t amr_launch_bins(const AmrLaunch& L, const int* list, int n, const float* brate, const DevClock* clk,
+                            float cfl, int kmax, int sweeps, int* a, int* b, cudaStream_t s);
+// Substep s of a cycle begins: the bin table's substep word, and the clock banks the substep.
+cudaError_t amr_launch_bins_tick(DevClock* clk, int* bins, int s, cudaStream_t st);
 // The mean fine fluxes of the matched faces listed in flist (leaf slot, face, buffer entry per
 // face), into L.fbuf; before the sweep.
 cudaError_t amr_launch_fine_flux(const AmrLaunch& L, const int* flist, int nf, const DevClock* clks, cudaStream_t s,

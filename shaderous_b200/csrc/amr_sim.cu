@@ -6,6 +6,8 @@
 // every regrid_every steps the Löhner flags
 // are read back, BlockTree.adapt decides the new mesh on the host, the new tables go up and the
 // regrid kernel fills the new leaves (amr_sim.ts:2648 applyRegrid, :3033 encodeFlags, :3525 readFlags).
+// With per-block timesteps (time_bins) time advances in cycles of 2^time_bins substeps
+// (amr_sim.ts:1509-1660 encodeCycle): see cycle_once.
 #include <cuda_runtime.h>
 
 #include <chrono>
@@ -58,6 +60,18 @@ struct shz_amr {
   long long launches = 0;
   std::string err;
   int device = 0;
+  // Per-block timesteps: the bin tables (the relaxation's two buffers; [0] the substep, [1 + slot]
+  // the bin), each leaf's own rate / dx from the cycle's first assemble, the substeps' block lists
+  // (built on the host from the bins), and the bookkeeping of pauses and work (amr_sim.ts:437-445).
+  int* d_bins[2] = {nullptr, nullptr};
+  float* d_brate = nullptr;
+  int* d_cyc = nullptr;
+  int32_t* h_cyc = nullptr;   // pinned: the lists of a cycle's substeps, uploaded in one copy
+  int32_t* h_bins = nullptr;  // pinned: the bin table read back at the start of each cycle
+  size_t cyc_cap = 0;
+  cudaEvent_t bins_ready = nullptr;
+  int bin_pause = 0, bin_pause_next = 0, cycles_since_poll = 0;
+  long long bin_cycles = 0, bin_updates = 0, bin_single = 0, seen_updates = 0, seen_single = 0;
 };
 
 namespace {
@@ -261,6 +275,156 @@ int step_once(shz_amr* a) {
   return 0;
 }
 
+// Per-block timesteps' pauses (amr_sim.ts:136-151): a run's first single steps, the polls of the
+// cycles' share of block updates, the share above which they pause, and the pauses.
+constexpr int BIN_START_STEPS = 16;
+constexpr int BIN_POLL_CYCLES = 4;
+constexpr double BIN_SHARE_MAX = 0.8;
+constexpr int BIN_PAUSE_STEPS = 192;
+constexpr int BIN_PAUSE_MAX = 1536;
+
+void reset_bins(shz_amr* a) {
+  a->bin_pause = a->cfg.time_bins > 0 ? BIN_START_STEPS : 0;
+  a->bin_pause_next = BIN_PAUSE_STEPS;
+  a->cycles_since_poll = 0;
+  a->bin_cycles = a->bin_updates = a->bin_single = a->seen_updates = a->seen_single = 0;
+}
+
+// Whether leaf `slot` has a face neighbour in a faster bin than its own: a same-level leaf, or a
+// child of a refined same-level neighbour that touches the shared face (amr/bins_lists.wgsl:27-51).
+bool faster_neighbor(const shz_amr* a, const int32_t* kb, int slot) {
+  const int S = shz::amr::BT_STRIDE;
+  const int32_t* bt = a->h_bt.data();
+  const int k = kb[1 + slot];
+  for (int f = 0; f < 2 * a->cfg.ndim; f++) {
+    const int nb = bt[(size_t)slot * S + 6 + f];
+    if (nb < 0 || nb == slot) continue;
+    if (bt[(size_t)nb * S + 4] & 2) {
+      if (kb[1 + nb] < k) return true;
+      continue;
+    }
+    // refined: its children on the shared face (beyond our lower face, its upper children)
+    const int axis = f >> 1, want = 1 - (f & 1);
+    for (int ch = 0; ch < 8; ch++) {
+      if (((ch >> axis) & 1) != want) continue;
+      const int c = bt[(size_t)nb * S + 12 + ch];
+      if (c >= 0 && (bt[(size_t)c * S + 4] & 2) && kb[1 + c] < k) return true;
+    }
+  }
+  return false;
+}
+
+// One cycle of per-block timesteps (amr_sim.ts:1509-1660 encodeCycle): 2^K substeps of the
+// clock's dt, after which every block is at the same time again.
+//   substep 0: every block steps. The assemble measures each leaf's rate; the clock sets the
+//     cycle's dt (short enough for the cycle to end by the stop time); the bins follow from the
+//     rates (first guess, dilation, relaxation); then predict and update, each block with its own
+//     step 2^k dt, and with its faster neighbours' fluxes through the shared faces for half of it.
+//   substeps s = 1 .. 2^K - 1: the blocks that start a step (s a multiple of 2^k) are assembled,
+//     the leaves among them predicted, and updated together with the leaves half way through their
+//     step that have a faster neighbour (the deposit of its second-step fluxes).
+// The bin table is read back once per cycle (while substep 0's passes run) and the substeps'
+// lists are built here, in the order of the block list (amr/bins_lists.wgsl gathers them with
+// atomics in no fixed order; no result depends on it). The state stays in one parity: the update
+// writes in place.
+int cycle_once(shz_amr* a) {
+  const int K = a->cfg.time_bins, n = 1 << K;
+  float4* u1 = a->u1[a->cur];
+  float4* u2 = a->u2[a->cur];
+  int* A = a->d_bins[0];
+  int* B = a->d_bins[1];
+  const int na = n_all(a), nl = n_leaves(a);
+  unsigned* scratch = a->rates + 4;  // the later substeps' assembles: rates nothing reads
+  AMR_CUDA(a, shz::amr_launch_bins_tick(a->clk, A, 0, a->stream));
+  AMR_CUDA(a, shz::amr_launch_assemble_bins(a->L, a->d_all, na, u1, u2, A, a->rates, a->slot, a->d_brate, a->stream));
+  AMR_CUDA(a, shz::launch_clock_multi(a->clk, a->rates, a->slot, 1, a->stream, n));
+  const int sweeps = (K + a->cfg.max_level + 2) | 1;
+  AMR_CUDA(a, shz::amr_launch_bins(a->L, a->d_all, na, a->d_brate, a->clk, (float)a->cfg.hydro.cfl, K, sweeps, A, B,
+                                   a->stream));
+  AMR_CUDA(a, cudaMemcpyAsync(a->h_bins, A, (size_t)(a->cfg.cap + 1) * sizeof(int32_t), cudaMemcpyDeviceToHost, a->stream));
+  AMR_CUDA(a, cudaMemcpyAsync(a->h_bins + a->cfg.cap + 1, &a->clk->held, sizeof(int), cudaMemcpyDeviceToHost, a->stream));
+  AMR_CUDA(a, cudaEventRecord(a->bins_ready, a->stream));
+  AMR_CUDA(a, shz::amr_launch_predict(a->L, a->d_leaves, nl, a->clk, a->stream, A));
+  AMR_CUDA(a, shz::amr_launch_update(a->L, a->d_leaves, nl, u1, u2, u1, u2, a->clk, a->stream, A));
+  a->launches += 7 + sweeps;
+  a->slot ^= 1;
+  AMR_CUDA(a, cudaEventSynchronize(a->bins_ready));
+  if (a->h_bins[a->cfg.cap + 1]) return 0;  // a held cycle: nothing to step
+  // the substeps' lists: per substep the counts of LA (assembled), LL (predicted), LU (updated),
+  // then the three lists
+  const size_t per = 3 + (size_t)na + 2 * (size_t)nl;
+  const size_t need = (size_t)(n - 1) * per;
+  if (need > a->cyc_cap) {
+    cudaFree(a->d_cyc);
+    cudaFreeHost(a->h_cyc);
+    a->d_cyc = nullptr;
+    a->h_cyc = nullptr;
+    a->cyc_cap = 0;
+    if (cudaMalloc(&a->d_cyc, need * sizeof(int32_t)) != cudaSuccess ||
+        cudaMallocHost(&a->h_cyc, need * sizeof(int32_t)) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(a, SHZ_E_OOM, "the block lists of a cycle (%zu ints) do not fit", need);
+    }
+    a->cyc_cap = need;
+  }
+  const int32_t* kb = a->h_bins;
+  const int32_t* bt = a->h_bt.data();
+  const int S = shz::amr::BT_STRIDE;
+  long long updates = nl;
+  for (int sub = 1; sub < n; sub++) {
+    int32_t* rec = a->h_cyc + (size_t)(sub - 1) * per;
+    int32_t* la = rec + 3;
+    int32_t* ll = la + na;
+    int32_t* lu = ll + nl;
+    int ca = 0, cl = 0, cu = 0;
+    for (int slot : a->h_all) {
+      const int k = kb[1 + slot];
+      const int phase = sub & ((1 << k) - 1);
+      const bool on = phase == 0;
+      const bool leaf = (bt[(size_t)slot * S + 4] & 2) != 0;
+      if (on) la[ca++] = slot;
+      if (on && leaf) ll[cl++] = slot;
+      const bool deposit = leaf && !on && k > 0 && phase == (1 << (k - 1)) && faster_neighbor(a, kb, slot);
+      if (leaf && (on || deposit)) lu[cu++] = slot;
+    }
+    rec[0] = ca;
+    rec[1] = cl;
+    rec[2] = cu;
+    updates += cu;
+  }
+  AMR_CUDA(a, cudaMemcpyAsync(a->d_cyc, a->h_cyc, need * sizeof(int32_t), cudaMemcpyHostToDevice, a->stream));
+  for (int sub = 1; sub < n; sub++) {
+    const int32_t* rec = a->h_cyc + (size_t)(sub - 1) * per;
+    const int* la = a->d_cyc + (size_t)(sub - 1) * per + 3;
+    const int* ll = la + na;
+    const int* lu = ll + nl;
+    AMR_CUDA(a, shz::amr_launch_bins_tick(a->clk, A, sub, a->stream));
+    AMR_CUDA(a, shz::amr_launch_assemble_bins(a->L, la, rec[0], u1, u2, A, scratch, 0, nullptr, a->stream));
+    AMR_CUDA(a, shz::amr_launch_predict(a->L, ll, rec[1], a->clk, a->stream, A));
+    AMR_CUDA(a, shz::amr_launch_update(a->L, lu, rec[2], u1, u2, u1, u2, a->clk, a->stream, A));
+    a->launches += 1 + (rec[0] > 0) + (rec[1] > 0) + (rec[2] > 0);
+  }
+  a->bin_cycles++;
+  a->bin_updates += updates;
+  a->bin_single += (long long)nl << K;
+  // a poll every few cycles: above the share, single steps for a while, longer each time
+  if (++a->cycles_since_poll >= BIN_POLL_CYCLES) {
+    a->cycles_since_poll = 0;
+    const long long du = a->bin_updates - a->seen_updates, ds = a->bin_single - a->seen_single;
+    a->seen_updates = a->bin_updates;
+    a->seen_single = a->bin_single;
+    if (ds > 0 && !a->cfg.time_bins_always) {
+      if ((double)du / (double)ds > BIN_SHARE_MAX) {
+        a->bin_pause = a->bin_pause_next;
+        a->bin_pause_next = std::min(BIN_PAUSE_MAX, 2 * a->bin_pause_next);
+      } else {
+        a->bin_pause_next = BIN_PAUSE_STEPS;
+      }
+    }
+  }
+  return 0;
+}
+
 // The refinement indicators of the current state: a fresh assemble, then the Löhner pass.
 int compute_flags(shz_amr* a) {
   AMR_CUDA(a, cudaMemsetAsync(a->rates + 2, 0, 2 * sizeof(unsigned), a->stream));
@@ -413,6 +577,7 @@ int shz_amr_create(const shz_amr_config* cfg, shz_amr** out) {
   if (c.ndim != 2 && c.ndim != 3) return refuse("ndim must be 2 or 3");
   if (c.nr < 1 || c.max_level < 0 || c.max_level > shz::amr::MAX_LEVELS) return refuse("nr >= 1 and max_level 0..7");
   if (c.hydro.recon == SHZ_RECON_PPM) return refuse("PPM reaches three cells; the blocks keep two ghost layers");
+  if (c.time_bins < 0 || c.time_bins > 5) return refuse("time_bins is 0 (off) to 5 (cycles of 32 substeps)");
   if (c.hydro.recon < 0 || c.hydro.recon > SHZ_RECON_KOREN) return refuse("recon must be minmod, mc, vanleer or koren");
   if (!(c.box > 0) || !(c.hydro.gamma > 1) || !(c.hydro.cfl > 0)) return refuse("box > 0, gamma > 1, cfl > 0");
   for (int ax = 0; ax < 3; ax++)
@@ -429,6 +594,8 @@ int shz_amr_create(const shz_amr_config* cfg, shz_amr** out) {
   Dev dv(c.hydro.device);
   shz_amr* a = new shz_amr();
   a->cfg = c;
+  // per-block timesteps run on the two passes, whose half-step atlas they keep
+  if (c.time_bins > 0) a->cfg.two_pass = 1;
   a->device = c.hydro.device;
   a->CB = c.ndim == 3 ? 4096 : 256;
   a->WN = c.ndim == 3 ? 8000 : 400;
@@ -451,7 +618,7 @@ int shz_amr_create(const shz_amr_config* cfg, shz_amr** out) {
   a->L.ndim = c.ndim;
   a->L.recon = c.hydro.recon;
   a->L.isen = c.hydro.isentropic != 0;
-  a->L.per_texel = c.two_pass != 0;
+  a->L.per_texel = a->cfg.two_pass != 0;
   auto bail = [&](int code, const char* what) {
     g_create_err = what;
     shz_amr_destroy(a);
@@ -466,7 +633,7 @@ int shz_amr_create(const shz_amr_config* cfg, shz_amr** out) {
   }
   ok = ok && cudaMalloc(&a->w1, cap * a->WN * sizeof(float4)) == cudaSuccess;
   ok = ok && cudaMalloc(&a->w2, cap * a->WN * sizeof(float4)) == cudaSuccess;
-  if (c.two_pass) {
+  if (a->cfg.two_pass) {
     ok = ok && cudaMalloc(&a->p1, cap * a->PN * sizeof(float4)) == cudaSuccess;
     ok = ok && cudaMalloc(&a->p2, cap * a->PN * sizeof(float4)) == cudaSuccess;
   }
@@ -476,7 +643,18 @@ int shz_amr_create(const shz_amr_config* cfg, shz_amr** out) {
   ok = ok && cudaMalloc(&a->d_rg, cap * shz::amr::RG_STRIDE * sizeof(int)) == cudaSuccess;
   ok = ok && cudaMalloc(&a->d_flags, cap * sizeof(float)) == cudaSuccess;
   ok = ok && cudaMalloc(&a->clk, sizeof(shz::DevClock)) == cudaSuccess;
-  ok = ok && cudaMalloc(&a->rates, 4 * sizeof(unsigned)) == cudaSuccess;
+  ok = ok && cudaMalloc(&a->rates, 6 * sizeof(unsigned)) == cudaSuccess;
+  if (ok) ok = cudaMemset(a->rates, 0, 6 * sizeof(unsigned)) == cudaSuccess;
+  if (c.time_bins > 0) {
+    for (int p = 0; p < 2; p++) {
+      ok = ok && cudaMalloc(&a->d_bins[p], (cap + 1) * sizeof(int)) == cudaSuccess;
+      if (ok) ok = cudaMemset(a->d_bins[p], 0, (cap + 1) * sizeof(int)) == cudaSuccess;
+    }
+    ok = ok && cudaMalloc(&a->d_brate, cap * sizeof(float)) == cudaSuccess;
+    if (ok) ok = cudaMemset(a->d_brate, 0, cap * sizeof(float)) == cudaSuccess;
+    ok = ok && cudaMallocHost(&a->h_bins, (cap + 2) * sizeof(int32_t)) == cudaSuccess;
+    ok = ok && cudaEventCreateWithFlags(&a->bins_ready, cudaEventDisableTiming) == cudaSuccess;
+  }
   ok = ok && cudaMalloc(&a->d_gp, sizeof(shz::KParams)) == cudaSuccess;
   // (room for the 9 totals or the 13 extended channels per block)
   ok = ok && cudaMalloc(&a->diag_part, (size_t)shz::amr_diag_blocks(c.cap) * 16 * sizeof(double)) == cudaSuccess;
@@ -488,7 +666,7 @@ int shz_amr_create(const shz_amr_config* cfg, shz_amr** out) {
     cudaGetLastError();
     char buf[160];
     snprintf(buf, sizeof buf, "the atlases of %d block slots (%.2f GB) do not fit", c.cap,
-             cap * (4.0 * a->CB + 2.0 * a->WN + (c.two_pass ? 2.0 * a->PN : 0.0)) * 16 / 1e9);
+             cap * (4.0 * a->CB + 2.0 * a->WN + (a->cfg.two_pass ? 2.0 * a->PN : 0.0)) * 16 / 1e9);
     return bail(SHZ_E_OOM, buf);
   }
   a->L.bt = a->d_bt;
@@ -505,6 +683,7 @@ int shz_amr_create(const shz_amr_config* cfg, shz_amr** out) {
     return bail(SHZ_E_CONFIG, e.what());
   }
   if (upload_tables(a) || write_clock(a, 0.0, 0)) return bail(SHZ_E_CUDA, a->err.c_str());
+  reset_bins(a);
   *out = a;
   return SHZ_OK;
 }
@@ -519,9 +698,13 @@ void shz_amr_destroy(shz_amr* a) {
     cudaFree(a->u2[p]);
   }
   void* bufs[] = {a->w1, a->w2, a->p1, a->p2, a->d_bt, a->d_all, a->d_leaves, a->d_rg, a->d_flags, a->d_gp,
-                  a->clk, a->rates, a->diag_part, a->diag_out, a->d_ghost, a->d_flist, a->fbuf, a->d_err};
+                  a->clk, a->rates, a->diag_part, a->diag_out, a->d_ghost, a->d_flist, a->fbuf, a->d_err,
+                  a->d_bins[0], a->d_bins[1], a->d_brate, a->d_cyc};
   for (void* b : bufs)
     if (b) cudaFree(b);
+  if (a->h_bins) cudaFreeHost(a->h_bins);
+  if (a->h_cyc) cudaFreeHost(a->h_cyc);
+  if (a->bins_ready) cudaEventDestroy(a->bins_ready);
   if (a->stream) cudaStreamDestroy(a->stream);
   delete a;
 }
@@ -562,16 +745,23 @@ int shz_amr_reset_problem(shz_amr* a, const shz_problem* prob) {
     if (!changed) break;
   }
   a->since_check = 0;
+  reset_bins(a);
   return write_clock(a, 0.0, 0);
 }
 
 int shz_amr_step(shz_amr* a, int32_t n) {
   if (!a || n < 0) return SHZ_E_CONFIG;
   Dev dv(a->device);
-  for (int i = 0; i < n; i++) {
-    int rc = step_once(a);
+  for (int i = 0; i < n;) {
+    // with per-block timesteps, whole cycles (which may run past n), unless paused
+    const bool cycle = a->cfg.time_bins > 0 && a->bin_pause == 0;
+    if (!cycle && a->bin_pause > 0) a->bin_pause--;
+    int rc = cycle ? cycle_once(a) : step_once(a);
     if (rc) return rc;
-    if (a->cfg.regrid_every > 0 && ++a->since_check >= a->cfg.regrid_every) {
+    const int took = cycle ? 1 << a->cfg.time_bins : 1;
+    i += took;
+    a->since_check += took;
+    if (a->cfg.regrid_every > 0 && a->since_check >= a->cfg.regrid_every) {
       a->since_check = 0;
       int changed = 0;
       if ((rc = check_and_regrid(a, nullptr, &changed))) return rc;
@@ -782,5 +972,29 @@ int shz_amr_profile(shz_amr* a, int32_t n, shz_profile_result* out) {
 }
 
 int64_t shz_amr_kernel_launches(const shz_amr* a) { return a ? a->launches : 0; }
+
+int shz_amr_bins(shz_amr* a, int32_t* bins, float* rates) {
+  if (!a || !bins) return SHZ_E_CONFIG;
+  Dev dv(a->device);
+  const int cap = a->cfg.cap;
+  if (a->cfg.time_bins <= 0) {
+    std::memset(bins, 0, (size_t)(cap + 1) * sizeof(int32_t));
+    if (rates) std::memset(rates, 0, (size_t)cap * sizeof(float));
+    return 0;
+  }
+  AMR_CUDA(a, cudaMemcpyAsync(bins, a->d_bins[0], (size_t)(cap + 1) * sizeof(int32_t), cudaMemcpyDeviceToHost, a->stream));
+  if (rates) AMR_CUDA(a, cudaMemcpyAsync(rates, a->d_brate, (size_t)cap * sizeof(float), cudaMemcpyDeviceToHost, a->stream));
+  AMR_CUDA(a, cudaStreamSynchronize(a->stream));
+  return check_err(a);
+}
+
+int shz_amr_bin_work(shz_amr* a, int64_t* cycles, int64_t* updates, int64_t* single, int32_t* paused) {
+  if (!a) return SHZ_E_CONFIG;
+  if (cycles) *cycles = a->bin_cycles;
+  if (updates) *updates = a->bin_updates;
+  if (single) *single = a->bin_single;
+  if (paused) *paused = a->bin_pause;
+  return 0;
+}
 
 }  // extern "C"
