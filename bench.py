@@ -72,16 +72,20 @@ def parse():
     return ap.parse_args()
 
 
-def amr_sedov(levels=4, nr=8, radius_cells=3.5, steps=24, cap=26000, grown=False, profile_window=False):
+def amr_sedov(levels=4, nr=8, radius_cells=3.5, steps=24, cap=26000, grown=False, profile_window=False, time_bins=0,
+              two_pass=False):
     """3D Sedov blast on the block grid: 16^3-cell blocks, levels 0-levels above nr^3 roots (finest
     nr * 16 << levels cells per side), E = 1 spread over the finest cells within radius_cells of
     the centre, Löhner refinement above 0.1 (below 0.05 merges), a refinement check every 8 steps.
-    Zone-updates are leaf cells x steps, the leaves counted at the start and end of the timed run."""
+    Zone-updates are leaf cells x steps, the leaves counted at the start and end of the timed run.
+    With per-block timesteps (time_bins) a step is a substep of the cycles (the fastest block's
+    step), so the same figure counts the single-step work the cycles stand for."""
     from shaderous_b200 import Config, Problem
     from shaderous_b200.amr import AmrConfig, AmrSim
 
     hyd = Config(gamma=5 / 3, bc_lo=(1, 1, 1), bc_hi=(1, 1, 1), recon="koren", isentropic=True, cfl=0.5, p_floor=1e-12)
-    cfg = AmrConfig(hydro=hyd, ndim=3, nr=nr, max_level=levels, cap=cap, refine_hi=0.1, refine_lo=0.05, regrid_every=8)
+    cfg = AmrConfig(hydro=hyd, ndim=3, nr=nr, max_level=levels, cap=cap, refine_hi=0.1, refine_lo=0.05, regrid_every=8,
+                    two_pass=two_pass, time_bins=time_bins, time_bins_always=time_bins > 0)
     t0 = time.perf_counter()
     with AmrSim(cfg) as a:
         if grown:
@@ -92,7 +96,8 @@ def amr_sedov(levels=4, nr=8, radius_cells=3.5, steps=24, cap=26000, grown=False
             prob = Problem("sedov", a=(1.0, 1e-5, 1.0, radius_cells))
         a.reset(prob)
         t_init = time.perf_counter() - t0
-        a.profile(8)  # warm-up, including one refinement check
+        # warm-up, including one refinement check (and, with bins, the run's first single steps)
+        a.profile(8 if not time_bins else 16 + (1 << time_bins))
         if profile_window:
             # one graph-replayed step between cudaProfilerStart/Stop, for `ncu --profile-from-start off`
             import torch
@@ -106,11 +111,16 @@ def amr_sedov(levels=4, nr=8, radius_cells=3.5, steps=24, cap=26000, grown=False
         n0 = len(a.leaves()[0])
         l0 = a.kernel_launches
         prof = a.profile(steps)
+        steps = prof["steps"]
         n1 = len(a.leaves()[0])
         _, lv, _ = a.leaves()
         launches = a.kernel_launches - l0
+        work = a.bin_work() if time_bins else None
     leaf_cells = 0.5 * (n0 + n1) * 4096
-    return {"value": leaf_cells * steps / (prof["total_ms"] / 1000.0), "unit": UNIT, "steps": steps,
+    extra = {}
+    if work:
+        extra = {"time_bins": time_bins, "block_update_share": work["updates"] / max(work["single"], 1)}
+    return {"value": leaf_cells * steps / (prof["total_ms"] / 1000.0), "unit": UNIT, "steps": steps, **extra,
             "ms_per_step": prof["total_ms"] / steps, "leaf_blocks": [n0, n1], "levels": int(lv.max()) + 1,
             "finest_cells_per_side": nr * 16 << levels, "radius_finest_cells": 0.2 * (nr * 16 << levels) if grown else radius_cells,
             "init_s": t_init, "gpu_launches": launches,

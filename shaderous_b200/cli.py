@@ -42,7 +42,7 @@ PRESETS = {
 }
 ALIASES = {"kh": "kelvin-helmholtz", "tgv": "taylor-green", "advect": "advection"}
 NUMERIC = {"gamma", "cfl", "rho_floor", "p_floor", "eta_dual", "shock_thresh", "box", "t_end", "refine_hi", "refine_lo"}
-INTEGER = {"dim", "n", "amr", "seed", "signal_dims", "regrid_every", "cap", "bc"}
+INTEGER = {"dim", "n", "amr", "seed", "signal_dims", "regrid_every", "cap", "bc", "tbins"}
 
 
 def parse_setup(query: str | None, ns) -> dict:
@@ -102,7 +102,8 @@ def build(setup: dict):
             raise SystemExit("error: an adaptive run needs dim 2 or 3 and n a multiple of 16 (the level-0 grid)")
         acfg = AmrConfig(hydro=cfg, ndim=dim, nr=n // 16, max_level=levels - 1, cap=int(setup.get("cap", 26000)),
                          box=box, refine_hi=float(setup.get("refine_hi", 0.1)),
-                         refine_lo=float(setup.get("refine_lo", 0.05)), regrid_every=int(setup.get("regrid_every", 8)))
+                         refine_lo=float(setup.get("refine_lo", 0.05)), regrid_every=int(setup.get("regrid_every", 8)),
+                         time_bins=int(setup.get("tbins", 0)))
         return AmrSim, acfg, prob, t_end
     return Sim, cfg, prob, t_end
 

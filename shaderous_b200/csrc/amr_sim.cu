@@ -560,6 +560,29 @@ int sample_leaves(shz_amr* a, const shz::ProblemCtx& q) {
   return rc;
 }
 
+// n steps (substeps of whole cycles with per-block timesteps, which may run past n); *taken: the
+// steps taken.
+int step_n(shz_amr* a, int n, int* taken) {
+  int i = 0;
+  while (i < n) {
+    // with per-block timesteps, whole cycles (which may run past n), unless paused
+    const bool cycle = a->cfg.time_bins > 0 && a->bin_pause == 0;
+    if (!cycle && a->bin_pause > 0) a->bin_pause--;
+    int rc = cycle ? cycle_once(a) : step_once(a);
+    if (rc) return rc;
+    const int took = cycle ? 1 << a->cfg.time_bins : 1;
+    i += took;
+    a->since_check += took;
+    if (a->cfg.regrid_every > 0 && a->since_check >= a->cfg.regrid_every) {
+      a->since_check = 0;
+      int changed = 0;
+      if ((rc = check_and_regrid(a, nullptr, &changed))) return rc;
+    }
+  }
+  if (taken) *taken = i;
+  return 0;
+}
+
 }  // namespace
 
 extern "C" {
@@ -752,22 +775,7 @@ int shz_amr_reset_problem(shz_amr* a, const shz_problem* prob) {
 int shz_amr_step(shz_amr* a, int32_t n) {
   if (!a || n < 0) return SHZ_E_CONFIG;
   Dev dv(a->device);
-  for (int i = 0; i < n;) {
-    // with per-block timesteps, whole cycles (which may run past n), unless paused
-    const bool cycle = a->cfg.time_bins > 0 && a->bin_pause == 0;
-    if (!cycle && a->bin_pause > 0) a->bin_pause--;
-    int rc = cycle ? cycle_once(a) : step_once(a);
-    if (rc) return rc;
-    const int took = cycle ? 1 << a->cfg.time_bins : 1;
-    i += took;
-    a->since_check += took;
-    if (a->cfg.regrid_every > 0 && a->since_check >= a->cfg.regrid_every) {
-      a->since_check = 0;
-      int changed = 0;
-      if ((rc = check_and_regrid(a, nullptr, &changed))) return rc;
-    }
-  }
-  return 0;
+  return step_n(a, n, nullptr);
 }
 
 int shz_amr_regrid(shz_amr* a, int32_t* changed) {
@@ -955,7 +963,8 @@ int shz_amr_profile(shz_amr* a, int32_t n, shz_profile_result* out) {
   AMR_CUDA(a, cudaEventCreate(&e1));
   const long long l0 = a->launches;
   AMR_CUDA(a, cudaEventRecord(e0, a->stream));
-  int rc = shz_amr_step(a, n);
+  int taken = 0;
+  int rc = step_n(a, n, &taken);
   AMR_CUDA(a, cudaEventRecord(e1, a->stream));
   AMR_CUDA(a, cudaEventSynchronize(e1));
   float ms = 0.f;
@@ -964,7 +973,7 @@ int shz_amr_profile(shz_amr* a, int32_t n, shz_profile_result* out) {
   cudaEventDestroy(e1);
   if (rc) return rc;
   if ((rc = check_err(a))) return rc;
-  out->steps = n;
+  out->steps = taken;
   out->total_ms = ms;
   out->sweep_ms = ms;
   out->launches = a->launches - l0;

@@ -37,6 +37,11 @@ def test_build_configs():
     assert cfg.recon == "ppm" and prob.kind == "tgv" and t_end == 1.0
     cls, cfg, prob, _ = build({"problem": "sedov", "dim": 3, "n": 32, "amr": 3})
     assert cls.__name__ == "AmrSim" and cfg.nr == 2 and cfg.max_level == 2 and cfg.hydro.bc_lo == (1, 1, 1)
+    assert cfg.time_bins == 0
+    # the reference's link parameter for per-block timesteps (tests/unit/levels.test.ts:37)
+    s = parse_setup("problem=sedov&dim=2&n=2048&amr=7&tbins=5", ns())
+    _, cfg, _, _ = build(s)
+    assert cfg.time_bins == 5 and cfg.max_level == 6 and cfg.nr == 128
     cls, cfg, _, _ = build({"problem": "sod", "dim": 1, "n": 512})
     assert cfg.n == (512, 1, 1) and cfg.bc_lo == (1, 0, 0) and cfg.recon == "minmod"
     assert set(PRESETS) >= {"sod", "kelvin-helmholtz", "sedov", "taylor-green", "blast"}
