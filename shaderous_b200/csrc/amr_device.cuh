@@ -363,6 +363,46 @@ __device__ __forceinline__ Cons mid_cons(const KParams& P, const float4* __restr
               make_float4(eint + 0.5f * rho * (a.y * a.y + a.z * a.z + a.w * a.w), eint, rho * b.y, 0.f)};
 }
 
+// coarse_cell for a coarse leaf part way through its step: the coarse cell and its neighbours
+// along the axes from its half-step atlas (which covers its first ghost layer, so no boundary
+// mapping is needed; amr/assemble.wgsl:59-66).
+template <int DIM, int R>
+__device__ __forceinline__ void coarse_cell_mid(const KParams& P, const int* __restrict__ bt, const float4* __restrict__ p1,
+                                                const float4* __restrict__ p2, int nr, int slot, const int* l, int cs,
+                                                Cons& uc, Slopes& sl, int* par) {
+  const int nc = nr * BS << bt_at(bt, cs, 0);
+  int lc[3];
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const int gf = a < DIM ? bt_at(bt, slot, 1 + a) * BS + l[a] : 0;
+    int gc = gf >> 1;
+    gc = ((gc % nc) + nc) % nc;
+    lc[a] = a < DIM ? gc - bt_at(bt, cs, 1 + a) * BS : 0;
+    par[a] = a < DIM ? (gf & 1) : 0;
+  }
+  uc = mid_cons<DIM>(P, p1, p2, cs, lc);
+  Cons m[3], p[3];
+  bool ok[3] = {true, true, true};
+#pragma unroll
+  for (int a = 0; a < DIM; a++) {
+    int at[3] = {lc[0], lc[1], lc[2]};
+    at[a] -= 1;
+    m[a] = mid_cons<DIM>(P, p1, p2, cs, at);
+    at[a] += 2;
+    p[a] = mid_cons<DIM>(P, p1, p2, cs, at);
+  }
+  sl = prolong_slopes<DIM, R>(uc, m, ok, p, ok, P.rho_floor);
+}
+template <int DIM, int R>
+__device__ __forceinline__ Cons from_coarse_mid(const KParams& P, const int* __restrict__ bt, const float4* __restrict__ p1,
+                                                const float4* __restrict__ p2, int nr, int slot, const int* l, int cs) {
+  Cons uc;
+  Slopes sl;
+  int par[3];
+  coarse_cell_mid<DIM, R>(P, bt, p1, p2, nr, slot, l, cs, uc, sl, par);
+  return prolong_child(uc, sl, par);
+}
+
 }  // namespace amrk
 
 // Persistent work-list grids: `per_sm` CTAs on each of the 148 SMs, or one per block when fewer.

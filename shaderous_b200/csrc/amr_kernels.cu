@@ -62,12 +62,17 @@ __device__ __forceinline__ void tab_load(const float* e, Cons& uc, Slopes& sl) {
 // block's face take their coarse cell's state and slopes from the block's table (built first,
 // once per coarse cell); with per_texel (the two-pass mode, the reference's structure) each
 // ghost forms them itself. Both give the same numbers.
-template <int DIM, int R, int MINB>
+// With per-block timesteps (BINS, the bin table `bins`), a source leaf part way through its step
+// gives its half-step state from p1, p2 (amr/assemble.wgsl with <mid>, amr/mid_on.wgsl), and each
+// leaf's own rate / dx also goes to brate[slot] for its bin.
+template <int DIM, int R, int MINB, bool BINS>
 __global__ void __launch_bounds__(NT, MINB) amr_assemble(const KParams* __restrict__ gp, const int* __restrict__ bt,
                                                    const int* __restrict__ list, int n, const float4* __restrict__ u1,
                                                    const float4* __restrict__ u2, float4* __restrict__ w1,
                                                    float4* __restrict__ w2, unsigned* __restrict__ rates, int rslot,
-                                                   int per_texel) {
+                                                   int per_texel, const float4* __restrict__ p1,
+                                                   const float4* __restrict__ p2, const int* __restrict__ bins,
+                                                   float* __restrict__ brate) {
   using T = Tab<DIM>;
   __shared__ float sRed[NT / 32];
   extern __shared__ __align__(16) float sTab[];
@@ -105,7 +110,9 @@ __global__ void __launch_bounds__(NT, MINB) amr_assemble(const KParams* __restri
         Cons uc;
         Slopes sl;
         int par[3];
-        coarse_cell<DIM, R>(bt, u1, u2, nr, slot, m, bt_at(bt, slot, 20 + f), P.rho_floor, uc, sl, par);
+        const int cs = bt_at(bt, slot, 20 + f);
+        if (BINS && mid_block(bt, bins, cs)) coarse_cell_mid<DIM, R>(P, bt, p1, p2, nr, slot, m, cs, uc, sl, par);
+        else coarse_cell<DIM, R>(bt, u1, u2, nr, slot, m, cs, P.rho_floor, uc, sl, par);
         tab_store(sTab + (size_t)(f * T::CPF + c) * TAB_VALS, uc, sl);
       }
       __syncthreads();
@@ -115,7 +122,8 @@ __global__ void __launch_bounds__(NT, MINB) amr_assemble(const KParams* __restri
       const Src s = ghost_src_any<DIM>(bt, slot, l);
       Cons u;
       if (s.kind == 0) {
-        u = u_at<DIM>(bt, u1, u2, s.slot, s.l);
+        if (BINS && mid_block(bt, bins, s.slot)) u = mid_cons<DIM>(P, p1, p2, s.slot, s.l);
+        else u = u_at<DIM>(bt, u1, u2, s.slot, s.l);
       } else if (cmask && s.from == slot) {
         // a ghost of this block's own coarse face: its coarse cell from the table
         int a = 0;
@@ -129,6 +137,8 @@ __global__ void __launch_bounds__(NT, MINB) amr_assemble(const KParams* __restri
         tab_load(sTab + (size_t)(f * T::CPF + c) * TAB_VALS, uc, sl);
         const int par[3] = {s.l[0] & 1, s.l[1] & 1, DIM == 3 ? (s.l[2] & 1) : 0};
         u = prolong_child(uc, sl, par);
+      } else if (BINS && mid_block(bt, bins, s.slot)) {
+        u = from_coarse_mid<DIM, R>(P, bt, p1, p2, nr, s.from, s.l, s.slot);
       } else {
         u = from_coarse<DIM, R>(bt, u1, u2, nr, s.from, s.l, s.slot, P.rho_floor);
       }
@@ -146,7 +156,10 @@ __global__ void __launch_bounds__(NT, MINB) amr_assemble(const KParams* __restri
       if (inside) rmax = fmaxf(rmax, rate_guard_f(fabsf(w[1]) + fabsf(w[2]) + fabsf(w[3]) + P.signal * w[6]) * inv_dx);
     }
     const float m = block_max(rmax, sRed);
-    if (threadIdx.x == 0 && leaf) atomicMax(rates + 2 * g + rslot, __float_as_uint(m));
+    if (threadIdx.x == 0 && leaf) {
+      atomicMax(rates + 2 * g + rslot, __float_as_uint(m));
+      if (BINS && brate) brate[slot] = m;
+    }
   }
 }
 
@@ -383,16 +396,17 @@ __global__ void amr_ghost_map(const int* __restrict__ bt, int slot, int* __restr
 // Host launchers.
 
 namespace {
-template <int DIM, int R, int MINB>
+template <int DIM, int R, int MINB, bool BINS = false>
 cudaError_t assemble_t(const AmrLaunch& L, int g, const int* list, int n, const float4* u1, const float4* u2,
-                       unsigned* rates, int rslot, cudaStream_t s) {
-  auto k = amrk::amr_assemble<DIM, R, MINB>;
+                       unsigned* rates, int rslot, cudaStream_t s, const int* bins = nullptr, float* brate = nullptr) {
+  auto k = amrk::amr_assemble<DIM, R, MINB, BINS>;
   // (set once per instantiation; not a stream operation)
   static const cudaError_t attr =
       cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)amrk::Tab<DIM>::BYTES);
   if (attr != cudaSuccess) return attr;
   const size_t smem = L.per_texel ? 0 : amrk::Tab<DIM>::BYTES;
-  k<<<g, amrk::NT, smem, s>>>(L.gp, L.bt, list, n, u1, u2, L.w1, L.w2, rates, rslot, L.per_texel ? 1 : 0);
+  k<<<g, amrk::NT, smem, s>>>(L.gp, L.bt, list, n, u1, u2, L.w1, L.w2, rates, rslot, L.per_texel ? 1 : 0, L.p1, L.p2,
+                              bins, brate);
   return cudaGetLastError();
 }
 template <int MINB>
@@ -416,6 +430,18 @@ cudaError_t amr_launch_assemble(const AmrLaunch& L, const int* list, int n, cons
     case 2: return assemble_v<3>(L, g, list, n, u1, u2, rates, rslot, s);
     default: return assemble_v<1>(L, g, list, n, u1, u2, rates, rslot, s);
   }
+}
+
+cudaError_t amr_launch_assemble_bins(const AmrLaunch& L, const int* list, int n, const float4* u1, const float4* u2,
+                                     const int* bins, unsigned* rates, int rslot, float* brate, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  const int g = grid_for(n, 4);
+  if (L.ndim == 3) {
+    SHZ_RECON_SWITCH(L.recon, false, return (assemble_t<3, R, 1, true>(L, g, list, n, u1, u2, rates, rslot, s, bins, brate)))
+  } else {
+    SHZ_RECON_SWITCH(L.recon, false, return (assemble_t<2, R, 1, true>(L, g, list, n, u1, u2, rates, rslot, s, bins, brate)))
+  }
+  return cudaSuccess;
 }
 
 cudaError_t amr_launch_flag(const AmrLaunch& L, const int* list, int n, float* flags, cudaStream_t s) {

@@ -29,6 +29,11 @@ struct AmrLaunch {
   // The assemble forms every coarse ghost's prolongation itself, as the reference does (the two-pass
   // mode), instead of from its per-block table of coarse cells; the numbers are the same.
   bool per_texel = false;
+  // Per-block timesteps, for the fused sweep, its neighbour-flux pass and the deposits: the bin
+  // table ([0] the substep, [1 + slot] the bin; null: one timestep) and, per slot, the first entry
+  // of its faces' fluxes in fbuf for this substep (-1: none).
+  const int* bins = nullptr;
+  const int* fbase = nullptr;
 };
 
 // rates: two 32-bit maxima per grid; the assemble folds the leaves' rate / dx into slot rslot.
@@ -66,6 +71,10 @@ cudaError_t amr_launch_fine_flux(const AmrLaunch& L, const int* flist, int nf, c
 // atlas), standing for predict + update.
 cudaError_t amr_launch_sweep(const AmrLaunch& L, const int* list, int n, const float4* u1, const float4* u2, float4* o1,
                              float4* o2, const DevClock* clks, cudaStream_t s, const tune::Choice* c = nullptr);
+// Per-block timesteps, fused form: the leaves in list half way through their step beside a faster
+// neighbour take that neighbour's second-step fluxes from fbuf, in place (amr/update.wgsl deposit).
+cudaError_t amr_launch_deposit(const AmrLaunch& L, const int* list, int n, float4* u1, float4* u2, const DevClock* clks,
+                               cudaStream_t s);
 cudaError_t amr_launch_flag(const AmrLaunch& L, const int* list, int n, float* flags, cudaStream_t s);
 cudaError_t amr_launch_regrid(const AmrLaunch& L, const int* rg, const int* list, int n, const float4* u1,
                               const float4* u2, float4* o1, float4* o2, cudaStream_t s);

@@ -115,6 +115,33 @@ void drop_graphs(shz_amr* a) {
     }
 }
 
+// The fine-flux buffer and its face list for at least `faces` matched faces (grown with the mesh).
+int grow_fbuf(shz_amr* a, int faces) {
+  if (faces <= a->fine_cap) return 0;
+  AMR_CUDA(a, cudaStreamSynchronize(a->stream));
+  cudaFree(a->d_flist);
+  cudaFree(a->fbuf);
+  a->d_flist = nullptr;
+  a->fbuf = nullptr;
+  a->fine_cap = 0;
+  const int want = faces + faces / 2 + 64;
+  const size_t fc = a->cfg.ndim == 3 ? 256 : 16;
+  if (cudaMalloc(&a->d_flist, (size_t)want * 3 * sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&a->fbuf, (size_t)want * fc * 2 * sizeof(float4)) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(a, SHZ_E_OOM, "the fine-flux buffer of %d matched faces does not fit", want);
+  }
+  a->fine_cap = want;
+  a->L.fbuf = a->fbuf;
+  // (the single steps' list of faces matched to refined neighbours moves with the buffer, and the
+  // steps' graphs captured the old addresses)
+  if (!a->h_flist.empty())
+    AMR_CUDA(a, cudaMemcpyAsync(a->d_flist, a->h_flist.data(), a->h_flist.size() * sizeof(int32_t),
+                                cudaMemcpyHostToDevice, a->stream));
+  drop_graphs(a);
+  return 0;
+}
+
 // The block table and the slot lists of the current tree, to the device.
 int upload_tables(shz_amr* a) {
   const int cap = a->cfg.cap;
@@ -140,23 +167,8 @@ int upload_tables(shz_amr* a) {
     }
   }
   a->nfine = (int)(a->h_flist.size() / 3);
-  if (a->nfine > a->fine_cap) {
-    AMR_CUDA(a, cudaStreamSynchronize(a->stream));
-    cudaFree(a->d_flist);
-    cudaFree(a->fbuf);
-    a->d_flist = nullptr;
-    a->fbuf = nullptr;
-    a->fine_cap = 0;
-    const int want = a->nfine + a->nfine / 2 + 64;
-    const size_t fc = a->cfg.ndim == 3 ? 256 : 16;
-    if (cudaMalloc(&a->d_flist, (size_t)want * 3 * sizeof(int)) != cudaSuccess ||
-        cudaMalloc(&a->fbuf, (size_t)want * fc * 2 * sizeof(float4)) != cudaSuccess) {
-      cudaGetLastError();
-      return fail(a, SHZ_E_OOM, "the fine-flux buffer of %d matched faces does not fit", want);
-    }
-    a->fine_cap = want;
-  }
-  a->L.fbuf = a->fbuf;
+  int rc = grow_fbuf(a, a->nfine);
+  if (rc) return rc;
   a->L.err = a->d_err;
   if (a->nfine > 0)
     AMR_CUDA(a, cudaMemcpyAsync(a->d_flist, a->h_flist.data(), a->h_flist.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
@@ -327,7 +339,9 @@ bool faster_neighbor(const shz_amr* a, const int32_t* kb, int slot) {
 // lists are built here, in the order of the block list (amr/bins_lists.wgsl gathers them with
 // atomics in no fixed order; no result depends on it). The state stays in one parity: the update
 // writes in place.
-int cycle_once(shz_amr* a) {
+void after_cycle(shz_amr* a, long long updates, int nl);
+
+int cycle_two(shz_amr* a) {
   const int K = a->cfg.time_bins, n = 1 << K;
   float4* u1 = a->u1[a->cur];
   float4* u2 = a->u2[a->cur];
@@ -404,10 +418,16 @@ int cycle_once(shz_amr* a) {
     AMR_CUDA(a, shz::amr_launch_update(a->L, lu, rec[2], u1, u2, u1, u2, a->clk, a->stream, A));
     a->launches += 1 + (rec[0] > 0) + (rec[1] > 0) + (rec[2] > 0);
   }
+  after_cycle(a, updates, nl);
+  return 0;
+}
+
+// The work of a cycle, and a poll every few cycles: above the share, single steps for a while,
+// longer each time (amr_sim.ts:2992-3020 pollBins).
+void after_cycle(shz_amr* a, long long updates, int nl) {
   a->bin_cycles++;
   a->bin_updates += updates;
-  a->bin_single += (long long)nl << K;
-  // a poll every few cycles: above the share, single steps for a while, longer each time
+  a->bin_single += (long long)nl << a->cfg.time_bins;
   if (++a->cycles_since_poll >= BIN_POLL_CYCLES) {
     a->cycles_since_poll = 0;
     const long long du = a->bin_updates - a->seen_updates, ds = a->bin_single - a->seen_single;
@@ -422,8 +442,127 @@ int cycle_once(shz_amr* a) {
       }
     }
   }
+}
+
+// The fused form of a cycle: as cycle_two, with the fused sweep over the leaves that start a step,
+// and ahead of it, per substep, the neighbour-flux pass over the faces of the leaves that update
+// whose neighbour is refined or a faster leaf; then the deposits of the leaves half way through
+// their step beside a faster neighbour. Only leaves are assembled (the sweep and the flux pass
+// read leaves' atlases alone). The bin table is read back before substep 0's sweep, whose faces
+// already depend on the bins.
+int cycle_fused(shz_amr* a) {
+  const int K = a->cfg.time_bins, n = 1 << K;
+  float4* u1 = a->u1[a->cur];
+  float4* u2 = a->u2[a->cur];
+  int* A = a->d_bins[0];
+  int* B = a->d_bins[1];
+  const int na = n_all(a), nl = n_leaves(a), cap = a->cfg.cap;
+  unsigned* scratch = a->rates + 4;
+  AMR_CUDA(a, shz::amr_launch_bins_tick(a->clk, A, 0, a->stream));
+  AMR_CUDA(a, shz::amr_launch_assemble_bins(a->L, a->d_leaves, nl, u1, u2, A, a->rates, a->slot, a->d_brate, a->stream));
+  AMR_CUDA(a, shz::launch_clock_multi(a->clk, a->rates, a->slot, 1, a->stream, n));
+  const int sweeps = (K + a->cfg.max_level + 2) | 1;
+  AMR_CUDA(a, shz::amr_launch_bins(a->L, a->d_all, na, a->d_brate, a->clk, (float)a->cfg.hydro.cfl, K, sweeps, A, B,
+                                   a->stream));
+  AMR_CUDA(a, cudaMemcpyAsync(a->h_bins, A, (size_t)(cap + 1) * sizeof(int32_t), cudaMemcpyDeviceToHost, a->stream));
+  AMR_CUDA(a, cudaMemcpyAsync(a->h_bins + cap + 1, &a->clk->held, sizeof(int), cudaMemcpyDeviceToHost, a->stream));
+  AMR_CUDA(a, cudaEventRecord(a->bins_ready, a->stream));
+  a->launches += 5 + sweeps;
+  a->slot ^= 1;
+  AMR_CUDA(a, cudaEventSynchronize(a->bins_ready));
+  if (a->h_bins[cap + 1]) return 0;  // a held cycle: nothing to step
+  // per substep: the leaves that start a step (swept), those that take a deposit, the faces whose
+  // fluxes come from the neighbour-flux pass (slot, face, entry), and each slot's first entry
+  const int32_t* kb = a->h_bins;
+  const int32_t* bt = a->h_bt.data();
+  const int S = shz::amr::BT_STRIDE;
+  const int nf = 2 * a->cfg.ndim;
+  struct Sub {
+    size_t ll, ld, e, fb;
+    int nll, nld, ne;
+  };
+  std::vector<Sub> subs(n);
+  std::vector<int32_t> buf;
+  buf.reserve((size_t)n * (2 * (size_t)nl + cap));
+  long long updates = 0;
+  int most = 0;
+  for (int sub = 0; sub < n; sub++) {
+    Sub& q = subs[sub];
+    std::vector<int32_t> ld, ents;
+    q.ll = buf.size();
+    for (int slot : a->h_leaves) {
+      const int k = kb[1 + slot];
+      const int phase = sub & ((1 << k) - 1);
+      if (phase == 0) buf.push_back(slot);
+      else if (k > 0 && phase == (1 << (k - 1)) && faster_neighbor(a, kb, slot)) ld.push_back(slot);
+    }
+    q.nll = (int)(buf.size() - q.ll);
+    q.ld = buf.size();
+    buf.insert(buf.end(), ld.begin(), ld.end());
+    q.nld = (int)ld.size();
+    q.fb = buf.size();
+    buf.resize(buf.size() + cap, -1);
+    int ne = 0;
+    auto faces_of = [&](int slot) {
+      const int k = kb[1 + slot];
+      for (int f = 0; f < nf; f++) {
+        const int nb = bt[(size_t)slot * S + 6 + f];
+        if (nb < 0) continue;
+        const bool leaf = (bt[(size_t)nb * S + 4] & 2) != 0;
+        if (leaf && (nb == slot || kb[1 + nb] >= k)) continue;
+        if (buf[q.fb + slot] < 0) buf[q.fb + slot] = ne;
+        ents.insert(ents.end(), {slot, f, ne});
+        ne++;
+      }
+    };
+    for (size_t i = q.ll; i < q.ll + q.nll; i++) faces_of(buf[i]);
+    for (int slot : ld) faces_of(slot);
+    q.e = buf.size();
+    buf.insert(buf.end(), ents.begin(), ents.end());
+    q.ne = ne;
+    most = std::max(most, ne);
+    updates += q.nll + q.nld;
+  }
+  int rc = grow_fbuf(a, most);
+  if (rc) return rc;
+  if (buf.size() > a->cyc_cap) {
+    AMR_CUDA(a, cudaStreamSynchronize(a->stream));
+    cudaFree(a->d_cyc);
+    cudaFreeHost(a->h_cyc);
+    a->d_cyc = nullptr;
+    a->h_cyc = nullptr;
+    a->cyc_cap = 0;
+    const size_t want = buf.size() + buf.size() / 4;
+    if (cudaMalloc(&a->d_cyc, want * sizeof(int32_t)) != cudaSuccess ||
+        cudaMallocHost(&a->h_cyc, want * sizeof(int32_t)) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(a, SHZ_E_OOM, "the block lists of a cycle (%zu ints) do not fit", want);
+    }
+    a->cyc_cap = want;
+  }
+  std::memcpy(a->h_cyc, buf.data(), buf.size() * sizeof(int32_t));
+  AMR_CUDA(a, cudaMemcpyAsync(a->d_cyc, a->h_cyc, buf.size() * sizeof(int32_t), cudaMemcpyHostToDevice, a->stream));
+  shz::AmrLaunch L = a->L;
+  L.bins = A;
+  for (int sub = 0; sub < n; sub++) {
+    const Sub& q = subs[sub];
+    const int* ll = a->d_cyc + q.ll;
+    L.fbase = a->d_cyc + q.fb;
+    if (sub > 0) {
+      AMR_CUDA(a, shz::amr_launch_bins_tick(a->clk, A, sub, a->stream));
+      AMR_CUDA(a, shz::amr_launch_assemble_bins(L, ll, q.nll, u1, u2, A, scratch, 0, nullptr, a->stream));
+      a->launches += 1 + (q.nll > 0);
+    }
+    AMR_CUDA(a, shz::amr_launch_fine_flux(L, a->d_cyc + q.e, q.ne, a->clk, a->stream));
+    AMR_CUDA(a, shz::amr_launch_sweep(L, ll, q.nll, u1, u2, u1, u2, a->clk, a->stream));
+    AMR_CUDA(a, shz::amr_launch_deposit(L, a->d_cyc + q.ld, q.nld, u1, u2, a->clk, a->stream));
+    a->launches += (q.ne > 0) + (q.nll > 0) + (q.nld > 0);
+  }
+  after_cycle(a, updates, nl);
   return 0;
 }
+
+int cycle_once(shz_amr* a) { return a->cfg.two_pass ? cycle_two(a) : cycle_fused(a); }
 
 // The refinement indicators of the current state: a fresh assemble, then the Löhner pass.
 int compute_flags(shz_amr* a) {
@@ -617,8 +756,6 @@ int shz_amr_create(const shz_amr_config* cfg, shz_amr** out) {
   Dev dv(c.hydro.device);
   shz_amr* a = new shz_amr();
   a->cfg = c;
-  // per-block timesteps run on the two passes, whose half-step atlas they keep
-  if (c.time_bins > 0) a->cfg.two_pass = 1;
   a->device = c.hydro.device;
   a->CB = c.ndim == 3 ? 4096 : 256;
   a->WN = c.ndim == 3 ? 8000 : 400;
@@ -656,7 +793,7 @@ int shz_amr_create(const shz_amr_config* cfg, shz_amr** out) {
   }
   ok = ok && cudaMalloc(&a->w1, cap * a->WN * sizeof(float4)) == cudaSuccess;
   ok = ok && cudaMalloc(&a->w2, cap * a->WN * sizeof(float4)) == cudaSuccess;
-  if (a->cfg.two_pass) {
+  if (a->cfg.two_pass || c.time_bins > 0) {
     ok = ok && cudaMalloc(&a->p1, cap * a->PN * sizeof(float4)) == cudaSuccess;
     ok = ok && cudaMalloc(&a->p2, cap * a->PN * sizeof(float4)) == cudaSuccess;
   }
@@ -689,7 +826,7 @@ int shz_amr_create(const shz_amr_config* cfg, shz_amr** out) {
     cudaGetLastError();
     char buf[160];
     snprintf(buf, sizeof buf, "the atlases of %d block slots (%.2f GB) do not fit", c.cap,
-             cap * (4.0 * a->CB + 2.0 * a->WN + (a->cfg.two_pass ? 2.0 * a->PN : 0.0)) * 16 / 1e9);
+             cap * (4.0 * a->CB + 2.0 * a->WN + (a->L.p1 || a->cfg.two_pass || c.time_bins > 0 ? 2.0 * a->PN : 0.0)) * 16 / 1e9);
     return bail(SHZ_E_OOM, buf);
   }
   a->L.bt = a->d_bt;

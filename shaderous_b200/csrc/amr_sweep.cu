@@ -55,10 +55,12 @@ __device__ __forceinline__ void load_w6(const float4* __restrict__ w1, const flo
 
 // The predictor of texel l0 of block `slot`, read from its primitive atlas, under the ghost rules
 // above; with the edge increments along `axis` at l0 itself (for its face states on that axis).
+// (bins: the per-block timesteps' bin table, or null; a ghost beside a neighbour part way through
+// its step is predicted in place, as beside a coarser block.)
 template <int DIM, int R, bool ISEN>
 __device__ __forceinline__ void predict_texel(const KParams& P, const int* __restrict__ bt, const float4* __restrict__ w1,
                                               const float4* __restrict__ w2, int slot, const int* l0, float h, int axis,
-                                              Pred& pr, float* su, float* sd) {
+                                              Pred& pr, float* su, float* sd, const int* __restrict__ bins = nullptr) {
   int l[3] = {l0[0], l0[1], l0[2]};
   float flip[3] = {1.f, 1.f, 1.f}, mask[3] = {1.f, 1.f, 1.f};
   int out = 0, oa = 0;
@@ -69,7 +71,7 @@ __device__ __forceinline__ void predict_texel(const KParams& P, const int* __res
   if (out == 1) {
     const int upper = l[oa] >= BS ? 1 : 0;
     const int nb = bt_at(bt, slot, 6 + 2 * oa + upper);
-    if (nb == -1) {
+    if (nb == -1 || (nb >= 0 && nb != slot && mid_block(bt, bins, nb))) {
 #pragma unroll
       for (int a = 0; a < DIM; a++)
         if (a != oa) mask[a] = (l[a] == 0 || l[a] == BS - 1) ? 0.f : 1.f;
@@ -126,10 +128,14 @@ __device__ __forceinline__ void predict_texel(const KParams& P, const int* __res
 struct Flux8 {
   float v[8];
 };
+// With per-block timesteps (bins) the fine leaf predicts with its own step (hf is the fine level's
+// h for the clock's dt) and its fluxes count for their share of this block's step (kb, deposit:
+// half for a faster child, none in a deposit for one in step; amr/update.wgsl:182-186).
 template <int DIM, int R, bool ISEN, int AXIS>
 __device__ __forceinline__ Flux8 fine_mean_flux(const KParams* __restrict__ Pp, const int* __restrict__ bt,
                                              const float4* __restrict__ w1, const float4* __restrict__ w2, int np, int l0,
-                                             int l1, int l2, bool hi, float hf) {
+                                             int l1, int l2, bool hi, float hf, const int* __restrict__ bins = nullptr,
+                                             int kb = 0, bool deposit = false) {
   const KParams& P = *Pp;
   Flux8 out;
 #pragma unroll
@@ -142,6 +148,13 @@ __device__ __forceinline__ Flux8 fine_mean_flux(const KParams* __restrict__ Pp, 
   if (DIM == 2) bits[2] = 0;
   const int ch = bt_at(bt, np, 12 + (bits[0] | (bits[1] << 1) | (bits[2] << 2)));
   if (ch < 0) return out;
+  float part = 1.f;
+  if (bins) {
+    const int kc = blk_bin(bins, ch);
+    part = kc < kb ? 0.5f : (deposit ? 0.f : 1.f);
+    if (part == 0.f) return out;
+    hf *= (float)(1 << kc);
+  }
   int a0[3] = {2 * (l[0] - (BS / 2) * hb[0]), 2 * (l[1] - (BS / 2) * hb[1]), DIM == 3 ? 2 * (l[2] - (BS / 2) * hb[2]) : 0};
   a0[AXIS] = upper ? BS - 1 : -1;
   constexpr int T1 = (AXIS + 1) % 3, T2 = (AXIS + 2) % 3;
@@ -156,8 +169,8 @@ __device__ __forceinline__ Flux8 fine_mean_flux(const KParams* __restrict__ Pp, 
       b[AXIS] += 1;
       Pred pa, pb;
       float sua[6], sda[6], sub[6], sdb[6];
-      predict_texel<DIM, R, ISEN>(P, bt, w1, w2, ch, a, hf, AXIS, pa, sua, sda);
-      predict_texel<DIM, R, ISEN>(P, bt, w1, w2, ch, b, hf, AXIS, pb, sub, sdb);
+      predict_texel<DIM, R, ISEN>(P, bt, w1, w2, ch, a, hf, AXIS, pa, sua, sda, bins);
+      predict_texel<DIM, R, ISEN>(P, bt, w1, w2, ch, b, hf, AXIS, pb, sub, sdb, bins);
       float L[7], Rr[7], f[8];
       face_state(pa, sua, 1.f, L);
       face_state(pb, sdb, -1.f, Rr);
@@ -165,9 +178,37 @@ __device__ __forceinline__ Flux8 fine_mean_flux(const KParams* __restrict__ Pp, 
 #pragma unroll
       for (int v = 0; v < 8; v++) out.v[v] += f[v];
     }
-  const float w = 1.f / (float)(n1 * n2);
+  float w = 1.f / (float)(n1 * n2);
+  if (bins) w *= part;
 #pragma unroll
   for (int v = 0; v < 8; v++) out.v[v] *= w;
+  return out;
+}
+
+// Per-block timesteps: the flux through the face of cell (l0, l1, l2) on side `hi` of axis AXIS
+// whose same-level neighbour np is a leaf in a faster bin, as np computes it with its own step
+// (hn: np's h), for half of this block's step (amr/update.wgsl:253-256).
+template <int DIM, int R, bool ISEN, int AXIS>
+__device__ __forceinline__ Flux8 fast_face_flux(const KParams* __restrict__ Pp, const int* __restrict__ bt,
+                                                const float4* __restrict__ w1, const float4* __restrict__ w2,
+                                                const int* __restrict__ bins, int np, int l0, int l1, int l2, bool hi,
+                                                float hn) {
+  const KParams& P = *Pp;
+  int a[3] = {l0, l1, l2};
+  a[AXIS] = hi ? -1 : BS - 1;  // np lies above: its ghost below its first cell; below: its last cell
+  int b[3] = {a[0], a[1], a[2]};
+  b[AXIS] += 1;
+  Pred pa, pb;
+  float sua[6], sda[6], sub[6], sdb[6];
+  predict_texel<DIM, R, ISEN>(P, bt, w1, w2, np, a, hn, AXIS, pa, sua, sda, bins);
+  predict_texel<DIM, R, ISEN>(P, bt, w1, w2, np, b, hn, AXIS, pb, sub, sdb, bins);
+  float L[7], Rr[7];
+  Flux8 out;
+  face_state(pa, sua, 1.f, L);
+  face_state(pb, sdb, -1.f, Rr);
+  riemann<AXIS>(L, Rr, P, out.v);
+#pragma unroll
+  for (int v = 0; v < 8; v++) out.v[v] *= 0.5f;
   return out;
 }
 
@@ -175,11 +216,14 @@ __device__ __forceinline__ Flux8 fine_mean_flux(const KParams* __restrict__ Pp, 
 // whose same-level neighbour is refined, the mean of the fine fluxes through each of its cells,
 // into the buffer entry the host assigned (entries: leaf slot, face, index). One thread per face
 // cell, so that the few blocks with such faces do not hold up a sweep's CTA.
+// With per-block timesteps (bins) the list also holds, per substep, the faces of the leaves that
+// update whose same-level neighbour is a leaf in a faster bin: that neighbour's own flux, half of
+// it; and the refined neighbours' fluxes carry their children's shares.
 template <int DIM, int R, bool ISEN>
 __global__ void __launch_bounds__(NT) amr_fine_flux(const KParams* __restrict__ gp, const int* __restrict__ bt,
                                                     const int* __restrict__ flist, int nf, const float4* __restrict__ w1,
                                                     const float4* __restrict__ w2, const DevClock* __restrict__ clks,
-                                                    float4* __restrict__ fbuf) {
+                                                    float4* __restrict__ fbuf, const int* __restrict__ bins) {
   constexpr int FC = DIM == 3 ? BS * BS : BS;  // cells of a face
   const long long total = (long long)nf * FC;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
@@ -196,9 +240,18 @@ __global__ void __launch_bounds__(NT) amr_fine_flux(const KParams* __restrict__ 
     const int t1 = c % BS, t2 = c / BS;
     const int edge = hi ? BS - 1 : 0;
     Flux8 F;
-    if (axis == 0) F = fine_mean_flux<DIM, R, ISEN, 0>(Pp, bt, w1, w2, np, edge, t1, t2, hi, hf);
-    else if (axis == 1) F = fine_mean_flux<DIM, R, ISEN, 1>(Pp, bt, w1, w2, np, t1, edge, t2, hi, hf);
-    else F = fine_mean_flux<DIM, R, ISEN, 2>(Pp, bt, w1, w2, np, t1, t2, edge, hi, hf);
+    if (bins && leaf_of(bt, np)) {
+      const float hn = (float)((0.5 * (dt * ldexp(1.0, blk_bin(bins, np)))) / (Pp->dx / ldexp(1.0, bt_at(bt, slot, 0))));
+      if (axis == 0) F = fast_face_flux<DIM, R, ISEN, 0>(Pp, bt, w1, w2, bins, np, edge, t1, t2, hi, hn);
+      else if (axis == 1) F = fast_face_flux<DIM, R, ISEN, 1>(Pp, bt, w1, w2, bins, np, t1, edge, t2, hi, hn);
+      else F = fast_face_flux<DIM, R, ISEN, 2>(Pp, bt, w1, w2, bins, np, t1, t2, edge, hi, hn);
+    } else {
+      const int kb = blk_bin(bins, slot);
+      const bool dep = !blk_active(bins, slot);
+      if (axis == 0) F = fine_mean_flux<DIM, R, ISEN, 0>(Pp, bt, w1, w2, np, edge, t1, t2, hi, hf, bins, kb, dep);
+      else if (axis == 1) F = fine_mean_flux<DIM, R, ISEN, 1>(Pp, bt, w1, w2, np, t1, edge, t2, hi, hf, bins, kb, dep);
+      else F = fine_mean_flux<DIM, R, ISEN, 2>(Pp, bt, w1, w2, np, t1, t2, edge, hi, hf, bins, kb, dep);
+    }
     float4* o = fbuf + ((size_t)k * FC + c) * 2;
     o[0] = make_float4(F.v[0], F.v[1], F.v[2], F.v[3]);
     o[1] = make_float4(F.v[4], F.v[5], F.v[6], F.v[7]);
@@ -225,12 +278,22 @@ __device__ __forceinline__ void read_w7(const float4* __restrict__ plane, int x,
   w[4] = b.x; w[5] = b.y; w[6] = b.z;
 }
 
+// Per-block timesteps (bins, the bin table; null: one timestep): each block steps with its own
+// 2^k dt; a ghost beside a neighbour part way through its step (whose ghosts the assemble filled
+// from its half step) is predicted in place, as beside a coarser block; faces whose same-level
+// neighbour is a faster leaf also take their flux from the buffer (entries from fbase[slot], per
+// substep); a block in a bin above 0 keeps its half steps (block and first ghost layer) in p1, p2
+// for its neighbours' ghosts and its own deposits while it is part way through its step. The
+// state is then updated in place (o1, o2 the arrays u1, u2): each cell is read once, by the
+// thread that writes it, and no other pass of the launch reads the state.
 template <int DIM, int R, bool ISEN>
 __global__ void __maxnreg__(80)
     amr_sweep(const KParams* __restrict__ gp, const int* __restrict__ bt, const int* __restrict__ list, int n,
               const float4* __restrict__ u1, const float4* __restrict__ u2, const float4* __restrict__ w1,
               const float4* __restrict__ w2, float4* __restrict__ o1, float4* __restrict__ o2,
-              const DevClock* __restrict__ clks, const float4* __restrict__ fbuf, int* __restrict__ err) {
+              const DevClock* __restrict__ clks, const float4* __restrict__ fbuf, int* __restrict__ err,
+              const int* __restrict__ bins, const int* __restrict__ fbase, float4* __restrict__ p1,
+              float4* __restrict__ p2) {
   constexpr int FC = DIM == 3 ? BS * BS : BS;  // cells of a face
   extern __shared__ __align__(128) float smem[];
   float* sW = smem;
@@ -261,7 +324,8 @@ __global__ void __maxnreg__(80)
   for (int i = blockIdx.x; i < n; i += gridDim.x) {
     const int slot = __ldg(list + i);
     const int g = bt_at(bt, slot, GRID_WORD);
-    const double dt = clks[g].dt;
+    const int kb = blk_bin(bins, slot);
+    const double dt = clks[g].dt * ldexp(1.0, kb);
     const double dxl = gp[g].dx / ldexp(1.0, bt_at(bt, slot, 0));
     const float dtdx = (float)(dt / dxl);
     const float h = (float)((0.5 * dt) / dxl);
@@ -286,7 +350,7 @@ __global__ void __maxnreg__(80)
     if (DIM >= 2 && ty == 0 && col_t) gface = 2;
     if (DIM >= 2 && ty == SX - 1 && col_t) gface = 3;
     const int gnb = gface >= 0 ? bt_at(bt, slot, 6 + gface) : 0;
-    const bool g_coarse = gface >= 0 && gnb == -1;
+    const bool g_coarse = gface >= 0 && (gnb == -1 || (gnb >= 0 && gnb != slot && mid_block(bt, bins, gnb)));
     const bool g_bc = gface >= 0 && gnb <= -2;
     const int g_src = !g_bc ? -1 : (gface == 0 ? tid + 1 : gface == 1 ? tid - 1 : gface == 2 ? tid + SX : tid - SX);
     const bool g_flip = g_bc && (-1 - gnb) == 2;
@@ -301,8 +365,9 @@ __global__ void __maxnreg__(80)
     for (int f = 0; f < 2 * DIM; f++) {
       const int nb = bt_at(bt, slot, 6 + f);
       if (nb >= 0 && !leaf_of(bt, nb)) fine |= 1u << f;
+      else if (bins && nb >= 0 && nb != slot && blk_bin(bins, nb) < kb) fine |= 1u << f;
     }
-    const int fine0 = bt_at(bt, slot, FINE_WORD);
+    const int fine0 = bins ? __ldg(fbase + slot) : bt_at(bt, slot, FINE_WORD);
     if (fine0 < 0 || fbuf == nullptr) fine = 0;
     auto matched = [&](int f, int cidx, float* F) {
       const float4* q = fbuf + ((size_t)(fine0 + __popc(fine & ((1u << f) - 1u))) * FC + cidx) * 2;
@@ -311,6 +376,16 @@ __global__ void __maxnreg__(80)
       F[4] = b.x; F[5] = b.y; F[6] = b.z; F[7] = b.w;
     };
     const int zlo_nb = DIM == 3 ? bt_at(bt, slot, 10) : 0, zhi_nb = DIM == 3 ? bt_at(bt, slot, 11) : 0;
+    // z ghosts predicted in place: beside a coarser block or one part way through its step
+    const bool zlo_in = DIM == 3 && (zlo_nb == -1 || (zlo_nb >= 0 && zlo_nb != slot && mid_block(bt, bins, zlo_nb)));
+    const bool zhi_in = DIM == 3 && (zhi_nb == -1 || (zhi_nb >= 0 && zhi_nb != slot && mid_block(bt, bins, zhi_nb)));
+    const bool keep = bins != nullptr && kb > 0;  // this block's half steps are kept
+    auto keep_pred = [&](int lz, const Pred& q) {
+      const int l[3] = {lx, ly, lz};
+      const size_t o = (size_t)slot * BG<DIM>::PN + ptex<DIM>(l);
+      p1[o] = make_float4(q.q[0], q.q[1], q.q[2], q.q[3]);
+      p2[o] = make_float4(q.q[4], q.q[5], q.flag, q.fo ? 1.f : 0.f);
+    };
 
     float zhi_prev[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
@@ -402,7 +477,7 @@ __global__ void __maxnreg__(80)
         const float rx = (lx == 0 || lx == BS - 1) ? 0.f : 1.f;
         const float ry = (ly == 0 || ly == BS - 1) ? 0.f : 1.f;
         const float rz = (lz == 0 || lz == BS - 1) ? 0.f : 1.f;
-        if (zghost && znb == -1) {
+        if (zghost && (j == -1 ? zlo_in : zhi_in)) {
           mask[0] = rx;
           mask[1] = ry;
         } else if (g_coarse) {
@@ -445,6 +520,7 @@ __global__ void __maxnreg__(80)
 #pragma unroll
           for (int v = 0; v < 6; v++) inc[v] = sKeep[v * SPN + tid];
           face_state(gq, inc, 1.f, zhi_prev);
+          if (keep) keep_pred(-1, gq);  // the lower boundary ghost: plane 0's half step, mirrored
         }
         if (j == BS - 1 && zhi_nb <= -2) {
 #pragma unroll
@@ -460,6 +536,7 @@ __global__ void __maxnreg__(80)
           pr.fo = sKeep[7 * SPN + tid] != 0.f;
         }
       }
+      if (keep && !(DIM == 3 && j == -1 && zlo_nb <= -2)) keep_pred(DIM == 3 ? j : 0, pr);
       if (tile_plane) {
         float f[7];
         face_state(pr, su[0], 1.f, f);
@@ -554,6 +631,70 @@ __global__ void __maxnreg__(80)
   }
 }
 
+// Per-block timesteps, the deposit (amr/update.wgsl:339-445 with g_deposit): a leaf half way
+// through its step beside a faster neighbour takes, on the cells of the shared faces, that
+// neighbour's fluxes of its second step for half of this block's step (from the buffer the
+// neighbour-flux pass filled), with the half-step pressure its own prediction kept from the start
+// of its step; no fluxes of its own. Cells on no such face keep their state. In place.
+template <int DIM>
+__global__ void __launch_bounds__(NT) amr_deposit(const KParams* __restrict__ gp, const int* __restrict__ bt,
+                                                  const int* __restrict__ list, int n, float4* __restrict__ u1,
+                                                  float4* __restrict__ u2, const float4* __restrict__ p2,
+                                                  const DevClock* __restrict__ clks, const int* __restrict__ bins,
+                                                  const int* __restrict__ fbase, const float4* __restrict__ fbuf) {
+  constexpr int FC = DIM == 3 ? BS * BS : BS;
+  for (int i = blockIdx.x; i < n; i += gridDim.x) {
+    const int slot = __ldg(list + i);
+    const int g = bt_at(bt, slot, GRID_WORD);
+    if (clks[g].held) continue;
+    const KParams& P = gp[g];
+    const int kb = blk_bin(bins, slot);
+    const double dt = clks[g].dt * ldexp(1.0, kb);
+    const float dtdx = (float)(dt / (P.dx / ldexp(1.0, bt_at(bt, slot, 0))));
+    unsigned fine = 0;
+    for (int f = 0; f < 2 * DIM; f++) {
+      const int nb = bt_at(bt, slot, 6 + f);
+      if (nb >= 0 && !leaf_of(bt, nb)) fine |= 1u << f;
+      else if (nb >= 0 && nb != slot && blk_bin(bins, nb) < kb) fine |= 1u << f;
+    }
+    const int fine0 = __ldg(fbase + slot);
+    if (!fine || fine0 < 0) continue;
+    for (int t = threadIdx.x; t < BG<DIM>::CB; t += NT) {
+      const int l[3] = {t % BS, (t / BS) % BS, DIM == 3 ? t / (BS * BS) : 0};
+      float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      bool touched = false;
+      for (int f = 0; f < 2 * DIM; f++) {
+        if (!(fine & (1u << f))) continue;
+        const int axis = f >> 1;
+        const bool hi = (f & 1) != 0;
+        if (l[axis] != (hi ? BS - 1 : 0)) continue;
+        const int nb = bt_at(bt, slot, 6 + f);
+        if (!leaf_of(bt, nb)) {
+          // the refined neighbour's child on this cell's face: only a faster one gives a deposit
+          int bits[3] = {l[0] >= BS / 2, l[1] >= BS / 2, DIM == 3 ? (l[2] >= BS / 2) : 0};
+          bits[axis] = hi ? 0 : 1;
+          const int ch = bt_at(bt, nb, 12 + (bits[0] | (bits[1] << 1) | (bits[2] << 2)));
+          if (ch < 0 || blk_bin(bins, ch) >= kb) continue;
+        }
+        touched = true;
+        const int cidx = axis == 0 ? l[1] + BS * l[2] : axis == 1 ? l[0] + BS * l[2] : l[0] + BS * l[1];
+        const float4* q = fbuf + ((size_t)(fine0 + __popc(fine & ((1u << f) - 1u))) * FC + cidx) * 2;
+        const float4 a = __ldg(q), b = __ldg(q + 1);
+        const float F[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+#pragma unroll
+        for (int v = 0; v < 8; v++) acc[v] = hi ? acc[v] - F[v] : acc[v] + F[v];
+      }
+      if (!touched) continue;
+      const size_t o = (size_t)slot * BG<DIM>::CB + t;
+      const float ph = __ldg(p2 + (size_t)slot * BG<DIM>::PN + ptex<DIM>(l)).x;
+      float4 na, nb4;
+      update_cell(u1[o], u2[o], acc, ph, dtdx, P, na, nb4);
+      u1[o] = na;
+      u2[o] = nb4;
+    }
+  }
+}
+
 }  // namespace amrk
 
 // Host launchers.
@@ -573,7 +714,7 @@ cudaError_t sweep_one(const AmrLaunch& L, const int* list, int n, const float4* 
   }();
   if (attr != cudaSuccess) return attr;
   k<<<grid_for(n, per_sm), amrk::SNT, amrk::SWEEP_SMEM, s>>>(L.gp, L.bt, list, n, u1, u2, L.w1, L.w2, o1, o2, clks, L.fbuf,
-                                                             L.err);
+                                                             L.err, L.bins, L.fbase, L.p1, L.p2);
   return cudaGetLastError();
 }
 }  // namespace
@@ -585,12 +726,21 @@ cudaError_t amr_launch_fine_flux(const AmrLaunch& L, const int* flist, int nf, c
   const int per_sm = c && c->per_sm > 0 ? c->per_sm : 8;
   const int g = (int)std::min<long long>((cells + amrk::NT - 1) / amrk::NT, 148LL * per_sm);
   if (L.ndim == 3) {
-    if (L.isen) { SHZ_RECON_SWITCH(L.recon, true, (amrk::amr_fine_flux<3, R, true><<<g, amrk::NT, 0, s>>>(L.gp, L.bt, flist, nf, L.w1, L.w2, clks, L.fbuf))) }
-    else { SHZ_RECON_SWITCH(L.recon, false, (amrk::amr_fine_flux<3, R, false><<<g, amrk::NT, 0, s>>>(L.gp, L.bt, flist, nf, L.w1, L.w2, clks, L.fbuf))) }
+    if (L.isen) { SHZ_RECON_SWITCH(L.recon, true, (amrk::amr_fine_flux<3, R, true><<<g, amrk::NT, 0, s>>>(L.gp, L.bt, flist, nf, L.w1, L.w2, clks, L.fbuf, L.bins))) }
+    else { SHZ_RECON_SWITCH(L.recon, false, (amrk::amr_fine_flux<3, R, false><<<g, amrk::NT, 0, s>>>(L.gp, L.bt, flist, nf, L.w1, L.w2, clks, L.fbuf, L.bins))) }
   } else {
-    if (L.isen) { SHZ_RECON_SWITCH(L.recon, true, (amrk::amr_fine_flux<2, R, true><<<g, amrk::NT, 0, s>>>(L.gp, L.bt, flist, nf, L.w1, L.w2, clks, L.fbuf))) }
-    else { SHZ_RECON_SWITCH(L.recon, false, (amrk::amr_fine_flux<2, R, false><<<g, amrk::NT, 0, s>>>(L.gp, L.bt, flist, nf, L.w1, L.w2, clks, L.fbuf))) }
+    if (L.isen) { SHZ_RECON_SWITCH(L.recon, true, (amrk::amr_fine_flux<2, R, true><<<g, amrk::NT, 0, s>>>(L.gp, L.bt, flist, nf, L.w1, L.w2, clks, L.fbuf, L.bins))) }
+    else { SHZ_RECON_SWITCH(L.recon, false, (amrk::amr_fine_flux<2, R, false><<<g, amrk::NT, 0, s>>>(L.gp, L.bt, flist, nf, L.w1, L.w2, clks, L.fbuf, L.bins))) }
   }
+  return cudaGetLastError();
+}
+
+cudaError_t amr_launch_deposit(const AmrLaunch& L, const int* list, int n, float4* u1, float4* u2, const DevClock* clks,
+                               cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  const int g = grid_for(n, 4);
+  if (L.ndim == 3) amrk::amr_deposit<3><<<g, amrk::NT, 0, s>>>(L.gp, L.bt, list, n, u1, u2, L.p2, clks, L.bins, L.fbase, L.fbuf);
+  else amrk::amr_deposit<2><<<g, amrk::NT, 0, s>>>(L.gp, L.bt, list, n, u1, u2, L.p2, clks, L.bins, L.fbase, L.fbuf);
   return cudaGetLastError();
 }
 

@@ -36,12 +36,12 @@ def top_bin(a):
     return int(max(b[1 + x] for x in s))
 
 
-@pytest.mark.parametrize("ndim", [2, 3])
-def test_bins_and_work_equal_the_oracle(ndim):
+@pytest.mark.parametrize("ndim,two_pass", [(2, False), (3, False), (2, True), (3, True)])
+def test_bins_and_work_equal_the_oracle(ndim, two_pass):
     hyd = Config(gamma=1.4, bc_lo=(1, 1, 1), bc_hi=(1, 1, 1), recon="koren", cfl=0.8, p_floor=1e-12)
     K, lev = 3, 2
     cfg = AmrConfig(hydro=hyd, ndim=ndim, nr=4 if ndim == 2 else 2, max_level=lev, cap=400 if ndim == 2 else 1200,
-                    regrid_every=0, time_bins=K, time_bins_always=True)
+                    regrid_every=0, time_bins=K, time_bins_always=True, two_pass=two_pass)
     with AmrSim(cfg) as a:
         a.reset(Problem("blast", a=(1, 10, 1, 0.1, 0.12)))
         assert a.bin_work()["paused"] == 16
@@ -67,10 +67,11 @@ def test_bins_and_work_equal_the_oracle(ndim):
         assert top_bin(a) >= 1  # the blast's surroundings step less often
 
 
-@pytest.mark.parametrize("K,deeper", [(3, 0), (5, 2)])
-def test_sod_2d_with_bins_against_exact(K, deeper):
+@pytest.mark.parametrize("K,deeper,two_pass", [(3, 0, False), (5, 2, False), (3, 0, True)])
+def test_sod_2d_with_bins_against_exact(K, deeper, two_pass):
     hyd = Config(gamma=1.4, bc_lo=(1, 1, 0), bc_hi=(1, 1, 0), p_floor=1e-12)
-    cfg = AmrConfig(hydro=hyd, ndim=2, nr=4, max_level=2 + deeper, cap=3000, time_bins=K, time_bins_always=True)
+    cfg = AmrConfig(hydro=hyd, ndim=2, nr=4, max_level=2 + deeper, cap=3000, time_bins=K, time_bins_always=True,
+                    two_pass=two_pass)
     with AmrSim(cfg) as a:
         a.reset(Problem("sod", a=(1, 0, 1, 0.125, 0, 0.1)))
         d0 = a.diagnostics()
@@ -120,11 +121,12 @@ def shock_radius(slots, lv, co, u1, nr, nb=128):
     return math.nan
 
 
-@pytest.mark.parametrize("K,levels", [(3, 2), (5, 3)])
-def test_sedov_3d_with_bins(K, levels):
+@pytest.mark.parametrize("K,levels,two_pass", [(3, 2, False), (5, 3, False), (3, 2, True)])
+def test_sedov_3d_with_bins(K, levels, two_pass):
     hyd = Config(gamma=1.4, bc_lo=(1, 1, 1), bc_hi=(1, 1, 1), p_floor=1e-12)
     nr = 128 // (BS << levels)  # 128 cells across at the finest level
-    cfg = AmrConfig(hydro=hyd, ndim=3, nr=nr, max_level=levels, cap=4000, time_bins=K, time_bins_always=True)
+    cfg = AmrConfig(hydro=hyd, ndim=3, nr=nr, max_level=levels, cap=4000, time_bins=K, time_bins_always=True,
+                    two_pass=two_pass)
     with AmrSim(cfg) as a:
         a.reset(Problem("sedov", a=(1.0, 1e-5, 1.0, 3.5)))
         d0 = a.diagnostics()
@@ -158,3 +160,29 @@ def test_cycles_pause_when_they_save_too_little():
         assert w["paused"] == 192
         _, _, steps = a.clock()
         assert steps == 16 + 16
+
+
+@pytest.mark.parametrize("ndim,recon,bcs", [
+    (2, "mc", ((2, 1, 0), (1, 0, 0))),
+    (2, "minmod", ((0, 0, 0), (0, 0, 0))),
+    (3, "minmod", ((2, 0, 1), (1, 2, 0))),
+    (3, "mc", ((1, 1, 1), (2, 2, 2))),
+])
+def test_fused_cycles_equal_two_pass_cycles(ndim, recon, bcs):
+    """The fused form of the cycles (one sweep per leaf, the neighbour-flux pass, the deposits) gives
+    the two passes' state bit for bit, remeshes included."""
+    hyd = Config(gamma=1.4, bc_lo=bcs[0], bc_hi=bcs[1], recon=recon, isentropic=False, cfl=0.6, p_floor=1e-12)
+    out = []
+    for two_pass in (False, True):
+        cfg = AmrConfig(hydro=hyd, ndim=ndim, nr=2, max_level=2, cap=1200 if ndim == 3 else 300, refine_hi=0.1,
+                        refine_lo=0.05, regrid_every=8, time_bins=3, time_bins_always=True, two_pass=two_pass)
+        with AmrSim(cfg) as a:
+            a.reset(Problem("blast", a=(1, 10, 1, 0.1, 0.15)))
+            a.run(steps=16 + 5 * 8)
+            out.append((a.leaves(), a.leaves_state(), a.clock(), a.bin_work(), top_bin(a)))
+    (sa, la, ca), (ua1, ua2), clka, wa, ta = out[0]
+    (sb, lb, cb), (ub1, ub2), clkb, wb, tb = out[1]
+    assert ta >= 1 and wa["cycles"] == 5
+    assert np.array_equal(la, lb) and np.array_equal(ca, cb)
+    assert clka == clkb and wa == wb
+    assert np.array_equal(ua1, ub1) and np.array_equal(ua2, ub2)
