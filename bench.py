@@ -63,7 +63,7 @@ def parse():
     ap.add_argument("--serve-requests", type=int, default=200)
     ap.add_argument("--section", choices=["all", "amr", "serving", "comparable"], default="all",
                     help="amr / serving: only that measurement, printed as its own JSON line")
-    ap.add_argument("--amr-variant", choices=["both", "spec", "developed"], default="both")
+    ap.add_argument("--amr-variant", choices=["both", "spec", "developed", "bins"], default="both")
     ap.add_argument("--amr-cap", type=int, default=26000, help="block slots of the AMR runs")
     ap.add_argument("--profile-window", action="store_true",
                     help="AMR section: bracket one step after the warm-up with cudaProfilerStart/Stop")
@@ -503,6 +503,8 @@ def main():
             if args.amr_variant in ("both", "developed"):
                 out["developed"] = amr_sedov(steps=max(args.steps, 8), grown=True, cap=args.amr_cap,
                                              profile_window=args.profile_window)
+            if args.amr_variant in ("both", "bins"):
+                out["developed_time_bins"] = amr_sedov(steps=64, grown=True, cap=args.amr_cap, time_bins=5)
         elif args.section == "comparable":
             out = comparable()
         else:
@@ -592,6 +594,8 @@ def main():
         amr = {"spec": amr_sedov(), "developed": amr_sedov(steps=16, grown=True)}
         amr["developed"]["note"] += ("; the same blast with the energy spread within 0.2 of the box, the mesh of the "
                                      "grown blast (about 20k blocks) that the spec's run reaches later")
+        # per-block timesteps (cycles of 32 substeps): zone-updates counted as single steps would make them
+        amr["developed_time_bins"] = amr_sedov(steps=64, grown=True, time_bins=5)
     if rank == 0 and not args.no_serving:
         serve = serving(args.serve_requests)
     comp = comparable() if rank == 0 and not args.no_comparable else None
