@@ -55,6 +55,43 @@ __device__ __forceinline__ void tab_load(const float* e, Cons& uc, Slopes& sl) {
   sl.f = e[32];
 }
 
+// The texels of a block's primitive region outside its own cells (the two ghost layers), numbered
+// 0 .. WN - CB - 1: in 3D the four ghost planes z = -2, -1, 16, 17 whole, then the ring of each
+// plane z = 0 .. 15; in 2D the ring of the one plane. A ring (20^2 - 16^2 = 144 texels) is the rows
+// y = -2, -1, then y = 16, 17, then x = -2, -1, 16, 17 of the rows y = 0 .. 15.
+__device__ __forceinline__ void ring_texel(int k, int& x, int& y) {
+  if (k < 2 * PAD) {
+    y = k / PAD - NG;
+    x = k % PAD - NG;
+  } else if (k < 4 * PAD) {
+    k -= 2 * PAD;
+    y = k / PAD + BS;
+    x = k % PAD - NG;
+  } else {
+    k -= 4 * PAD;
+    y = k >> 2;
+    const int c = k & 3;
+    x = c < 2 ? c - NG : c - 2 + BS;
+  }
+}
+template <int DIM>
+__device__ __forceinline__ void shell_texel(int i, int* l) {
+  constexpr int RING = PAD * PAD - BS * BS;
+  if (DIM == 2) {
+    ring_texel(i, l[0], l[1]);
+    l[2] = 0;
+  } else if (i < 2 * NG * PAD * PAD) {
+    const int p = i / (PAD * PAD), r = i % (PAD * PAD);
+    l[2] = p < NG ? p - NG : p - NG + BS;
+    l[0] = r % PAD - NG;
+    l[1] = r / PAD - NG;
+  } else {
+    const int j = i - 2 * NG * PAD * PAD;
+    l[2] = j / RING;
+    ring_texel(j % RING, l[0], l[1]);
+  }
+}
+
 // 1. Primitives of every block in the list with two ghost layers; the rate / dx maximum over the
 // leaves' own cells (assemble.wgsl:78-154; PER_DX in clock.wgsl). MINB: the CTAs per SM the
 // register budget is planned for (the autotuner's variant): more CTAs hide the gather's latency,
@@ -117,8 +154,22 @@ __global__ void __launch_bounds__(NT, MINB) amr_assemble(const KParams* __restri
       }
       __syncthreads();
     }
-    for (int t = threadIdx.x; t < BG<DIM>::WN; t += NT) {
-      int l[3] = {t % PAD - NG, (t / PAD) % PAD - NG, DIM == 3 ? t / (PAD * PAD) - NG : 0};
+    // the block's own cells (a parent's restricted from its children), with the rate maximum
+#pragma unroll 4
+    for (int t = threadIdx.x; t < BG<DIM>::CB; t += NT) {
+      const int l[3] = {t & (BS - 1), (t >> 4) & (BS - 1), DIM == 3 ? t >> 8 : 0};
+      const Cons u = u_at<DIM>(bt, u1, u2, slot, l);
+      float w[7];
+      prim_from_cons(u.a, u.b, P, 1.f, 1.f, 1.f, w);
+      const size_t o = (size_t)slot * BG<DIM>::WN + wtex<DIM>(l);
+      w1[o] = make_float4(w[0], w[1], w[2], w[3]);
+      w2[o] = make_float4(w[4], w[5], w[6], 0.f);
+      if (leaf) rmax = fmaxf(rmax, rate_guard_f(fabsf(w[1]) + fabsf(w[2]) + fabsf(w[3]) + P.signal * w[6]) * inv_dx);
+    }
+    // the ghost layers, each from its source
+    for (int i = threadIdx.x; i < BG<DIM>::WN - BG<DIM>::CB; i += NT) {
+      int l[3];
+      shell_texel<DIM>(i, l);
       const Src s = ghost_src_any<DIM>(bt, slot, l);
       Cons u;
       if (s.kind == 0) {
@@ -147,13 +198,9 @@ __global__ void __launch_bounds__(NT, MINB) amr_assemble(const KParams* __restri
       u.a.w *= s.flip[2];
       float w[7];
       prim_from_cons(u.a, u.b, P, 1.f, 1.f, 1.f, w);
-      const size_t o = (size_t)slot * BG<DIM>::WN + t;
+      const size_t o = (size_t)slot * BG<DIM>::WN + wtex<DIM>(l);
       w1[o] = make_float4(w[0], w[1], w[2], w[3]);
       w2[o] = make_float4(w[4], w[5], w[6], 0.f);
-      bool inside = leaf;
-#pragma unroll
-      for (int q = 0; q < DIM; q++) inside = inside && l[q] >= 0 && l[q] < BS;
-      if (inside) rmax = fmaxf(rmax, rate_guard_f(fabsf(w[1]) + fabsf(w[2]) + fabsf(w[3]) + P.signal * w[6]) * inv_dx);
     }
     const float m = block_max(rmax, sRed);
     if (threadIdx.x == 0 && leaf) {

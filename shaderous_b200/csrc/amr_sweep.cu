@@ -286,7 +286,7 @@ __device__ __forceinline__ void read_w7(const float4* __restrict__ plane, int x,
 // for its neighbours' ghosts and its own deposits while it is part way through its step. The
 // state is then updated in place (o1, o2 the arrays u1, u2): each cell is read once, by the
 // thread that writes it, and no other pass of the launch reads the state.
-template <int DIM, int R, bool ISEN>
+template <int DIM, int R, bool ISEN, bool BINS>
 __global__ void __maxnreg__(80)
     amr_sweep(const KParams* __restrict__ gp, const int* __restrict__ bt, const int* __restrict__ list, int n,
               const float4* __restrict__ u1, const float4* __restrict__ u2, const float4* __restrict__ w1,
@@ -324,8 +324,8 @@ __global__ void __maxnreg__(80)
   for (int i = blockIdx.x; i < n; i += gridDim.x) {
     const int slot = __ldg(list + i);
     const int g = bt_at(bt, slot, GRID_WORD);
-    const int kb = blk_bin(bins, slot);
-    const double dt = clks[g].dt * ldexp(1.0, kb);
+    const int kb = BINS ? blk_bin(bins, slot) : 0;
+    const double dt = BINS ? clks[g].dt * ldexp(1.0, kb) : clks[g].dt;
     const double dxl = gp[g].dx / ldexp(1.0, bt_at(bt, slot, 0));
     const float dtdx = (float)(dt / dxl);
     const float h = (float)((0.5 * dt) / dxl);
@@ -350,7 +350,7 @@ __global__ void __maxnreg__(80)
     if (DIM >= 2 && ty == 0 && col_t) gface = 2;
     if (DIM >= 2 && ty == SX - 1 && col_t) gface = 3;
     const int gnb = gface >= 0 ? bt_at(bt, slot, 6 + gface) : 0;
-    const bool g_coarse = gface >= 0 && (gnb == -1 || (gnb >= 0 && gnb != slot && mid_block(bt, bins, gnb)));
+    const bool g_coarse = gface >= 0 && (gnb == -1 || (BINS && gnb >= 0 && gnb != slot && mid_block(bt, bins, gnb)));
     const bool g_bc = gface >= 0 && gnb <= -2;
     const int g_src = !g_bc ? -1 : (gface == 0 ? tid + 1 : gface == 1 ? tid - 1 : gface == 2 ? tid + SX : tid - SX);
     const bool g_flip = g_bc && (-1 - gnb) == 2;
@@ -365,9 +365,9 @@ __global__ void __maxnreg__(80)
     for (int f = 0; f < 2 * DIM; f++) {
       const int nb = bt_at(bt, slot, 6 + f);
       if (nb >= 0 && !leaf_of(bt, nb)) fine |= 1u << f;
-      else if (bins && nb >= 0 && nb != slot && blk_bin(bins, nb) < kb) fine |= 1u << f;
+      else if (BINS && nb >= 0 && nb != slot && blk_bin(bins, nb) < kb) fine |= 1u << f;
     }
-    const int fine0 = bins ? __ldg(fbase + slot) : bt_at(bt, slot, FINE_WORD);
+    const int fine0 = BINS ? __ldg(fbase + slot) : bt_at(bt, slot, FINE_WORD);
     if (fine0 < 0 || fbuf == nullptr) fine = 0;
     auto matched = [&](int f, int cidx, float* F) {
       const float4* q = fbuf + ((size_t)(fine0 + __popc(fine & ((1u << f) - 1u))) * FC + cidx) * 2;
@@ -377,9 +377,9 @@ __global__ void __maxnreg__(80)
     };
     const int zlo_nb = DIM == 3 ? bt_at(bt, slot, 10) : 0, zhi_nb = DIM == 3 ? bt_at(bt, slot, 11) : 0;
     // z ghosts predicted in place: beside a coarser block or one part way through its step
-    const bool zlo_in = DIM == 3 && (zlo_nb == -1 || (zlo_nb >= 0 && zlo_nb != slot && mid_block(bt, bins, zlo_nb)));
-    const bool zhi_in = DIM == 3 && (zhi_nb == -1 || (zhi_nb >= 0 && zhi_nb != slot && mid_block(bt, bins, zhi_nb)));
-    const bool keep = bins != nullptr && kb > 0;  // this block's half steps are kept
+    const bool zlo_in = DIM == 3 && (zlo_nb == -1 || (BINS && zlo_nb >= 0 && zlo_nb != slot && mid_block(bt, bins, zlo_nb)));
+    const bool zhi_in = DIM == 3 && (zhi_nb == -1 || (BINS && zhi_nb >= 0 && zhi_nb != slot && mid_block(bt, bins, zhi_nb)));
+    const bool keep = BINS && kb > 0;  // this block's half steps are kept
     auto keep_pred = [&](int lz, const Pred& q) {
       const int l[3] = {lx, ly, lz};
       const size_t o = (size_t)slot * BG<DIM>::PN + ptex<DIM>(l);
@@ -700,10 +700,10 @@ __global__ void __launch_bounds__(NT) amr_deposit(const KParams* __restrict__ gp
 // Host launchers.
 
 namespace {
-template <int DIM, int R, bool ISEN>
+template <int DIM, int R, bool ISEN, bool BINS>
 cudaError_t sweep_one(const AmrLaunch& L, const int* list, int n, const float4* u1, const float4* u2, float4* o1,
                       float4* o2, const DevClock* clks, cudaStream_t s, int per_sm) {
-  auto k = amrk::amr_sweep<DIM, R, ISEN>;
+  auto k = amrk::amr_sweep<DIM, R, ISEN, BINS>;
   // (set once per instantiation; an attribute call is not a stream operation, so a first call
   // inside a stream capture is fine)
   static const cudaError_t attr = [&] {
@@ -748,12 +748,23 @@ cudaError_t amr_launch_sweep(const AmrLaunch& L, const int* list, int n, const f
                              float4* o2, const DevClock* clks, cudaStream_t s, const tune::Choice* c) {
   if (n <= 0) return cudaSuccess;
   const int per_sm = c && c->per_sm > 0 ? c->per_sm : 2;
+  // (per-block timesteps in their own instantiation: the plain sweep's registers stay its own)
+  if (L.bins) {
+    if (L.ndim == 3) {
+      if (L.isen) { SHZ_RECON_SWITCH(L.recon, true, return (sweep_one<3, R, true, true>(L, list, n, u1, u2, o1, o2, clks, s, per_sm))) }
+      else { SHZ_RECON_SWITCH(L.recon, false, return (sweep_one<3, R, false, true>(L, list, n, u1, u2, o1, o2, clks, s, per_sm))) }
+    } else {
+      if (L.isen) { SHZ_RECON_SWITCH(L.recon, true, return (sweep_one<2, R, true, true>(L, list, n, u1, u2, o1, o2, clks, s, per_sm))) }
+      else { SHZ_RECON_SWITCH(L.recon, false, return (sweep_one<2, R, false, true>(L, list, n, u1, u2, o1, o2, clks, s, per_sm))) }
+    }
+    return cudaSuccess;
+  }
   if (L.ndim == 3) {
-    if (L.isen) { SHZ_RECON_SWITCH(L.recon, true, return (sweep_one<3, R, true>(L, list, n, u1, u2, o1, o2, clks, s, per_sm))) }
-    else { SHZ_RECON_SWITCH(L.recon, false, return (sweep_one<3, R, false>(L, list, n, u1, u2, o1, o2, clks, s, per_sm))) }
+    if (L.isen) { SHZ_RECON_SWITCH(L.recon, true, return (sweep_one<3, R, true, false>(L, list, n, u1, u2, o1, o2, clks, s, per_sm))) }
+    else { SHZ_RECON_SWITCH(L.recon, false, return (sweep_one<3, R, false, false>(L, list, n, u1, u2, o1, o2, clks, s, per_sm))) }
   } else {
-    if (L.isen) { SHZ_RECON_SWITCH(L.recon, true, return (sweep_one<2, R, true>(L, list, n, u1, u2, o1, o2, clks, s, per_sm))) }
-    else { SHZ_RECON_SWITCH(L.recon, false, return (sweep_one<2, R, false>(L, list, n, u1, u2, o1, o2, clks, s, per_sm))) }
+    if (L.isen) { SHZ_RECON_SWITCH(L.recon, true, return (sweep_one<2, R, true, false>(L, list, n, u1, u2, o1, o2, clks, s, per_sm))) }
+    else { SHZ_RECON_SWITCH(L.recon, false, return (sweep_one<2, R, false, false>(L, list, n, u1, u2, o1, o2, clks, s, per_sm))) }
   }
   return cudaSuccess;
 }
