@@ -484,9 +484,9 @@ cudaError_t amr_launch_assemble_bins(const AmrLaunch& L, const int* list, int n,
   if (n <= 0) return cudaSuccess;
   const int g = grid_for(n, 4);
   if (L.ndim == 3) {
-    SHZ_RECON_SWITCH(L.recon, false, return (assemble_t<3, R, 1, true>(L, g, list, n, u1, u2, rates, rslot, s, bins, brate)))
+    SHZ_RECON_SWITCH(L.recon, false, return (assemble_t<3, R, 2, true>(L, g, list, n, u1, u2, rates, rslot, s, bins, brate)))
   } else {
-    SHZ_RECON_SWITCH(L.recon, false, return (assemble_t<2, R, 1, true>(L, g, list, n, u1, u2, rates, rslot, s, bins, brate)))
+    SHZ_RECON_SWITCH(L.recon, false, return (assemble_t<2, R, 2, true>(L, g, list, n, u1, u2, rates, rslot, s, bins, brate)))
   }
   return cudaSuccess;
 }
