@@ -158,7 +158,8 @@ std::vector<Block*> BlockTree::coarser_around(const Block* b) const {
 }
 
 // tree.ts:346-352 refineCost.
-int BlockTree::refine_cost(const Block* b, std::unordered_set<const Block*>& seen) const {
+template <class Set>
+int BlockTree::refine_cost(const Block* b, Set& seen) const {
   if (seen.count(b) || !b->leaf()) return 0;
   seen.insert(b);
   int cost = nchild;
@@ -174,11 +175,17 @@ int BlockTree::cost_to_refine(const std::vector<Block*>& list) const {
 }
 
 // tree.ts:366-386 refine: split a leaf, first splitting coarser neighbours so balance holds.
-std::vector<Block*> BlockTree::refine(Block* b, const std::unordered_set<Block*>* forbidden) {
+std::vector<Block*> BlockTree::refine(Block* b, const std::unordered_set<Block*>* forbidden,
+                                      BlockSet* need_out, int* cost_out) {
   std::vector<Block*> done;
   if (!b->leaf() || b->level >= level_limit) return done;
-  std::unordered_set<const Block*> need;
-  if (refine_cost(b, need) > (int)free_.size()) return done;
+  BlockSet need;
+  const int cost = refine_cost(b, need);
+  if (cost > (int)free_.size()) {
+    if (need_out) *need_out = std::move(need);
+    if (cost_out) *cost_out = cost;
+    return done;
+  }
   if (forbidden)
     for (const Block* q : need)
       if (forbidden->count(const_cast<Block*>(q))) return done;
@@ -224,8 +231,7 @@ void BlockTree::coarsen(Block* p) {
 
 // tree.ts:420-430 evictable: parents with only leaf children, scored by their most strongly
 // flagged child; the lowest tier first, then the least flagged (a stable sort, as Array.sort).
-std::vector<BlockTree::Evictable> BlockTree::evictable(const std::vector<Block*>& lv,
-                                                       const std::unordered_map<const Block*, double>& ind,
+std::vector<BlockTree::Evictable> BlockTree::evictable(const std::vector<Block*>& lv, const SlotVals& ind,
                                                        const std::function<double(const Block*)>& tier) const {
   std::vector<Block*> parents;
   std::unordered_set<const Block*> seen;
@@ -238,10 +244,7 @@ std::vector<BlockTree::Evictable> BlockTree::evictable(const std::vector<Block*>
     for (Block* ch : p->children) any |= !ch->leaf();
     if (any) continue;
     double score = -std::numeric_limits<double>::infinity();
-    for (Block* ch : p->children) {
-      auto it = ind.find(ch);
-      score = std::max(score, it == ind.end() ? 0.0 : it->second);
-    }
+    for (Block* ch : p->children) score = std::max(score, ind.get(ch, 0.0));
     out.push_back({p, score, tier ? tier(p) : NO_TIER});
   }
   std::stable_sort(out.begin(), out.end(), [](const Evictable& a, const Evictable& b) {
@@ -265,33 +268,47 @@ bool BlockTree::near(const Block* a, const Block* q) const {
 
 // tree.ts:449-467 makeRoom. The candidates' tests are the reference's, in its order; those that
 // do not involve b (touched, live, leaf children, canCoarsen) are pure functions of the tree and
-// the touched set, which change together, so they are evaluated once per version of the tree:
-// adapt calls this for every flagged leaf, and on a full slot budget each call scans thousands
-// of candidates.
+// the touched set, which change together, so they are evaluated once per version of the tree and
+// the candidates that failed them are not visited again: adapt calls this for every flagged leaf,
+// and on a full slot budget each call would scan thousands of candidates. The stopping test (tier
+// and score against b's) holds from some candidate on, in the sorted order, so checking it at the
+// candidates that pass stops where the full scan would (the ones in between add nothing).
 bool BlockTree::make_room(Block* b, double level, const std::vector<Evictable>& ev,
                           const std::unordered_set<const Block*>& touched, double tier, std::vector<Block*>& out,
-                          EvictCache& cache) {
+                          EvictCache& cache, const BlockSet* need_in, int cost_in) {
   out.clear();
   if (!b->leaf() || b->level >= level_limit) return false;
-  std::unordered_set<const Block*> need;
-  int shortage = refine_cost(b, need) - (int)free_.size();
+  BlockSet own;
+  const BlockSet& need = need_in ? *need_in : own;
+  int shortage = (need_in ? cost_in : refine_cost(b, own)) - (int)free_.size();
   if (shortage <= 0) return false;
-  if (cache.version != version_ || cache.ok.size() != ev.size()) {
-    cache.ok.assign(ev.size(), -1);  // -1: not yet evaluated at this version
+  if (cache.version != version_) {
+    cache.ok_idx.clear();
+    cache.evaluated = 0;
     cache.version = version_;
   }
-  for (size_t i = 0; i < ev.size(); i++) {
-    const Evictable& e = ev[i];
-    Block* p = e.p;
-    if (e.tier < tier || (e.tier == tier && e.score >= EVICT_MARGIN * level)) break;
-    if (cache.ok[i] < 0) {
+  auto stop = [&](const Evictable& e) { return e.tier < tier || (e.tier == tier && e.score >= EVICT_MARGIN * level); };
+  size_t k = 0;
+  for (;;) {
+    size_t i;
+    if (k < cache.ok_idx.size()) {
+      i = (size_t)cache.ok_idx[k++];
+      if (stop(ev[i])) break;
+    } else {
+      if (cache.evaluated >= ev.size()) break;
+      i = cache.evaluated;
+      if (stop(ev[i])) break;
+      cache.evaluated++;
+      Block* p = ev[i].p;
       bool ok = !(touched.count(p) || !live(p) || p->leaf());
       if (ok)
         for (Block* ch : p->children) ok = ok && ch->leaf() && touched.count(ch) == 0;
       ok = ok && can_coarsen(p);
-      cache.ok[i] = ok ? 1 : 0;
+      if (!ok) continue;
+      cache.ok_idx.push_back((int)i);
+      k = cache.ok_idx.size();
     }
-    if (!cache.ok[i]) continue;
+    Block* p = ev[i].p;
     if (need.count(p)) continue;
     bool close = false;
     for (const Block* q : need)
@@ -327,12 +344,16 @@ struct Run {
     touched.insert(p);
     ops[p->slot] = op;
   }
+  // (refine: the blocks a failed split would take, for make_room)
+  BlockSet need;
+  int cost = -1;
   bool step(int what, Block* b) {
     std::vector<int> s = {what, b->level};
     for (int a = 0; a < t.ndim; a++) s.push_back(b->c[a]);
     steps.push_back(s);
     if (what == ADAPT_REFINE) {
-      const std::vector<Block*> split = t.refine(b, &evicted);
+      cost = -1;
+      const std::vector<Block*> split = t.refine(b, &evicted, &need, &cost);
       for (Block* q : split) {
         touched.insert(q);
         for (int o = 0; o < (int)q->children.size(); o++) {
@@ -374,22 +395,24 @@ struct Run {
 std::vector<RegridOp> BlockTree::adapt(const std::function<double(const Block*)>& indicator, double hi, double lo,
                                        const std::function<double(const Block*)>& tier) {
   const std::vector<Block*> before = leaves();
-  std::unordered_map<const Block*, double> ind, tiers;
+  SlotVals ind, tiers;
+  ind.init(cap);
+  tiers.init(cap);
   for (Block* b : before) {
     const double t = tier ? tier(b) : NO_TIER;
-    tiers[b] = t;
+    tiers.set(b, t);
     const double raw = indicator(b);
-    ind[b] = (t < NO_TIER && raw >= 0) ? std::max(raw, ZONE_INDICATOR) : raw;
+    ind.set(b, (t < NO_TIER && raw >= 0) ? std::max(raw, ZONE_INDICATOR) : raw);
   }
   std::unordered_set<const Block*> touched;
   Run run{*this, touched, {}, {}, {}};
 
   std::vector<Block*> wanted;
   for (Block* b : before)
-    if (ind[b] > hi && b->level < level_limit) wanted.push_back(b);
+    if (ind.get(b, 0.0) > hi && b->level < level_limit) wanted.push_back(b);
   std::stable_sort(wanted.begin(), wanted.end(), [&](Block* a, Block* b) {
-    const double ta = tiers[a], tb = tiers[b];
-    if (ta == tb) return ind[a] > ind[b];
+    const double ta = tiers.get(a, NO_TIER), tb = tiers.get(b, NO_TIER);
+    if (ta == tb) return ind.get(a, 0.0) > ind.get(b, 0.0);
     return ta < tb;
   });
   bool have_ev = false;
@@ -403,21 +426,20 @@ std::vector<RegridOp> BlockTree::adapt(const std::function<double(const Block*)>
         ev = evictable(before, ind, tier);
         have_ev = true;
       }
-      if (make_room(b, ind[b], ev, touched, tiers[b], room, ev_cache)) {
+      // (the failed split's own count, if it got that far: make_room needs the same at this version)
+      const bool known = run.cost >= 0;
+      if (make_room(b, ind.get(b, 0.0), ev, touched, tiers.get(b, NO_TIER), room, ev_cache, known ? &run.need : nullptr,
+                    run.cost)) {
         for (Block* p : room) run.step(ADAPT_EVICT, p);
         run.step(ADAPT_REFINE, b);
       }
     }
   }
 
-  auto ind_of = [&](const Block* b) {
-    auto it = ind.find(b);
-    return it == ind.end() ? 0.0 : it->second;
-  };
+  auto ind_of = [&](const Block* b) { return ind.get(b, 0.0); };
   auto hot = [&](const Block* b) {
     if (ind_of(b) > lo) return true;
-    auto tt = tiers.find(b);
-    if (tt != tiers.end() && tt->second < NO_TIER) return true;
+    if (tiers.has(b) && tiers.get(b, NO_TIER) < NO_TIER) return true;
     if (ind_of(b) < 0) return false;
     for (int f = 0; f < nface; f++) {
       Neighbor nb = neighbor(b, f);

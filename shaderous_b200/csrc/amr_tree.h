@@ -42,6 +42,25 @@ struct Block {
   bool leaf() const { return children.empty(); }
 };
 
+// A set of the few blocks one refinement takes (a leaf and the coarser neighbours balance splits
+// with it), searched linearly: cheaper than a hash set at that size, and adapt asks for one per
+// flagged leaf.
+struct BlockSet {
+  std::vector<const Block*> v;
+  size_t count(const Block* b) const {
+    for (const Block* x : v)
+      if (x == b) return 1;
+    return 0;
+  }
+  bool insert(const Block* b) {
+    if (count(b)) return false;
+    v.push_back(b);
+    return true;
+  }
+  std::vector<const Block*>::const_iterator begin() const { return v.begin(); }
+  std::vector<const Block*>::const_iterator end() const { return v.end(); }
+};
+
 struct RegridOp {
   int kind = RG_NONE;
   int src = -1;
@@ -78,7 +97,10 @@ class BlockTree {
   Block* get(int level, const int c[3]) const;
   Neighbor neighbor(const Block* b, int f) const;
   Block* at_offset(const Block* b, const int d[3]) const;
-  std::vector<Block*> refine(Block* b, const std::unordered_set<Block*>* forbidden = nullptr);
+  // need_out / cost_out (if given): the blocks the split would take and their slots, once computed
+  // (a refinement that fails for want of slots hands them on to make_room).
+  std::vector<Block*> refine(Block* b, const std::unordered_set<Block*>* forbidden = nullptr,
+                             BlockSet* need_out = nullptr, int* cost_out = nullptr);
   bool can_coarsen(const Block* p) const;
   void coarsen(Block* p);
   int cost_to_refine(const std::vector<Block*>& list) const;
@@ -105,23 +127,44 @@ class BlockTree {
   bool live(const Block* b) const;
   Block* same_level(const Block* b, int f) const;
   std::vector<Block*> coarser_around(const Block* b) const;
-  int refine_cost(const Block* b, std::unordered_set<const Block*>& seen) const;
+  template <class Set>
+  int refine_cost(const Block* b, Set& seen) const;
   struct Evictable {
     Block* p;
     double score;
     double tier;
   };
-  std::vector<Evictable> evictable(const std::vector<Block*>& leaves, const std::unordered_map<const Block*, double>& ind,
+  // A value per block, held by slot with the block it belongs to (a slot freed and taken again in
+  // one re-mesh belongs to another block: blocks are never reused, so identity tells them apart).
+  struct SlotVals {
+    std::vector<const Block*> who;
+    std::vector<double> v;
+    void init(int n) {
+      who.assign(n, nullptr);
+      v.assign(n, 0.0);
+    }
+    void set(const Block* b, double x) {
+      who[b->slot] = b;
+      v[b->slot] = x;
+    }
+    bool has(const Block* b) const { return who[b->slot] == b; }
+    double get(const Block* b, double dflt) const { return who[b->slot] == b ? v[b->slot] : dflt; }
+  };
+  std::vector<Evictable> evictable(const std::vector<Block*>& leaves, const SlotVals& ind,
                                    const std::function<double(const Block*)>& tier) const;
   bool near(const Block* a, const Block* q) const;
   // The part of make_room's test of a candidate that does not depend on the block being refined,
-  // per entry of `ev`, for one version of the tree (recomputed when the tree has changed).
+  // for one version of the tree (recomputed when the tree has changed): the entries of `ev` below
+  // `evaluated` have been tested, and ok_idx lists those that passed, in order.
   struct EvictCache {
-    std::vector<signed char> ok;
+    std::vector<int> ok_idx;
+    size_t evaluated = 0;
     uint64_t version = ~0ull;
   };
+  // need / cost: b's refine_cost set and count if already computed at this version (else null).
   bool make_room(Block* b, double level, const std::vector<Evictable>& ev, const std::unordered_set<const Block*>& touched,
-                 double tier, std::vector<Block*>& out, EvictCache& cache);
+                 double tier, std::vector<Block*>& out, EvictCache& cache,
+                 const BlockSet* need = nullptr, int cost = 0);
 
   std::deque<Block> arena_;  // blocks are never freed while the tree lives (identity for live())
   std::unordered_map<int64_t, Block*> blocks_;
