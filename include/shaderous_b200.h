@@ -287,7 +287,9 @@ int shz_tree_stats(const shz_tree* t, int32_t* blocks, int32_t* free_slots, int3
  * A step is assemble -> clock -> predict -> update (src/amr/amr_sim.ts:2709-2946), captured as
  * one CUDA graph; every regrid_every steps (REGRID_EVERY = 8, amr_sim.ts:73) the Löhner
  * indicator (amr/flag.wgsl) drives BlockTree.adapt and the new leaves are filled
- * (amr/regrid.wgsl). Limiters minmod, mc, vanleer and koren (PPM needs a third ghost layer).
+ * (amr/regrid.wgsl). The check is made at the start of the next step, from that step's own
+ * assemble, as the reference applies a re-mesh at the start of the next steps (applyRegrid).
+ * Limiters minmod, mc, vanleer and koren (PPM needs a third ghost layer).
  */
 typedef struct shz_amr_config {
   shz_config hydro;     /* physics and boundaries; n[] and dx are ignored */

@@ -5,7 +5,8 @@
 // sweep: amr_kernels.cu), or of four with two_pass (predict and update in place of the last two);
 // every regrid_every steps the Löhner flags
 // are read back, BlockTree.adapt decides the new mesh on the host, the new tables go up and the
-// regrid kernel fills the new leaves (amr_sim.ts:2648 applyRegrid, :3033 encodeFlags, :3525 readFlags).
+// regrid kernel fills the new leaves (amr_sim.ts:2648 applyRegrid, :3033 encodeFlags, :3525 readFlags);
+// the check runs at the start of the next step, from that step's own assemble (check_step).
 // With per-block timesteps (time_bins) time advances in cycles of 2^time_bins substeps
 // (amr_sim.ts:1509-1660 encodeCycle): see cycle_once.
 #include <cuda_runtime.h>
@@ -54,6 +55,8 @@ struct shz_amr {
   std::vector<float> h_flags;
   int cur = 0, slot = 0;
   long long since_check = 0;
+  // a refinement check is due before the next single step: its assemble is that step's own
+  bool flags_due = false;
   cudaStream_t stream = nullptr;
   cudaGraphExec_t graphs[4] = {nullptr, nullptr, nullptr, nullptr};
   long long graph_launches[4] = {0, 0, 0, 0};  // kernels one replay of each graph launches
@@ -223,13 +226,20 @@ int n_leaves(const shz_amr* a) { return (int)a->h_leaves.size(); }
 // enqueued. With tune_now (an eager step, never a capture), kernels whose shape is not tuned yet
 // are timed in place over their candidates first (each candidate repeats the same step's work);
 // the clock is read back so that a held step (which only copies) tunes nothing.
-int enqueue_step(shz_amr* a, bool tune_now, long long* launches) {
+// The assemble of a step (its first kernel).
+int enqueue_assemble(shz_amr* a, bool tune_now, long long* launches) {
   // (the two passes predict same-level ghosts at their source, whose atlas may be a parent's;
   // everything the fused sweep reads is a leaf's)
   const int* asm_list = a->cfg.two_pass ? a->d_all : a->d_leaves;
   const int asm_n = a->cfg.two_pass ? n_all(a) : n_leaves(a);
   AMR_CUDA(a, shz::amr_assemble_tuned(a->L, asm_list, asm_n, a->u1[a->cur], a->u2[a->cur], a->rates, a->slot, a->stream,
                                       tune_now, launches));
+  return 0;
+}
+
+// The rest of a step after its assemble: the clock, then the fine-flux pass and the sweep (or the
+// two passes).
+int enqueue_rest(shz_amr* a, bool tune_now, long long* launches) {
   AMR_CUDA(a, shz::launch_clock_multi(a->clk, a->rates, a->slot, 1, a->stream));
   *launches += 1;
   if (tune_now) {
@@ -249,6 +259,11 @@ int enqueue_step(shz_amr* a, bool tune_now, long long* launches) {
                                      a->u2[1 - a->cur], a->clk, a->stream, tune_now, launches));
   }
   return 0;
+}
+
+int enqueue_step(shz_amr* a, bool tune_now, long long* launches) {
+  int rc = enqueue_assemble(a, tune_now, launches);
+  return rc ? rc : enqueue_rest(a, tune_now, launches);
 }
 
 // One step, as the CUDA graph of its kernels for this (state parity, rate slot); the graphs
@@ -611,6 +626,51 @@ int check_and_regrid(shz_amr* a, const std::vector<double>* extra, int* changed)
   return 0;
 }
 
+// A single step that begins with the refinement check due after the last (amr_sim.ts applies a
+// re-mesh decided after a step at the start of the next, applyRegrid): the step's own assemble
+// gives the primitives the Löhner pass reads, so the check needs no assemble of its own. If the
+// mesh changes, the new leaves are filled and the step runs on the new mesh (its assemble's rate
+// taken back); if not, the step goes on from its assemble. Launched eagerly, not from a graph.
+int check_step(shz_amr* a) {
+  a->flags_due = false;
+  long long n = 0;
+  int rc = enqueue_assemble(a, false, &n);
+  if (rc) return rc;
+  AMR_CUDA(a, cudaMemsetAsync(a->d_flags, 0, sizeof(float) * a->cfg.cap, a->stream));
+  AMR_CUDA(a, shz::amr_launch_flag(a->L, a->d_leaves, n_leaves(a), a->d_flags, a->stream));
+  n += 1;
+  a->h_flags.resize(a->cfg.cap);
+  AMR_CUDA(a, cudaMemcpyAsync(a->h_flags.data(), a->d_flags, sizeof(float) * a->cfg.cap, cudaMemcpyDeviceToHost, a->stream));
+  AMR_CUDA(a, cudaStreamSynchronize(a->stream));
+  a->launches += n;
+  std::vector<RegridOp> ops;
+  try {
+    ops = a->tree->adapt([&](const shz::amr::Block* b) { return (double)a->h_flags[b->slot]; }, a->cfg.refine_hi,
+                         a->cfg.refine_lo);
+  } catch (const std::exception& e) {
+    return fail(a, SHZ_E_CONFIG, "adapt: %s", e.what());
+  }
+  if (!ops.empty()) {
+    a->h_rg.resize((size_t)a->cfg.cap * shz::amr::RG_STRIDE);
+    BlockTree::regrid_table(ops, a->cfg.cap, a->h_rg.data());
+    AMR_CUDA(a, cudaMemcpyAsync(a->d_rg, a->h_rg.data(), a->h_rg.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                                a->stream));
+    if ((rc = upload_tables(a))) return rc;
+    AMR_CUDA(a, shz::amr_launch_regrid(a->L, a->d_rg, a->d_leaves, n_leaves(a), a->u1[a->cur], a->u2[a->cur],
+                                       a->u1[1 - a->cur], a->u2[1 - a->cur], a->stream));
+    a->launches += 1;
+    a->cur ^= 1;
+    AMR_CUDA(a, cudaMemsetAsync(a->rates + a->slot, 0, sizeof(unsigned), a->stream));
+    return step_once(a);
+  }
+  n = 0;
+  if ((rc = enqueue_rest(a, false, &n))) return rc;
+  a->launches += n;
+  a->cur ^= 1;
+  a->slot ^= 1;
+  return 0;
+}
+
 // Level-0 cell size and the finest grid, for sampling problems.
 double dx0_of(const shz_amr_config& c) { return c.box / (c.nr * shz::amr::BS); }
 
@@ -707,15 +767,21 @@ int step_n(shz_amr* a, int n, int* taken) {
     // with per-block timesteps, whole cycles (which may run past n), unless paused
     const bool cycle = a->cfg.time_bins > 0 && a->bin_pause == 0;
     if (!cycle && a->bin_pause > 0) a->bin_pause--;
-    int rc = cycle ? cycle_once(a) : step_once(a);
+    int rc = 0;
+    if (cycle && a->flags_due) {
+      // the mesh is checked between cycles, before the next begins
+      a->flags_due = false;
+      int changed = 0;
+      if ((rc = check_and_regrid(a, nullptr, &changed))) return rc;
+    }
+    rc = cycle ? cycle_once(a) : a->flags_due ? check_step(a) : step_once(a);
     if (rc) return rc;
     const int took = cycle ? 1 << a->cfg.time_bins : 1;
     i += took;
     a->since_check += took;
     if (a->cfg.regrid_every > 0 && a->since_check >= a->cfg.regrid_every) {
       a->since_check = 0;
-      int changed = 0;
-      if ((rc = check_and_regrid(a, nullptr, &changed))) return rc;
+      a->flags_due = true;
     }
   }
   if (taken) *taken = i;
@@ -905,6 +971,7 @@ int shz_amr_reset_problem(shz_amr* a, const shz_problem* prob) {
     if (!changed) break;
   }
   a->since_check = 0;
+  a->flags_due = false;
   reset_bins(a);
   return write_clock(a, 0.0, 0);
 }
@@ -919,6 +986,7 @@ int shz_amr_regrid(shz_amr* a, int32_t* changed) {
   if (!a || !changed) return SHZ_E_CONFIG;
   Dev dv(a->device);
   int ch = 0;
+  a->flags_due = false;
   int rc = check_and_regrid(a, nullptr, &ch);
   *changed = ch;
   return rc;
