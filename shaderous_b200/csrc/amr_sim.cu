@@ -42,6 +42,8 @@ struct shz_amr {
   shz::KParams* d_gp = nullptr;  // this run's parameters: grid 0 of the passes' per-grid table
   float* d_flags = nullptr;
   shz::DevClock* clk = nullptr;
+  shz::DevClock* clk_save = nullptr;  // the clock before a step taken ahead of its refinement check
+  cudaEvent_t flags_ready = nullptr;
   unsigned* rates = nullptr;  // slots 0, 1: the steps'; 2, 3: the refinement check's
   double *diag_part = nullptr, *diag_out = nullptr;
   int* d_ghost = nullptr;
@@ -53,6 +55,7 @@ struct shz_amr {
   int nfine = 0, fine_cap = 0;
   std::vector<int32_t> h_bt, h_all, h_leaves, h_rg, h_flist;
   std::vector<float> h_flags;
+  float* h_flags_pinned = nullptr;  // the refinement check's flags, copied back while the step runs
   int cur = 0, slot = 0;
   long long since_check = 0;
   // a refinement check is due before the next single step: its assemble is that step's own
@@ -628,9 +631,12 @@ int check_and_regrid(shz_amr* a, const std::vector<double>* extra, int* changed)
 
 // A single step that begins with the refinement check due after the last (amr_sim.ts applies a
 // re-mesh decided after a step at the start of the next, applyRegrid): the step's own assemble
-// gives the primitives the Löhner pass reads, so the check needs no assemble of its own. If the
-// mesh changes, the new leaves are filled and the step runs on the new mesh (its assemble's rate
-// taken back); if not, the step goes on from its assemble. Launched eagerly, not from a graph.
+// gives the primitives the Löhner pass reads, so the check needs no assemble of its own. The rest
+// of the step is launched at once, ahead of the decision (the reference's speculation behind an
+// unanswered check, amr_sim.ts:2762-2775), and BlockTree.adapt runs on the host meanwhile. The step
+// writes the other parity, so the state it started from is still there: if the mesh changes, the
+// clock is put back as it was, the new leaves are filled from that state and the step runs again
+// on the new mesh (its rate taken back); if not, the step stands. Launched eagerly, not from a graph.
 int check_step(shz_amr* a) {
   a->flags_due = false;
   long long n = 0;
@@ -640,9 +646,14 @@ int check_step(shz_amr* a) {
   AMR_CUDA(a, shz::amr_launch_flag(a->L, a->d_leaves, n_leaves(a), a->d_flags, a->stream));
   n += 1;
   a->h_flags.resize(a->cfg.cap);
-  AMR_CUDA(a, cudaMemcpyAsync(a->h_flags.data(), a->d_flags, sizeof(float) * a->cfg.cap, cudaMemcpyDeviceToHost, a->stream));
-  AMR_CUDA(a, cudaStreamSynchronize(a->stream));
+  AMR_CUDA(a, cudaMemcpyAsync(a->h_flags_pinned, a->d_flags, sizeof(float) * a->cfg.cap, cudaMemcpyDeviceToHost,
+                              a->stream));
+  AMR_CUDA(a, cudaEventRecord(a->flags_ready, a->stream));
+  AMR_CUDA(a, cudaMemcpyAsync(a->clk_save, a->clk, sizeof(shz::DevClock), cudaMemcpyDeviceToDevice, a->stream));
+  if ((rc = enqueue_rest(a, false, &n))) return rc;
   a->launches += n;
+  AMR_CUDA(a, cudaEventSynchronize(a->flags_ready));
+  std::memcpy(a->h_flags.data(), a->h_flags_pinned, sizeof(float) * a->cfg.cap);
   std::vector<RegridOp> ops;
   try {
     ops = a->tree->adapt([&](const shz::amr::Block* b) { return (double)a->h_flags[b->slot]; }, a->cfg.refine_hi,
@@ -651,6 +662,9 @@ int check_step(shz_amr* a) {
     return fail(a, SHZ_E_CONFIG, "adapt: %s", e.what());
   }
   if (!ops.empty()) {
+    // the step taken ahead is void: the clock as it was, the rate slot empty for the new mesh
+    AMR_CUDA(a, cudaMemcpyAsync(a->clk, a->clk_save, sizeof(shz::DevClock), cudaMemcpyDeviceToDevice, a->stream));
+    AMR_CUDA(a, cudaMemsetAsync(a->rates + a->slot, 0, sizeof(unsigned), a->stream));
     a->h_rg.resize((size_t)a->cfg.cap * shz::amr::RG_STRIDE);
     BlockTree::regrid_table(ops, a->cfg.cap, a->h_rg.data());
     AMR_CUDA(a, cudaMemcpyAsync(a->d_rg, a->h_rg.data(), a->h_rg.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
@@ -660,12 +674,8 @@ int check_step(shz_amr* a) {
                                        a->u1[1 - a->cur], a->u2[1 - a->cur], a->stream));
     a->launches += 1;
     a->cur ^= 1;
-    AMR_CUDA(a, cudaMemsetAsync(a->rates + a->slot, 0, sizeof(unsigned), a->stream));
     return step_once(a);
   }
-  n = 0;
-  if ((rc = enqueue_rest(a, false, &n))) return rc;
-  a->launches += n;
   a->cur ^= 1;
   a->slot ^= 1;
   return 0;
@@ -869,6 +879,9 @@ int shz_amr_create(const shz_amr_config* cfg, shz_amr** out) {
   ok = ok && cudaMalloc(&a->d_rg, cap * shz::amr::RG_STRIDE * sizeof(int)) == cudaSuccess;
   ok = ok && cudaMalloc(&a->d_flags, cap * sizeof(float)) == cudaSuccess;
   ok = ok && cudaMalloc(&a->clk, sizeof(shz::DevClock)) == cudaSuccess;
+  ok = ok && cudaMalloc(&a->clk_save, sizeof(shz::DevClock)) == cudaSuccess;
+  ok = ok && cudaMallocHost(&a->h_flags_pinned, cap * sizeof(float)) == cudaSuccess;
+  ok = ok && cudaEventCreateWithFlags(&a->flags_ready, cudaEventDisableTiming) == cudaSuccess;
   ok = ok && cudaMalloc(&a->rates, 6 * sizeof(unsigned)) == cudaSuccess;
   if (ok) ok = cudaMemset(a->rates, 0, 6 * sizeof(unsigned)) == cudaSuccess;
   if (c.time_bins > 0) {
@@ -925,10 +938,12 @@ void shz_amr_destroy(shz_amr* a) {
   }
   void* bufs[] = {a->w1, a->w2, a->p1, a->p2, a->d_bt, a->d_all, a->d_leaves, a->d_rg, a->d_flags, a->d_gp,
                   a->clk, a->rates, a->diag_part, a->diag_out, a->d_ghost, a->d_flist, a->fbuf, a->d_err,
-                  a->d_bins[0], a->d_bins[1], a->d_brate, a->d_cyc};
+                  a->d_bins[0], a->d_bins[1], a->d_brate, a->d_cyc, a->clk_save};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (a->h_bins) cudaFreeHost(a->h_bins);
+  if (a->h_flags_pinned) cudaFreeHost(a->h_flags_pinned);
+  if (a->flags_ready) cudaEventDestroy(a->flags_ready);
   if (a->h_cyc) cudaFreeHost(a->h_cyc);
   if (a->bins_ready) cudaEventDestroy(a->bins_ready);
   if (a->stream) cudaStreamDestroy(a->stream);
