@@ -219,3 +219,25 @@ def test_periodic_runs_with_bins_conserve(case, two_pass):
     scale = abs(d0.mass)  # momentum per unit of mass moving at 1 (the flows' speeds are of order 1)
     assert abs(d1.momentum[0] - d0.momentum[0]) / scale < 1e-6
     assert abs(d1.momentum[1] - d0.momentum[1]) / scale < 1e-6
+
+
+@pytest.mark.parametrize("ndim", [2, 3])
+def test_bins_on_a_single_periodic_root(ndim):
+    """One root block on a periodic box is its own neighbour across every face (the table's
+    neighbour entry is the block itself): the bin rules, the flux pass and the deposits skip it as
+    a neighbour. The one block is in the fastest bin; the cycles conserve."""
+    hyd = Config(gamma=1.4, bc_lo=(0, 0, 0), bc_hi=(0, 0, 0), recon="mc", cfl=0.7)
+    cfg = AmrConfig(hydro=hyd, ndim=ndim, nr=1, max_level=0, cap=4, regrid_every=8, time_bins=2,
+                    time_bins_always=True)
+    with AmrSim(cfg) as a:
+        a.reset(Problem("blast", a=(1, 10, 1, 0.1, 0.2)))
+        tab = a.table()
+        assert all(int(tab[0, 6 + f]) == 0 for f in range(2 * ndim))
+        d0 = a.diagnostics()
+        a.run(steps=16 + 10 * 4)
+        d1 = a.diagnostics()
+        work = a.bin_work()
+        kb, _ = a.bins()
+    assert work["cycles"] == 10 and work["updates"] == work["single"] == 10 * 4 and kb[1] == 0
+    assert abs(d1.mass - d0.mass) / d0.mass < 1e-6
+    assert abs(d1.e_tot - d0.e_tot) / d0.e_tot < 1e-6
