@@ -116,8 +116,11 @@ __device__ __forceinline__ float ppm_slope(float am, float a, float ap) {
   const float d = 0.5f * (ap - am);
   return same_sign(ap - a, a - am) ? copysignf(fminf(fabsf(d), fminf(2.f * fabsf(a - am), 2.f * fabsf(ap - a))), d) : 0.f;
 }
-__device__ __forceinline__ void ppm_incs(float a2m, float am, float a, float ap, float a2p, float& su, float& sd) {
-  const float dm = ppm_slope(a2m, am, a), d0 = ppm_slope(am, a, ap), dp = ppm_slope(a, ap, a2p);
+// The edge increments of one cell from its neighbours and the limited slopes at the cells below,
+// at and above it (dm, d0, dp): a sweep that has the slopes already (carried along its march) gives
+// them here.
+__device__ __forceinline__ void ppm_incs_d(float am, float a, float ap, float dm, float d0, float dp, float& su,
+                                           float& sd) {
   float al = 0.5f * (am + a) - (d0 - dm) * (1.f / 6.f);
   float ar = 0.5f * (a + ap) - (dp - d0) * (1.f / 6.f);
   if ((ar - a) * (a - al) <= 0.f) {
@@ -130,6 +133,9 @@ __device__ __forceinline__ void ppm_incs(float a2m, float am, float a, float ap,
   }
   su = 2.f * (ar - a);
   sd = 2.f * (a - al);
+}
+__device__ __forceinline__ void ppm_incs(float a2m, float am, float a, float ap, float a2p, float& su, float& sd) {
+  ppm_incs_d(am, a, ap, ppm_slope(a2m, am, a), ppm_slope(am, a, ap), ppm_slope(a, ap, a2p), su, sd);
 }
 
 // The edge increments of one cell along one axis (hydro.ts:282-293; the ghost form :347-356):

@@ -248,6 +248,12 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, REC
 
   const int jb = (DIM == 3) ? z0 - 1 : 0;
   const int je = (DIM == 3) ? z1 : 0;
+  // PPM along z: each plane's limited slope of the column's cell is used by the planes below, at
+  // and above it; it is formed once, when plane j + 1's is first needed, and carried up the march
+  // (zs_m, zs_0: the slopes at planes j - 1 and j; both formed at the first plane).
+  constexpr bool ZCARRY = RECON == R_PPM && DIM == 3;
+  float zs_m[6], zs_0[6];
+  bool zs_ready = false;
   for (int j = jb; j <= je; j++) {
     // 1. primitives of plane j + ZH (the plane itself when there is no march)
     const int lp = (DIM == 3) ? j + ZH : 0;
@@ -273,6 +279,33 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, REC
       __syncthreads();
     }
     const float* sWj = ring((DIM == 3) ? j : 0);
+    if constexpr (ZCARRY) {
+      if (!zs_ready) {
+        float c2[7], c1[7], a0[7], b1[7];
+        read_w<DIM, RECON>(ring(j - 2), wx, wy, c2);
+        read_w<DIM, RECON>(ring(j - 1), wx, wy, c1);
+        read_w<DIM, RECON>(sWj, wx, wy, a0);
+        read_w<DIM, RECON>(ring(j + 1), wx, wy, b1);
+#pragma unroll
+        for (int v = 0; v < 6; v++) {
+          zs_m[v] = ppm_slope(c2[v], c1[v], a0[v]);
+          zs_0[v] = ppm_slope(c1[v], a0[v], b1[v]);
+        }
+        zs_ready = true;
+      }
+    }
+    // the z edge increments of this plane's cell (c; m, p below and above) from the carried
+    // slopes and the new one at plane j + 1; the slopes then move up a plane
+    auto z_edges = [&](const float* m, const float* c, const float* p, float* su_z, float* sd_z) {
+      const float* p2s = ring(j + 2) + wy * G::WX + wx;
+#pragma unroll
+      for (int v = 0; v < 6; v++) {
+        const float zp = ppm_slope(c[v], p[v], p2s[v * WN]);
+        ppm_incs_d(m[v], c[v], p[v], zs_m[v], zs_0[v], zp, su_z[v], sd_z[v]);
+        zs_m[v] = zs_0[v];
+        zs_0[v] = zp;
+      }
+    };
 
     if constexpr (DIM == 3) {
       // The z ghost planes (outflow / reflect) need only their edges toward the domain, at the
@@ -285,11 +318,13 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, REC
         with_cs(c, P);
         read_w<DIM, RECON>(ring(j - 1) + 0, wx, wy, m);
         read_w<DIM, RECON>(ring(j + 1) + 0, wx, wy, p);
-        if constexpr (RECON == R_PPM) {
-          read_w<DIM, RECON>(ring(j - 2), wx, wy, m2);
-          read_w<DIM, RECON>(ring(j + 2), wx, wy, p2);
+        if constexpr (ZCARRY) {
+          (void)m2;
+          (void)p2;
+          z_edges(m, c, p, su, sd);
+        } else {
+          axis_edges<RECON, ISEN>(m2, m, c, p, p2, P.inv_gamma, su, sd);
         }
-        axis_edges<RECON, ISEN>(m2, m, c, p, p2, P.inv_gamma, su, sd);
         if (zg_lo) {
 #pragma unroll
           for (int v = 0; v < 6; v++) gsu[v] = su[v];
@@ -347,11 +382,11 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, REC
       if constexpr (DIM == 3) {
         read_w<DIM, RECON>(ring(j - 1), wx, wy, m);
         read_w<DIM, RECON>(ring(j + 1), wx, wy, p);
-        if constexpr (RECON == R_PPM) {
-          read_w<DIM, RECON>(ring(j - 2), wx, wy, m2);
-          read_w<DIM, RECON>(ring(j + 2), wx, wy, p2);
+        if constexpr (ZCARRY) {
+          z_edges(m, c, p, su[2], sd[2]);
+        } else {
+          axis_edges<RECON, ISEN>(m2, m, c, p, p2, P.inv_gamma, su[2], sd[2]);
         }
-        axis_edges<RECON, ISEN>(m2, m, c, p, p2, P.inv_gamma, su[2], sd[2]);
         conv += p[3] - m[3];
         jump = fmaxf(jump, fabsf(p[4] - m[4]) / fminf(p[4], m[4]));
       }
