@@ -43,9 +43,10 @@ template <int DIM, int RECON>
 struct Geo {
   static constexpr int H = (RECON == R_PPM) ? 3 : 2;   // halo of the primitives' region
   static constexpr int ZH = (RECON == R_PPM) ? 2 : 1;  // planes each way the predictor reads along z
-  // 3D: 16 x 12 columns, so that two CTAs of 8 warps leave 128 registers a thread (below)
+  // 16 x 12 columns (8 warps a CTA): in 3D two CTAs leave 128 registers a thread (below); in 2D
+  // three CTAs fit per SM at the 2D kernel's 72 registers (two of 16 x 16 did: 10-13 % slower)
   static constexpr int TX = (DIM == 1) ? 126 : 16;
-  static constexpr int TY = (DIM == 1) ? 1 : (DIM == 3) ? 12 : 16;
+  static constexpr int TY = (DIM == 1) ? 1 : 12;
   static constexpr int PX = TX + 2;
   static constexpr int PY = (DIM >= 2) ? TY + 2 : 1;
   static constexpr int NT = PX * PY;
@@ -56,9 +57,9 @@ struct Geo {
   static constexpr int WC = 6;                               // primitives kept per cell (no sound speed)
   static constexpr int NBUF = (DIM == 3) ? 2 * ZH + 1 : 1;   // ring of planes: the predictor's z stencil
   static constexpr int NF = (DIM >= 2) ? 2 : 1;              // in-plane face directions
-  // Registers per thread such that two CTAs are resident per SM. Warps are spread over the SM's
-  // four sub-partitions, each with a 16K-register file: two 11-warp CTAs (2D) put 6 warps on one,
-  // and 6 x 32 x 80 <= 16384; two 8-warp CTAs (3D) put 4, and 4 x 32 x 128 = 16384. The 3D sweep
+  // Registers per thread such that two CTAs are resident per SM (three in 2D). Warps are spread
+  // over the SM's four sub-partitions, each with a 16K-register file: three 8-warp CTAs (2D) put 6
+  // warps on one, and 6 x 32 x 80 <= 16384; two (3D) put 4, and 4 x 32 x 128 = 16384. The 3D sweep
   // needs the registers more than the wider columns: at 80 it spilled, and 16 x 12 columns with
   // 128 registers ran 6 % faster than 16 x 16 with 80 (the PPM Taylor-Green vortex at 512^3).
   static constexpr int MAXREG = (DIM == 1) ? 64 : (DIM == 3) ? 128 : 80;
