@@ -121,18 +121,18 @@ __device__ __forceinline__ float ppm_slope(float am, float a, float ap) {
 // them here.
 __device__ __forceinline__ void ppm_incs_d(float am, float a, float ap, float dm, float d0, float dp, float& su,
                                            float& sd) {
-  float al = 0.5f * (am + a) - (d0 - dm) * (1.f / 6.f);
-  float ar = 0.5f * (a + ap) - (dp - d0) * (1.f / 6.f);
-  if ((ar - a) * (a - al) <= 0.f) {
-    al = a;
-    ar = a;
-  } else {
-    const float da = ar - al, a6 = 6.f * (a - 0.5f * (al + ar));
-    if (da * a6 > da * da) al = 3.f * a - 2.f * ar;
-    else if (-da * da > da * a6) ar = 3.f * a - 2.f * al;
-  }
-  su = 2.f * (ar - a);
-  sd = 2.f * (a - al);
+  const float al = 0.5f * (am + a) - (d0 - dm) * (1.f / 6.f);
+  const float ar = 0.5f * (a + ap) - (dp - d0) * (1.f / 6.f);
+  // the monotonicity cases by selects (the same values as branches, without divergence): a local
+  // extremum flattens the parabola; an overshooting edge is pulled in
+  const bool flat = (ar - a) * (a - al) <= 0.f;
+  const float da = ar - al, a6 = 6.f * (a - 0.5f * (al + ar));
+  const bool pull_l = da * a6 > da * da;
+  const bool pull_r = !pull_l && -da * da > da * a6;
+  const float al2 = flat ? a : (pull_l ? 3.f * a - 2.f * ar : al);
+  const float ar2 = flat ? a : (pull_r ? 3.f * a - 2.f * al : ar);
+  su = 2.f * (ar2 - a);
+  sd = 2.f * (a - al2);
 }
 __device__ __forceinline__ void ppm_incs(float a2m, float am, float a, float ap, float a2p, float& su, float& sd) {
   ppm_incs_d(am, a, ap, ppm_slope(a2m, am, a), ppm_slope(am, a, ap), ppm_slope(a, ap, a2p), su, sd);
