@@ -68,12 +68,11 @@ __device__ __forceinline__ void update_cell(const float4 a, const float4 b, cons
   const float ke = (0.5f * (mx * mx + my * my + mz * mz)) / rho;
   const float eth = E - ke;
   const float emin = P.e_floor;
-  if (eth > P.eta_dual * E && eth >= emin) {
-    eint = eth;
-  } else {
-    if (!(eint >= emin)) eint = emin;
-    E = ke + eint;
-  }
+  // the dual-energy switch by selects (a warp whose cells choose differently runs one path)
+  const bool from_total = eth > P.eta_dual * E && eth >= emin;
+  const float eadv = (eint >= emin) ? eint : emin;
+  eint = from_total ? eth : eadv;
+  E = from_total ? E : ke + eadv;
   na = make_float4(rho, mx, my, mz);
   nb = make_float4(E, eint, b.z + dtdx * acc[6], b.w);
 }
