@@ -214,3 +214,35 @@ def test_fused_sweep_equals_two_passes(ndim, recon, isen, bcs):
             assert np.abs(x[..., comp] - y[..., comp]).sum() / scale < 2e-5, comp
     assert d0.steps == d1.steps == 20
     assert d0.t == pytest.approx(d1.t, rel=1e-5)
+
+
+@pytest.mark.parametrize("two_pass", [False, True])
+def test_folded_checks_equal_explicit_checks(two_pass):
+    """The refinement check folded into the next step (its flags from that step's own assemble, the
+    step launched ahead of the host's decision and taken again on a new mesh) gives the same meshes
+    and states, bit for bit, as an explicit check after every 8th step."""
+    hyd = Config(gamma=5 / 3, bc_lo=(1, 1, 1), bc_hi=(1, 1, 1), recon="koren", cfl=0.5, p_floor=1e-12)
+    out = []
+    for folded in (True, False):
+        cfg = AmrConfig(hydro=hyd, ndim=2, nr=4, max_level=2, cap=400, refine_hi=0.1, refine_lo=0.05,
+                        regrid_every=8 if folded else 0, two_pass=two_pass)
+        with AmrSim(cfg) as a:
+            a.reset(Problem("blast", a=(1, 10, 1, 0.1, 0.15)))
+            meshes = []
+            for _ in range(12):
+                if folded:
+                    a.step(8)
+                else:
+                    a.step(8)
+                    a.regrid()
+                _, lv, co = a.leaves()
+                meshes.append(sorted((int(x), *map(int, c)) for x, c in zip(lv, co)))
+            a.step(1)  # the folded run's due check happens here
+            _, lv, co = a.leaves()
+            meshes.append(sorted((int(x), *map(int, c)) for x, c in zip(lv, co)))
+            out.append((meshes, a.leaves_state(), a.clock()))
+    (ma, (a1, a2), ca), (mb, (b1, b2), cb) = out
+    assert len(set(map(tuple, map(tuple, ma)))) > 1  # the mesh changed along the way
+    # the explicit check lands one step earlier than the folded one; after the next step both agree
+    assert ma[-1] == mb[-1] and ca == cb
+    assert np.array_equal(a1, b1) and np.array_equal(a2, b2)
