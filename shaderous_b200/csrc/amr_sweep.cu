@@ -56,9 +56,11 @@ __device__ __forceinline__ void load_w6(const float4* __restrict__ w1, const flo
 // The predictor of texel l0 of block `slot`, read from its primitive atlas, under the ghost rules
 // above; with the edge increments along `axis` at l0 itself (for its face states on that axis).
 // (bins: the per-block timesteps' bin table, or null; a ghost beside a neighbour part way through
-// its step is predicted in place, as beside a coarser block.)
+// its step is predicted in place, as beside a coarser block.) Not inlined: the flux pass calls it
+// from eight places per axis, and one shared copy keeps the pass's code in the instruction cache
+// (inlined, instruction-fetch stalls led; the pass ran 4-7 % of the step slower).
 template <int DIM, int R, bool ISEN>
-__device__ __forceinline__ void predict_texel(const KParams& P, const int* __restrict__ bt, const float4* __restrict__ w1,
+__device__ __noinline__ void predict_texel(const KParams& P, const int* __restrict__ bt, const float4* __restrict__ w1,
                                               const float4* __restrict__ w2, int slot, const int* l0, float h, int axis,
                                               Pred& pr, float* su, float* sd, const int* __restrict__ bins = nullptr) {
   int l[3] = {l0[0], l0[1], l0[2]};
