@@ -354,6 +354,32 @@ int shz_amr_bins(shz_amr* a, int32_t* bins, float* rates);
  * left before the cycles resume (the start of a run, or a pause when they saved too little). */
 int shz_amr_bin_work(shz_amr* a, int64_t* cycles, int64_t* updates, int64_t* single, int32_t* paused);
 
+/* Restart on blocks from a snapshot (io/capture.ts restartFrom, amr_sim.ts:1867-1875 and
+ * 1943-1971). The snapshot's leaves: n blocks, each a level and a position in blocks at that level
+ * (3 ints, z 0 in 2D), on a root grid of root_size[3] cells in blocks of block_size[3] cells,
+ * spanning [lo, hi] along each axis (the Snapshot's rootSize, blockSize, lo, hi); shift is how
+ * many levels finer the file's root cells are than this run's (levels count from the file's
+ * root). */
+typedef struct {
+  int32_t n;
+  const int32_t* levels;
+  const int32_t* coords;
+  int32_t root_size[3];
+  int32_t block_size[3];
+  double lo[3], hi[3];
+  int32_t shift;
+} shz_mesh_spec;
+/* Rebuild the tree as a restart does: up to max_level passes of adapt() that refine every leaf
+ * the snapshot is finer than at one of its children's centres and merge none. The leaves' state
+ * is zero afterwards (set it with shz_amr_set_leaves_state) and the clock at 0. A point the
+ * snapshot's leaves do not cover is refused. */
+int shz_amr_reset_mesh(shz_amr* a, const shz_mesh_spec* mesh);
+/* Replace the state of every leaf, leaves in shz_amr_leaves order, each as shz_amr_get_leaves_state
+ * gives it (16^ndim cells, x fastest, float4 u1 and u2). */
+int shz_amr_set_leaves_state(shz_amr* a, const float* u1, const float* u2);
+/* Set the clock's time and step count (a restart's, Restart.time and .steps). */
+int shz_amr_set_clock(shz_amr* a, double t, int64_t steps);
+
 /*
  * Serving: independent hydro runs ("requests") of uneven sizes kept resident in HBM and advanced
  * together. Every request is a uniform grid of 16^ndim-cell blocks; the blocks of all running

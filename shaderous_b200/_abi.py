@@ -107,6 +107,19 @@ class shz_amr_config(C.Structure):
     ]
 
 
+class shz_mesh_spec(C.Structure):
+    _fields_ = [
+        ("n", C.c_int32),
+        ("levels", C.c_void_p),
+        ("coords", C.c_void_p),
+        ("root_size", C.c_int32 * 3),
+        ("block_size", C.c_int32 * 3),
+        ("lo", C.c_double * 3),
+        ("hi", C.c_double * 3),
+        ("shift", C.c_int32),
+    ]
+
+
 class shz_request(C.Structure):
     _fields_ = [
         ("ndim", C.c_int32),
@@ -222,6 +235,9 @@ SIGNATURES = [
     ("shz_amr_bins", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("shz_amr_bin_work", C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
                                    C.POINTER(C.c_int32)]),
+    ("shz_amr_reset_mesh", C.c_int, [C.c_void_p, C.POINTER(shz_mesh_spec)]),
+    ("shz_amr_set_leaves_state", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("shz_amr_set_clock", C.c_int, [C.c_void_p, C.c_double, C.c_int64]),
     ("shz_server_create", C.c_int, [C.POINTER(shz_server_config), C.POINTER(C.c_void_p)]),
     ("shz_server_destroy", None, [C.c_void_p]),
     ("shz_server_error", C.c_char_p, [C.c_void_p]),

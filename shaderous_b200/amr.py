@@ -174,6 +174,32 @@ class AmrSim:
         self._ok(self._lib.shz_amr_bin_work(self._h, C.byref(cy), C.byref(up), C.byref(si), C.byref(pa)))
         return {"cycles": cy.value, "updates": up.value, "single": si.value, "paused": pa.value}
 
+    def reset_mesh(self, levels, coords, root_size, block_size, lo, hi, shift: int = 0):
+        """Rebuild the mesh from a snapshot's leaves as a restart does (shz_amr_reset_mesh): the
+        leaves' state is zero and the clock 0 until set_leaves_state and set_clock."""
+        lv = np.ascontiguousarray(levels, np.int32)
+        co = np.ascontiguousarray(coords, np.int32).reshape(-1, 3)
+        m = _abi.shz_mesh_spec()
+        m.n = len(lv)
+        m.levels, m.coords = lv.ctypes.data, co.ctypes.data
+        m.root_size[:] = [int(v) for v in root_size]
+        m.block_size[:] = [int(v) for v in block_size]
+        m.lo[:] = [float(v) for v in lo]
+        m.hi[:] = [float(v) for v in hi]
+        m.shift = int(shift)
+        self._ok(self._lib.shz_amr_reset_mesh(self._h, C.byref(m)))
+
+    def set_leaves_state(self, u1: np.ndarray, u2: np.ndarray):
+        """Replace every leaf's state: arrays shaped as leaves_state() gives them."""
+        n = len(self.leaves()[0])
+        cb = self.cfg.cells_per_block
+        u1 = np.ascontiguousarray(u1, np.float32).reshape(n, cb, 4)
+        u2 = np.ascontiguousarray(u2, np.float32).reshape(n, cb, 4)
+        self._ok(self._lib.shz_amr_set_leaves_state(self._h, u1.ctypes.data, u2.ctypes.data))
+
+    def set_clock(self, t: float, steps: int = 0):
+        self._ok(self._lib.shz_amr_set_clock(self._h, float(t), int(steps)))
+
     def uniform_level(self, level: int = 0):
         """Leaves all at one level assembled into a uniform (nz, ny, nx, 4) pair of arrays."""
         s, lv, co = self.leaves()

@@ -9,9 +9,12 @@ describe` (tools/headless/cli.mjs, flags.mjs) for the problems and outputs this 
 
 Outputs, as the reference's runner writes them: `diag.jsonl` (one line of diagnostics per output
 time, at the start, every --every of simulated time and at the end) and `manifest.json` (the
-setup, the outputs). With --state, each output also writes the state as NNNN-tT-state.npz (u1,
-u2 float32 arrays; uniform grids). Screenshots, slices, movies and .athdf files need the
-reference's renderer or an HDF5 library and are not written.
+setup, the outputs). With --athdf, each output also writes the run as an Athena++ HDF5 snapshot
+NNNN-tT.athdf (src/io/athdf.ts; --gzip 1-9 compresses the cells), and --from FILE.athdf starts
+the run from such a file (capture.ts restartFrom: its time, steps and gas, on a uniform grid or
+on blocks). With --state, each output writes the raw state as NNNN-tT-state.npz (u1, u2 float32
+arrays; uniform grids). Screenshots, slices and movies need the reference's renderer and are not
+written.
 """
 from __future__ import annotations
 
@@ -22,7 +25,7 @@ import math
 import sys
 import time
 from pathlib import Path
-from urllib.parse import parse_qsl
+from urllib.parse import parse_qsl, urlencode
 
 # Presets: problem kind, parameters, box (side), boundaries (lo, hi), gamma, end time, limiter.
 # The parameters follow include/shaderous_b200.h SHZ_PROB_*.
@@ -127,12 +130,24 @@ def run_one(setup: dict, ns, out: Path, log) -> dict:
     t0 = time.perf_counter()
     with cls(cfg) as sim, open(out / "diag.jsonl", "w") as diag:
         sim.reset(prob)
+        if getattr(ns, "from_file", None):
+            from .athdf import read_athdf, restart
+
+            restart(sim, read_athdf(ns.from_file))
+            manifest["from"] = str(ns.from_file)
 
         def output(k: int):
             rec = _diag_record(sim, time.perf_counter() - t0)
             diag.write(json.dumps(rec) + "\n")
             diag.flush()
             entry = {"index": k, "t": rec["t"], "steps": rec["steps"]}
+            if getattr(ns, "athdf", False):
+                from .athdf import capture, write_athdf
+
+                name = f"{k:04d}-t{rec['t']:.6g}.athdf"
+                meta = {"program": "shaderous", "build": "b200", "query": urlencode({k2: str(v) for k2, v in setup.items()})}
+                write_athdf(capture(sim, meta), out / name, gzip=getattr(ns, "gzip", 0) or 0)
+                entry["athdf"] = name
             if ns.state and hasattr(sim, "read_state"):
                 u1, u2 = sim.read_state()
                 name = f"{k:04d}-t{rec['t']:.6g}-state.npz"
@@ -192,6 +207,9 @@ def main(argv=None) -> int:
     ap.add_argument("--timeout", type=float, help="give up after this many seconds of wall time")
     ap.add_argument("--out", help="output folder (default runs/<problem>-<date>)")
     ap.add_argument("--state", action="store_true", help="write the state at each output (.npz)")
+    ap.add_argument("--athdf", action="store_true", help="write an Athena++ HDF5 snapshot at each output")
+    ap.add_argument("--gzip", type=int, default=0, help="deflate level 1-9 for the snapshots' cells (0: none)")
+    ap.add_argument("--from", dest="from_file", metavar="FILE", help="start from an .athdf snapshot")
     ap.add_argument("--vary", action="append", metavar="KEY=V1,V2,..")
     ap.add_argument("--quiet", action="store_true")
     ns = ap.parse_args(argv)

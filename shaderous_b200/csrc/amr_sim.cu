@@ -19,6 +19,7 @@
 #include <limits>
 #include <memory>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/shaderous_b200.h"
@@ -1224,6 +1225,121 @@ int shz_amr_bin_work(shz_amr* a, int64_t* cycles, int64_t* updates, int64_t* sin
   if (single) *single = a->bin_single;
   if (paused) *paused = a->bin_pause;
   return 0;
+}
+
+int shz_amr_reset_mesh(shz_amr* a, const shz_mesh_spec* m) {
+  if (!a || !m || m->n < 1 || !m->levels || !m->coords) return SHZ_E_CONFIG;
+  int root[3];
+  for (int ax = 0; ax < 3; ax++) {
+    if (m->block_size[ax] < 1 || m->root_size[ax] < m->block_size[ax] || m->root_size[ax] % m->block_size[ax] ||
+        !(m->hi[ax] > m->lo[ax]))
+      return fail(a, SHZ_E_CONFIG, "the snapshot's root grid along axis %d is not whole blocks over a box", ax);
+    root[ax] = m->root_size[ax] / m->block_size[ax];
+  }
+  Dev dv(a->device);
+  const shz_amr_config& c = a->cfg;
+  // The snapshot's leaves by level and position (SnapshotSampler, io/snapshot.ts): 20 bits per
+  // axis and the level above them.
+  auto key = [](int l, long long i, long long j, long long k) {
+    return ((uint64_t)l << 60) | ((uint64_t)k << 40) | ((uint64_t)j << 20) | (uint64_t)i;
+  };
+  std::unordered_map<uint64_t, int> index;
+  index.reserve((size_t)m->n * 2);
+  int top = 0;
+  for (int b = 0; b < m->n; b++) {
+    const int l = m->levels[b];
+    if (l < 0 || l > 15) return fail(a, SHZ_E_CONFIG, "snapshot block %d: level %d", b, l);
+    for (int ax = 0; ax < 3; ax++) {
+      const long long span = (long long)root[ax] << l;
+      if (m->coords[3 * b + ax] < 0 || m->coords[3 * b + ax] >= span || span > (1 << 20))
+        return fail(a, SHZ_E_CONFIG, "snapshot block %d lies outside its root grid", b);
+    }
+    index.emplace(key(l, m->coords[3 * b], m->coords[3 * b + 1], m->coords[3 * b + 2]), b);
+    top = std::max(top, l);
+  }
+  // SnapshotSampler.level at a point: the finest leaf whose block holds it; -1 if none does.
+  auto level_at = [&](const double x[3]) {
+    double f[3];
+    for (int ax = 0; ax < 3; ax++) {
+      const double v = (x[ax] - m->lo[ax]) / (m->hi[ax] - m->lo[ax]);
+      // an axis of one cell is the same at every point along it
+      f[ax] = m->root_size[ax] == 1 ? 0.0 : std::min(std::max(v, 0.0), 1 - 1e-7);
+    }
+    for (int l = top; l >= 0; l--) {
+      long long at[3];
+      for (int ax = 0; ax < 3; ax++) {
+        const long long span = (long long)root[ax] << l;
+        at[ax] = std::min((long long)std::floor(f[ax] * (double)span), span - 1);
+      }
+      if (index.count(key(l, at[0], at[1], at[2]))) return l;
+    }
+    return -1;
+  };
+  try {
+    a->tree.reset(new BlockTree(c.ndim, c.nr, c.max_level, c.cap, c.hydro.bc_lo, c.hydro.bc_hi));
+  } catch (const std::exception& e) {
+    return fail(a, SHZ_E_CONFIG, "%s", e.what());
+  }
+  const double dx0 = dx0_of(c), half = c.box / 2;
+  const bool three = c.ndim == 3;
+  bool uncovered = false;
+  // finerInSnapshot (amr_sim.ts:1867-1875): the snapshot is finer than the block at the centre of
+  // one of its children; levels shifted to this run's root and never below 0.
+  auto finer = [&](const shz::amr::Block* b) {
+    const double size = shz::amr::BS * dx0 / (double)(1 << b->level);
+    for (int o = 0; o < (three ? 8 : 4); o++) {
+      double x[3] = {0, 0, 0};
+      for (int ax = 0; ax < (three ? 3 : 2); ax++) x[ax] = (b->c[ax] + (((o >> ax) & 1) + 0.5) / 2) * size - half;
+      const int l = level_at(x);
+      if (l < 0) {
+        uncovered = true;
+        return 0.0;
+      }
+      if (std::max(0, l + m->shift) > b->level) return 1.0;
+    }
+    return 0.0;
+  };
+  for (int pass = 0; pass < c.max_level; pass++) {
+    std::vector<RegridOp> ops;
+    try {
+      ops = a->tree->adapt(finer, 0.5, -1.0);
+    } catch (const std::exception& e) {
+      return fail(a, SHZ_E_CONFIG, "adapt: %s", e.what());
+    }
+    if (uncovered) return fail(a, SHZ_E_CONFIG, "the snapshot does not cover the whole domain");
+    if (ops.empty()) break;
+  }
+  int rc = upload_tables(a);
+  if (rc) return rc;
+  a->cur = 0;
+  a->slot = 0;
+  const size_t bytes = (size_t)c.cap * a->CB * sizeof(float4);
+  AMR_CUDA(a, cudaMemsetAsync(a->u1[0], 0, bytes, a->stream));
+  AMR_CUDA(a, cudaMemsetAsync(a->u2[0], 0, bytes, a->stream));
+  a->since_check = 0;
+  a->flags_due = false;
+  reset_bins(a);
+  return write_clock(a, 0.0, 0);
+}
+
+int shz_amr_set_leaves_state(shz_amr* a, const float* u1, const float* u2) {
+  if (!a || !u1 || !u2) return SHZ_E_CONFIG;
+  Dev dv(a->device);
+  const size_t bytes = (size_t)a->CB * sizeof(float4);
+  for (int i = 0; i < n_leaves(a); i++) {
+    const size_t s = (size_t)a->h_leaves[i] * a->CB;
+    AMR_CUDA(a, cudaMemcpyAsync(a->u1[a->cur] + s, u1 + (size_t)i * a->CB * 4, bytes, cudaMemcpyHostToDevice, a->stream));
+    AMR_CUDA(a, cudaMemcpyAsync(a->u2[a->cur] + s, u2 + (size_t)i * a->CB * 4, bytes, cudaMemcpyHostToDevice, a->stream));
+  }
+  AMR_CUDA(a, cudaStreamSynchronize(a->stream));
+  return 0;
+}
+
+int shz_amr_set_clock(shz_amr* a, double t, int64_t steps) {
+  if (!a || !std::isfinite(t) || steps < 0) return SHZ_E_CONFIG;
+  Dev dv(a->device);
+  reset_bins(a);
+  return write_clock(a, t, steps);
 }
 
 }  // extern "C"

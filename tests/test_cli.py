@@ -73,3 +73,28 @@ def test_run_writes_outputs(tmp_path):
     assert r.returncode == 0, r.stderr
     lines = [json.loads(x) for x in (out2 / "diag.jsonl").read_text().splitlines()]
     assert lines[-1]["steps"] == 20
+
+
+@pytest.mark.gpu
+def test_run_writes_snapshots_and_restarts_from_one(tmp_path):
+    """--athdf writes an Athena++ snapshot at each output; --from starts a run from one, which then
+    goes on from the file's time and steps (the reference's headless checkpoints and --from)."""
+    out = tmp_path / "blast"
+    r = subprocess.run([sys.executable, "-m", "shaderous_b200", "run", "problem=blast&dim=2&n=32&amr=2", "--steps", "12",
+                        "--out", str(out), "--athdf", "--gzip", "1", "--quiet"],
+                       capture_output=True, text=True, cwd=ROOT, timeout=600)
+    assert r.returncode == 0, r.stderr
+    man = json.loads((out / "manifest.json").read_text())
+    last = out / man["outputs"][-1]["athdf"]
+    from shaderous_b200.athdf import read_athdf
+
+    snap = read_athdf(last)
+    assert snap.steps == 12 and snap.meta["program"] == "shaderous" and "problem=blast" in snap.meta["query"]
+    out2 = tmp_path / "again"
+    r = subprocess.run([sys.executable, "-m", "shaderous_b200", "run", "problem=blast&dim=2&n=32&amr=2", "--steps", "4",
+                        "--from", str(last), "--out", str(out2), "--quiet"], capture_output=True, text=True, cwd=ROOT,
+                       timeout=600)
+    assert r.returncode == 0, r.stderr
+    lines = [json.loads(x) for x in (out2 / "diag.jsonl").read_text().splitlines()]
+    assert lines[0]["steps"] == 12 and lines[-1]["steps"] == 16
+    assert abs(lines[0]["t"] - snap.time) < 1e-12
