@@ -454,8 +454,10 @@ const char* shz_version(void);
  * Candidates differ only in launch shape, never in arithmetic: the state is the same whichever
  * wins. Kernels and their knobs:
  *   0 uniform sweep: tz = planes a CTA marches along z (3D);
- *   1 AMR assemble: variant = register budget (0: 1, 1: 2, 2: 3 CTAs per SM), per_sm = CTAs of
- *     the work-list grid per SM;
+ *   1 AMR assemble: variant = register budget (0: 1, 1: 2, 2: 3 CTAs per SM) of the one-pass
+ *     kernel, or the split form (3: 2, 4: 3 CTAs per SM for its second pass): a light first
+ *     pass for the blocks' own cells and same-level ghosts, then the ghosts beyond a level
+ *     change over only the blocks that have them; per_sm = CTAs of the work-list grid per SM;
  *   2 AMR fused sweep: per_sm;
  *   3 AMR fine-flux pass: per_sm.
  */
@@ -467,6 +469,9 @@ typedef struct shz_tune_entry {
 } shz_tune_entry;
 /* Turn the tuner on (default) or off (every launch takes the default shape). Process-wide. */
 int shz_tune_enable(int32_t on);
+/* Pin one AMR kernel's choice (kernel 1-3 above; variant, per_sm with 0 for the default grid)
+ * for every key, used instead of the tuned one; variant < 0 unpins. Process-wide. */
+int shz_tune_pin(int32_t kernel, int32_t variant, int32_t per_sm);
 /* Forget every choice. */
 void shz_tune_reset(void);
 

@@ -236,6 +236,7 @@ SIGNATURES = [
     ("shz_amr_bin_work", C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
                                    C.POINTER(C.c_int32)]),
     ("shz_amr_reset_mesh", C.c_int, [C.c_void_p, C.POINTER(shz_mesh_spec)]),
+    ("shz_tune_pin", C.c_int, [C.c_int32, C.c_int32, C.c_int32]),
     ("shz_amr_set_leaves_state", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("shz_amr_set_clock", C.c_int, [C.c_void_p, C.c_double, C.c_int64]),
     ("shz_server_create", C.c_int, [C.POINTER(shz_server_config), C.POINTER(C.c_void_p)]),

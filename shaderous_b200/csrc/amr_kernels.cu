@@ -92,6 +92,13 @@ __device__ __forceinline__ void shell_texel(int i, int* l) {
   }
 }
 
+// A ghost whose source is a cell of a same-level leaf (not a parent, whose cells are restricted,
+// and not a leaf part way through a longer step, whose half step is read): one load gives it.
+template <bool BINS>
+__device__ __forceinline__ bool plain_src(const int* __restrict__ bt, const int* __restrict__ bins, const Src& s) {
+  return s.kind == 0 && leaf_of(bt, s.slot) && !(BINS && mid_block(bt, bins, s.slot));
+}
+
 // 1. Primitives of every block in the list with two ghost layers; the rate / dx maximum over the
 // leaves' own cells (assemble.wgsl:78-154; PER_DX in clock.wgsl). MINB: the CTAs per SM the
 // register budget is planned for (the autotuner's variant): more CTAs hide the gather's latency,
@@ -102,7 +109,9 @@ __device__ __forceinline__ void shell_texel(int i, int* l) {
 // With per-block timesteps (BINS, the bin table `bins`), a source leaf part way through its step
 // gives its half-step state from p1, p2 (amr/assemble.wgsl with <mid>, amr/mid_on.wgsl), and each
 // leaf's own rate / dx also goes to brate[slot] for its bin.
-template <int DIM, int R, int MINB, bool BINS>
+// REST: the second pass of the split form, after amr_assemble_plain: only the ghosts whose source
+// is not a same-level leaf's cell (restriction, prolongation, half steps); no rate.
+template <int DIM, int R, int MINB, bool BINS, bool REST>
 __global__ void __launch_bounds__(NT, MINB) amr_assemble(const KParams* __restrict__ gp, const int* __restrict__ bt,
                                                    const int* __restrict__ list, int n, const float4* __restrict__ u1,
                                                    const float4* __restrict__ u2, float4* __restrict__ w1,
@@ -112,6 +121,7 @@ __global__ void __launch_bounds__(NT, MINB) amr_assemble(const KParams* __restri
                                                    float* __restrict__ brate) {
   using T = Tab<DIM>;
   __shared__ float sRed[NT / 32];
+  __shared__ unsigned sPlain;  // REST: bit d set when the ghosts of neighbour direction d are plain
   extern __shared__ __align__(16) float sTab[];
   for (int i = blockIdx.x; i < n; i += gridDim.x) {
     float rmax = 0.f;
@@ -126,6 +136,20 @@ __global__ void __launch_bounds__(NT, MINB) amr_assemble(const KParams* __restri
 #pragma unroll
       for (int f = 0; f < 2 * DIM; f++)
         if (bt_at(bt, slot, 6 + f) == -1) cmask |= 1u << f;
+    if (REST && threadIdx.x < 32) {
+      // Which neighbour directions' ghosts the first pass filled: every texel of a direction
+      // resolves through the same hops to the same kind of source (the hops move an out-of-range
+      // axis into the block whatever its ghost layer), so one texel per direction decides.
+      const int d = threadIdx.x;
+      bool plain = false;
+      if (d < (DIM == 3 ? 27 : 9) && d != (DIM == 3 ? 13 : 4)) {
+        const int l[3] = {d % 3 == 0 ? -1 : d % 3 == 2 ? BS : 0, (d / 3) % 3 == 0 ? -1 : (d / 3) % 3 == 2 ? BS : 0,
+                          DIM == 3 ? (d / 9 == 0 ? -1 : d / 9 == 2 ? BS : 0) : 0};
+        plain = plain_src<BINS>(bt, bins, ghost_src_any<DIM>(bt, slot, l));
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, plain);
+      if (d == 0) sPlain = m;
+    }
     if (cmask) {
       // the table of this block's coarse faces (the previous block's reads of it ended at the
       // barriers of its rate maximum)
@@ -152,11 +176,11 @@ __global__ void __launch_bounds__(NT, MINB) amr_assemble(const KParams* __restri
         else coarse_cell<DIM, R>(bt, u1, u2, nr, slot, m, cs, P.rho_floor, uc, sl, par);
         tab_store(sTab + (size_t)(f * T::CPF + c) * TAB_VALS, uc, sl);
       }
-      __syncthreads();
     }
+    if (cmask || REST) __syncthreads();
     // the block's own cells (a parent's restricted from its children), with the rate maximum
 #pragma unroll 4
-    for (int t = threadIdx.x; t < BG<DIM>::CB; t += NT) {
+    for (int t = threadIdx.x; t < (REST ? 0 : BG<DIM>::CB); t += NT) {
       const int l[3] = {t & (BS - 1), (t >> 4) & (BS - 1), DIM == 3 ? t >> 8 : 0};
       const Cons u = u_at<DIM>(bt, u1, u2, slot, l);
       float w[7];
@@ -170,6 +194,11 @@ __global__ void __launch_bounds__(NT, MINB) amr_assemble(const KParams* __restri
     for (int i = threadIdx.x; i < BG<DIM>::WN - BG<DIM>::CB; i += NT) {
       int l[3];
       shell_texel<DIM>(i, l);
+      if (REST) {
+        const int d = (l[0] < 0 ? 0 : l[0] >= BS ? 2 : 1) + 3 * (l[1] < 0 ? 0 : l[1] >= BS ? 2 : 1) +
+                      (DIM == 3 ? 9 * (l[2] < 0 ? 0 : l[2] >= BS ? 2 : 1) : 0);
+        if ((sPlain >> d) & 1u) continue;
+      }
       const Src s = ghost_src_any<DIM>(bt, slot, l);
       Cons u;
       if (s.kind == 0) {
@@ -201,6 +230,110 @@ __global__ void __launch_bounds__(NT, MINB) amr_assemble(const KParams* __restri
       const size_t o = (size_t)slot * BG<DIM>::WN + wtex<DIM>(l);
       w1[o] = make_float4(w[0], w[1], w[2], w[3]);
       w2[o] = make_float4(w[4], w[5], w[6], 0.f);
+    }
+    if (REST) {
+      __syncthreads();  // the coarse table is rebuilt for the next block
+      continue;
+    }
+    const float m = block_max(rmax, sRed);
+    if (threadIdx.x == 0 && leaf) {
+      atomicMax(rates + 2 * g + rslot, __float_as_uint(m));
+      if (BINS && brate) brate[slot] = m;
+    }
+  }
+}
+
+// 1a. The first pass of the split assemble: what needs no more than one load of a cell per texel,
+// at the occupancy of a light kernel (4 CTAs per SM): every block's own cells, with the rate
+// maximum, and the ghosts whose source is a same-level leaf's cell (its face, edge and corner
+// neighbours at its own level, and its images across the domain's faces). The rest of the ghosts
+// are the second pass's (amr_assemble with REST). Every texel gets the same numbers as in the
+// one-pass kernel: the same load, velocity signs and prim_from_cons.
+template <int DIM, bool BINS>
+__global__ void __launch_bounds__(NT, 4) amr_assemble_plain(const KParams* __restrict__ gp, const int* __restrict__ bt,
+                                                        const int* __restrict__ list, int n, const float4* __restrict__ u1,
+                                                        const float4* __restrict__ u2, float4* __restrict__ w1,
+                                                        float4* __restrict__ w2, unsigned* __restrict__ rates, int rslot,
+                                                        const int* __restrict__ bins, float* __restrict__ brate) {
+  __shared__ float sRed[NT / 32];
+  constexpr int NS = BG<DIM>::WN - BG<DIM>::CB;
+  constexpr int U = 1;  // shell texels a thread resolves, then loads together (more spill in 3D)
+  for (int i = blockIdx.x; i < n; i += gridDim.x) {
+    float rmax = 0.f;
+    const int slot = __ldg(list + i);
+    const int g = bt_at(bt, slot, GRID_WORD);
+    const KParams& P = gp[g];
+    const bool leaf = leaf_of(bt, slot);
+    const float inv_dx = (float)(ldexp(1.0, bt_at(bt, slot, 0)) / P.dx);
+    if (leaf) {
+      // a leaf's own cells: u_at's load of its own cell
+#pragma unroll 4
+      for (int t = threadIdx.x; t < BG<DIM>::CB; t += NT) {
+        const int l[3] = {t & (BS - 1), (t >> 4) & (BS - 1), DIM == 3 ? t >> 8 : 0};
+        const size_t c = (size_t)slot * BG<DIM>::CB + t;
+        const float4 ua = __ldg(u1 + c), ub = __ldg(u2 + c);
+        float w[7];
+        prim_from_cons(ua, ub, P, 1.f, 1.f, 1.f, w);
+        const size_t o = (size_t)slot * BG<DIM>::WN + wtex<DIM>(l);
+        w1[o] = make_float4(w[0], w[1], w[2], w[3]);
+        w2[o] = make_float4(w[4], w[5], w[6], 0.f);
+        rmax = fmaxf(rmax, rate_guard_f(fabsf(w[1]) + fabsf(w[2]) + fabsf(w[3]) + P.signal * w[6]) * inv_dx);
+      }
+    } else {
+      // a parent's (the two-pass form assembles every block): restricted from its children
+      for (int t = threadIdx.x; t < BG<DIM>::CB; t += NT) {
+        const int l[3] = {t & (BS - 1), (t >> 4) & (BS - 1), DIM == 3 ? t >> 8 : 0};
+        const Cons u = u_at<DIM>(bt, u1, u2, slot, l);
+        float w[7];
+        prim_from_cons(u.a, u.b, P, 1.f, 1.f, 1.f, w);
+        const size_t o = (size_t)slot * BG<DIM>::WN + wtex<DIM>(l);
+        w1[o] = make_float4(w[0], w[1], w[2], w[3]);
+        w2[o] = make_float4(w[4], w[5], w[6], 0.f);
+      }
+    }
+    for (int i0 = threadIdx.x; i0 < NS; i0 += U * NT) {
+      long long src[U];
+      int dst[U];  // the texel (13 bits), and bits 13-15: the velocity components whose sign flips
+#pragma unroll
+      for (int q = 0; q < U; q++) {
+        const int k = i0 + q * NT;
+        src[q] = -1;
+        dst[q] = 0;
+        if (k < NS) {
+          int l[3];
+          shell_texel<DIM>(k, l);
+          const Src s = ghost_src_any<DIM>(bt, slot, l);
+          if (plain_src<BINS>(bt, bins, s)) {
+            // u_at's index for a leaf, clamped as there
+            const int c[3] = {min(max(s.l[0], 0), BS - 1), min(max(s.l[1], 0), BS - 1),
+                              DIM == 3 ? min(max(s.l[2], 0), BS - 1) : 0};
+            src[q] = (long long)s.slot * BG<DIM>::CB + cell_ix<DIM>(c);
+            dst[q] = wtex<DIM>(l) | (s.flip[0] < 0.f ? 1 << 13 : 0) | (s.flip[1] < 0.f ? 1 << 14 : 0) |
+                     (s.flip[2] < 0.f ? 1 << 15 : 0);
+          }
+        }
+      }
+      float4 a[U], b[U];
+#pragma unroll
+      for (int q = 0; q < U; q++) {
+        if (src[q] >= 0) {
+          a[q] = __ldg(u1 + src[q]);
+          b[q] = __ldg(u2 + src[q]);
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < U; q++) {
+        if (src[q] < 0) continue;
+        Cons u{a[q], b[q]};
+        u.a.y *= (dst[q] >> 13) & 1 ? -1.f : 1.f;
+        u.a.z *= (dst[q] >> 14) & 1 ? -1.f : 1.f;
+        u.a.w *= (dst[q] >> 15) & 1 ? -1.f : 1.f;
+        float w[7];
+        prim_from_cons(u.a, u.b, P, 1.f, 1.f, 1.f, w);
+        const size_t o = (size_t)slot * BG<DIM>::WN + (dst[q] & 0x1FFF);
+        w1[o] = make_float4(w[0], w[1], w[2], w[3]);
+        w2[o] = make_float4(w[4], w[5], w[6], 0.f);
+      }
     }
     const float m = block_max(rmax, sRed);
     if (threadIdx.x == 0 && leaf) {
@@ -443,10 +576,10 @@ __global__ void amr_ghost_map(const int* __restrict__ bt, int slot, int* __restr
 // Host launchers.
 
 namespace {
-template <int DIM, int R, int MINB, bool BINS = false>
+template <int DIM, int R, int MINB, bool BINS = false, bool REST = false>
 cudaError_t assemble_t(const AmrLaunch& L, int g, const int* list, int n, const float4* u1, const float4* u2,
                        unsigned* rates, int rslot, cudaStream_t s, const int* bins = nullptr, float* brate = nullptr) {
-  auto k = amrk::amr_assemble<DIM, R, MINB, BINS>;
+  auto k = amrk::amr_assemble<DIM, R, MINB, BINS, REST>;
   // (set once per instantiation; not a stream operation)
   static const cudaError_t attr =
       cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)amrk::Tab<DIM>::BYTES);
@@ -466,16 +599,103 @@ cudaError_t assemble_v(const AmrLaunch& L, int g, const int* list, int n, const 
   }
   return cudaSuccess;
 }
+// The split form: the plain pass (own cells and same-level ghosts, 4 CTAs per SM), then the rest
+// of the ghosts with the MINB register budget.
+template <bool BINS>
+cudaError_t assemble_plain(const AmrLaunch& L, const int* list, int n, const float4* u1, const float4* u2,
+                           unsigned* rates, int rslot, cudaStream_t s, const int* bins, float* brate) {
+  const int g = grid_for(n, 4);
+  if (L.ndim == 3)
+    amrk::amr_assemble_plain<3, BINS><<<g, amrk::NT, 0, s>>>(L.gp, L.bt, list, n, u1, u2, L.w1, L.w2, rates, rslot, bins, brate);
+  else
+    amrk::amr_assemble_plain<2, BINS><<<g, amrk::NT, 0, s>>>(L.gp, L.bt, list, n, u1, u2, L.w1, L.w2, rates, rslot, bins, brate);
+  return cudaGetLastError();
+}
+template <int MINB>
+cudaError_t assemble_split(const AmrLaunch& L, int per_sm, const int* list, int n, const float4* u1, const float4* u2,
+                           unsigned* rates, int rslot, cudaStream_t s) {
+  cudaError_t e = assemble_plain<false>(L, list, n, u1, u2, rates, rslot, s, nullptr, nullptr);
+  if (e != cudaSuccess || L.nrest == 0) return e;
+  const int* rl = L.nrest > 0 ? L.rest : list;
+  const int rn = L.nrest > 0 ? L.nrest : n;
+  const int g = grid_for(rn, per_sm);
+  if (L.ndim == 3) {
+    SHZ_RECON_SWITCH(L.recon, false, return (assemble_t<3, R, MINB, false, true>(L, g, rl, rn, u1, u2, rates, rslot, s)))
+  } else {
+    SHZ_RECON_SWITCH(L.recon, false, return (assemble_t<2, R, MINB, false, true>(L, g, rl, rn, u1, u2, rates, rslot, s)))
+  }
+  return cudaSuccess;
+}
 }  // namespace
 
 cudaError_t amr_launch_assemble(const AmrLaunch& L, const int* list, int n, const float4* u1, const float4* u2,
                                 unsigned* rates, int rslot, cudaStream_t s, const tune::Choice* c) {
   if (n <= 0) return cudaSuccess;
-  const int g = grid_for(n, c && c->per_sm > 0 ? c->per_sm : 4);
+  const int per_sm = c && c->per_sm > 0 ? c->per_sm : 4;
+  const int g = grid_for(n, per_sm);
   switch (c ? c->variant : 0) {
     case 1: return assemble_v<2>(L, g, list, n, u1, u2, rates, rslot, s);
     case 2: return assemble_v<3>(L, g, list, n, u1, u2, rates, rslot, s);
+    case 3: return assemble_split<2>(L, per_sm, list, n, u1, u2, rates, rslot, s);
+    case 4: return assemble_split<3>(L, per_sm, list, n, u1, u2, rates, rslot, s);
     default: return assemble_v<1>(L, g, list, n, u1, u2, rates, rslot, s);
+  }
+}
+
+void amr_rest_blocks(const int32_t* bt, int ndim, const int32_t* list, int n, std::vector<int32_t>& out) {
+  using amrk::BS;
+  out.clear();
+  const int S = amrk::BTS;
+  auto leaf = [&](int s) { return (bt[(size_t)s * S + 4] & 2) != 0; };
+  for (int i = 0; i < n; i++) {
+    const int slot = list[i];
+    bool rest = !leaf(slot);
+    for (int d = 0; d < (ndim == 3 ? 27 : 9) && !rest; d++) {
+      const int dir[3] = {d % 3 - 1, (d / 3) % 3 - 1, ndim == 3 ? d / 9 - 1 : 0};
+      if (!dir[0] && !dir[1] && !dir[2]) continue;
+      int m[3];
+      for (int a = 0; a < 3; a++) m[a] = dir[a] < 0 ? -1 : dir[a] > 0 ? BS : 0;
+      // ghost_src_any's hops across all but the last out-of-range axis
+      int cur = slot;
+      for (int hop = 0; hop < ndim; hop++) {
+        int out = 0, axis = -1;
+        for (int a = 0; a < ndim; a++)
+          if (m[a] < 0 || m[a] >= BS) {
+            out++;
+            if (axis < 0) axis = a;
+          }
+        if (out <= 1) break;
+        const int upper = m[axis] >= BS ? 1 : 0;
+        const int nb = bt[(size_t)cur * S + 6 + 2 * axis + upper];
+        if (nb >= 0) {
+          cur = nb;
+          m[axis] += upper ? -BS : BS;
+        } else if (nb <= -2) {
+          if (-1 - nb == 2) m[axis] = upper ? 2 * BS - 1 - m[axis] : -1 - m[axis];
+          else m[axis] = upper ? BS - 1 : 0;
+        } else {
+          for (int a = 0; a < ndim; a++)
+            if (a != axis) m[a] = std::min(std::max(m[a], 0), BS - 1);
+        }
+      }
+      // ghost_src's kind and source block, then plain_src
+      int out = 0, axis = 0;
+      for (int a = 0; a < ndim; a++)
+        if (m[a] < 0 || m[a] >= BS) {
+          out++;
+          axis = a;
+        }
+      int src = cur;
+      if (out > 1) {
+        rest = true;
+      } else if (out == 1) {
+        const int nb = bt[(size_t)cur * S + 6 + 2 * axis + (m[axis] >= BS ? 1 : 0)];
+        if (nb >= 0) src = nb;
+        else if (nb == -1) rest = true;
+      }
+      if (!rest && !leaf(src)) rest = true;
+    }
+    if (rest) out.push_back(slot);
   }
 }
 

@@ -2,6 +2,9 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <cstdint>
+#include <vector>
+
 #include "hydro_math.cuh"
 #include "tune.h"
 
@@ -34,7 +37,18 @@ struct AmrLaunch {
   // of its faces' fluxes in fbuf for this substep (-1: none).
   const int* bins = nullptr;
   const int* fbase = nullptr;
+  // The split assemble's second pass walks these blocks only (amr_rest_blocks over the list the
+  // assemble is given); nrest < 0: every block of that list.
+  const int* rest = nullptr;
+  int nrest = -1;
 };
+
+// The blocks of `list` (n slots; bt the host copy of the block table, 32 ints a row) with a ghost
+// texel whose source is not a cell of a same-level leaf: a coarser leaf beyond a face, or a
+// refined neighbour, whose cells are restricted; every parent. Each of the 26 (2D: 8) neighbour
+// directions is resolved as the assemble's ghost_src_any resolves every texel in it (the hops
+// and the final face give the same blocks wherever the texel lies in that direction's region).
+void amr_rest_blocks(const int32_t* bt, int ndim, const int32_t* list, int n, std::vector<int32_t>& out);
 
 // rates: two 32-bit maxima per grid; the assemble folds the leaves' rate / dx into slot rslot.
 // c: the autotuner's choice (null: the default shape), as for the fine-flux pass and the sweep.

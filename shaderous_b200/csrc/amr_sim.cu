@@ -52,6 +52,8 @@ struct shz_amr {
   // faces matched to refined neighbours (fused sweep): (leaf slot, face, entry) triples and the
   // buffer of their mean fine fluxes, grown with the mesh
   int* d_flist = nullptr;
+  int* d_rest = nullptr;  // the split assemble's second-pass blocks (amr_rest_blocks)
+  std::vector<int32_t> h_rest;
   float4* fbuf = nullptr;
   int nfine = 0, fine_cap = 0;
   std::vector<int32_t> h_bt, h_all, h_leaves, h_rg, h_flist;
@@ -184,6 +186,14 @@ int upload_tables(shz_amr* a) {
   AMR_CUDA(a, cudaMemcpyAsync(a->d_all, a->h_all.data(), a->h_all.size() * sizeof(int32_t), cudaMemcpyHostToDevice, a->stream));
   AMR_CUDA(a, cudaMemcpyAsync(a->d_leaves, a->h_leaves.data(), a->h_leaves.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
                               a->stream));
+  // the blocks of the assemble's list with ghosts beyond a level change (the split assemble's rest)
+  const std::vector<int32_t>& asm_list = a->cfg.two_pass ? a->h_all : a->h_leaves;
+  shz::amr_rest_blocks(a->h_bt.data(), a->cfg.ndim, asm_list.data(), (int)asm_list.size(), a->h_rest);
+  if (!a->h_rest.empty())
+    AMR_CUDA(a, cudaMemcpyAsync(a->d_rest, a->h_rest.data(), a->h_rest.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                                a->stream));
+  a->L.rest = a->d_rest;
+  a->L.nrest = (int)a->h_rest.size();
   AMR_CUDA(a, cudaStreamSynchronize(a->stream));
   drop_graphs(a);
   return 0;
@@ -877,6 +887,7 @@ int shz_amr_create(const shz_amr_config* cfg, shz_amr** out) {
   ok = ok && cudaMalloc(&a->d_bt, cap * shz::amr::BT_STRIDE * sizeof(int)) == cudaSuccess;
   ok = ok && cudaMalloc(&a->d_all, cap * sizeof(int)) == cudaSuccess;
   ok = ok && cudaMalloc(&a->d_leaves, cap * sizeof(int)) == cudaSuccess;
+  ok = ok && cudaMalloc(&a->d_rest, cap * sizeof(int)) == cudaSuccess;
   ok = ok && cudaMalloc(&a->d_rg, cap * shz::amr::RG_STRIDE * sizeof(int)) == cudaSuccess;
   ok = ok && cudaMalloc(&a->d_flags, cap * sizeof(float)) == cudaSuccess;
   ok = ok && cudaMalloc(&a->clk, sizeof(shz::DevClock)) == cudaSuccess;
@@ -939,7 +950,7 @@ void shz_amr_destroy(shz_amr* a) {
   }
   void* bufs[] = {a->w1, a->w2, a->p1, a->p2, a->d_bt, a->d_all, a->d_leaves, a->d_rg, a->d_flags, a->d_gp,
                   a->clk, a->rates, a->diag_part, a->diag_out, a->d_ghost, a->d_flist, a->fbuf, a->d_err,
-                  a->d_bins[0], a->d_bins[1], a->d_brate, a->d_cyc, a->clk_save};
+                  a->d_bins[0], a->d_bins[1], a->d_brate, a->d_cyc, a->clk_save, a->d_rest};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (a->h_bins) cudaFreeHost(a->h_bins);

@@ -787,7 +787,7 @@ namespace {
 cudaError_t run_tuned(const tune::Key& k, const std::vector<tune::Choice>& cands, bool tune_now, cudaStream_t s,
                       const std::function<cudaError_t(const tune::Choice*)>& launch, long long* launches) {
   tune::Choice c;
-  if (tune::lookup(k, &c)) {
+  if (tune::pinned(k.kernel, &c) || tune::lookup(k, &c)) {
     *launches += 1;
     return launch(&c);
   }
@@ -813,6 +813,9 @@ cudaError_t amr_assemble_tuned(const AmrLaunch& L, const int* list, int n, const
   std::vector<tune::Choice> cands;
   for (int v : {0, 1, 2})
     for (int p : {4, 2, 8}) cands.push_back(mk(v, p));
+  // the split form (variants 3, 4): the plain pass, then the rest at 2 or 3 CTAs' register budget
+  for (int v : {3, 4})
+    for (int p : {2, 4}) cands.push_back(mk(v, p));
   return run_tuned(amr_tune_key(tune::K_AMR_ASSEMBLE, L, n), cands, tune_now, s,
                    [&](const tune::Choice* c) { return amr_launch_assemble(L, list, n, u1, u2, rates, rslot, s, c); },
                    launches);

@@ -59,6 +59,8 @@ struct Engine {
   float4* u2[2] = {nullptr, nullptr};
   float4 *w1 = nullptr, *w2 = nullptr;
   int *d_bt = nullptr, *d_list = nullptr, *d_glist = nullptr;
+  int* d_rest = nullptr;  // the split assemble's second-pass blocks (none on uniform grids' blocks)
+  std::vector<int32_t> h_rest;
   shz::KParams* d_gp = nullptr;
   shz::DevClock* d_clk = nullptr;
   unsigned* d_rates = nullptr;
@@ -159,6 +161,7 @@ int engine_init(shz_server* s, Engine& e, int ndim, double budget) {
   SV_CUDA(s, cudaMalloc(&e.d_bt, cap * 32 * sizeof(int)));
   SV_CUDA(s, cudaMalloc(&e.d_list, cap * sizeof(int)));
   SV_CUDA(s, cudaMalloc(&e.d_glist, cap * sizeof(int)));
+  SV_CUDA(s, cudaMalloc(&e.d_rest, cap * sizeof(int)));
   SV_CUDA(s, cudaMalloc(&e.d_gp, e.gmax * sizeof(shz::KParams)));
   SV_CUDA(s, cudaMalloc(&e.d_clk, e.gmax * sizeof(shz::DevClock)));
   SV_CUDA(s, cudaMalloc(&e.d_rates, 2 * e.gmax * sizeof(unsigned)));
@@ -195,7 +198,7 @@ void engine_free(Engine& e) {
     cudaFree(e.u1[p]);
     cudaFree(e.u2[p]);
   }
-  void* b[] = {e.w1, e.w2, e.d_err, e.d_bt, e.d_list, e.d_glist, e.d_gp, e.d_clk, e.d_rates, e.d_part, e.d_out};
+  void* b[] = {e.w1, e.w2, e.d_err, e.d_bt, e.d_list, e.d_glist, e.d_gp, e.d_clk, e.d_rates, e.d_part, e.d_out, e.d_rest};
   for (void* x : b)
     if (x) cudaFree(x);
   if (e.stream) cudaStreamDestroy(e.stream);
@@ -331,6 +334,11 @@ int rebuild(shz_server* s, Engine& e) {
     SV_CUDA(s, cudaMemcpyAsync(e.d_bt, e.h_bt.data(), (size_t)e.high * 32 * sizeof(int32_t), cudaMemcpyHostToDevice, e.stream));
   if (!e.h_list.empty())
     SV_CUDA(s, cudaMemcpyAsync(e.d_list, e.h_list.data(), e.h_list.size() * sizeof(int32_t), cudaMemcpyHostToDevice, e.stream));
+  shz::amr_rest_blocks(e.h_bt.data(), e.ndim, e.h_list.data(), (int)e.h_list.size(), e.h_rest);
+  if (!e.h_rest.empty())
+    SV_CUDA(s, cudaMemcpyAsync(e.d_rest, e.h_rest.data(), e.h_rest.size() * sizeof(int32_t), cudaMemcpyHostToDevice, e.stream));
+  e.L.rest = e.d_rest;
+  e.L.nrest = (int)e.h_rest.size();
   SV_CUDA(s, cudaStreamSynchronize(e.stream));
   drop_graphs(e);
   e.dirty = false;

@@ -42,6 +42,26 @@ int size_class(long long units) {
   return c;
 }
 
+namespace {
+Choice g_pin[K_COUNT];
+bool g_pinned[K_COUNT] = {};
+}  // namespace
+
+void pin(int kernel, const Choice* c) {
+  if (kernel < 0 || kernel >= K_COUNT) return;
+  std::lock_guard<std::mutex> lk(g_mu);
+  g_pinned[kernel] = c != nullptr;
+  if (c) g_pin[kernel] = *c;
+}
+
+bool pinned(int kernel, Choice* out) {
+  if (kernel < 0 || kernel >= K_COUNT) return false;
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!g_pinned[kernel]) return false;
+  *out = g_pin[kernel];
+  return true;
+}
+
 bool lookup(const Key& k, Choice* out) {
   if (!enabled()) return false;
   std::lock_guard<std::mutex> lk(g_mu);
@@ -114,6 +134,21 @@ int shz_tune_enable(int32_t on) {
 }
 
 void shz_tune_reset(void) { shz::tune::reset(); }
+
+int shz_tune_pin(int32_t kernel, int32_t variant, int32_t per_sm) {
+  if (kernel < 0 || kernel >= shz::tune::K_COUNT) return SHZ_E_CONFIG;
+  if (variant < 0) {
+    shz::tune::pin(kernel, nullptr);
+    return 0;
+  }
+  // the variants each kernel compiles (the assemble's 0-4; the others' 0)
+  if (variant > (kernel == shz::tune::K_AMR_ASSEMBLE ? 4 : 0) || per_sm < 0 || per_sm > 32) return SHZ_E_CONFIG;
+  shz::tune::Choice c;
+  c.variant = variant;
+  c.per_sm = per_sm;
+  shz::tune::pin(kernel, &c);
+  return 0;
+}
 
 int shz_tune_entries(shz_tune_entry* out, int32_t max, int32_t* n) {
   if (!n || max < 0 || (max > 0 && !out)) return SHZ_E_CONFIG;

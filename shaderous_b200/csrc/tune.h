@@ -53,6 +53,11 @@ int size_class(long long units);
 // The tuned choice for `k`, if any.
 bool lookup(const Key& k, Choice* out);
 
+// A choice pinned for every key of one kernel (a check that every candidate gives the same
+// state, or a fixed shape): the drivers use it instead of tuning. pin(kernel, nullptr) unpins.
+void pin(int kernel, const Choice* c);
+bool pinned(int kernel, Choice* out);
+
 // Whether `k` still needs tuning (the tuner is on and no choice is stored).
 bool needs(const Key& k);
 

@@ -24,6 +24,15 @@ def reset() -> None:
     _abi.load().shz_tune_reset()
 
 
+def pin(kernel: str, variant: int | None, per_sm: int = 0) -> None:
+    """Use this choice for every launch of an AMR kernel ("amr_assemble", "amr_sweep",
+    "amr_fine_flux") instead of the tuned one; ``variant=None`` unpins."""
+    k = {v: n for n, v in KERNELS.items()}[kernel]
+    rc = _abi.load().shz_tune_pin(k, -1 if variant is None else int(variant), int(per_sm))
+    if rc != 0:
+        raise ValueError(f"no choice {variant}, {per_sm} for {kernel}")
+
+
 def entries() -> list[dict]:
     """The tuned choices: key, choice, and the mean times of the choice and of the default."""
     lib = _abi.load()
