@@ -442,7 +442,6 @@ __global__ void __maxnreg__(80)
       }
       const float4* pj = ring(DIM == 3 ? j : 0);
       const bool zghost = DIM == 3 && (j == -1 || j == BS);
-      const int znb = j == -1 ? zlo_nb : zhi_nb;  // (meaningful on the z ghost planes)
 
       // the predictor at plane j
       float c[7];
