@@ -32,6 +32,15 @@ struct Tab {
   static constexpr int CPF = DIM == 3 ? 64 : 8;  // coarse cells per face
   static constexpr size_t BYTES = (size_t)2 * DIM * CPF * TAB_VALS * sizeof(float);
 };
+// The second pass's table of the edge and corner ghosts that reach a coarser leaf through a
+// same-level neighbour: 8 coarse cells along each of the 12 edges (a coarse cell spans 2 fine
+// texels along the edge and both ghost layers across it) and one per corner in 3D; one per corner
+// in 2D. Entries in the same layout as the face table's.
+template <int DIM>
+struct EdgeTab {
+  static constexpr int N = DIM == 3 ? 12 * (BS / 2) + 8 : 4;
+  static constexpr size_t BYTES = (size_t)N * TAB_VALS * sizeof(float);
+};
 
 __device__ __forceinline__ void tab_store(float* e, const Cons& uc, const Slopes& sl) {
   const float4 v[8] = {uc.a, uc.b, sl.s[0].a, sl.s[0].b, sl.s[1].a, sl.s[1].b, sl.s[2].a, sl.s[2].b};
@@ -92,6 +101,23 @@ __device__ __forceinline__ void shell_texel(int i, int* l) {
   }
 }
 
+// The neighbour direction of texel l: codes 0, 1, 2 per axis for below, inside and above the
+// block, d = x + 3 y + 9 z.
+template <int DIM>
+__device__ __forceinline__ int dir_code(const int* l) {
+  return (l[0] < 0 ? 0 : l[0] >= BS ? 2 : 1) + 3 * (l[1] < 0 ? 0 : l[1] >= BS ? 2 : 1) +
+         (DIM == 3 ? 9 * (l[2] < 0 ? 0 : l[2] >= BS ? 2 : 1) : 0);
+}
+
+// Edge-table entries of neighbour direction d (codes 0, 1, 2 per axis for below, inside and above
+// the block, d = x + 3 y + 9 z) when its ghosts reach a coarser leaf through another block: a 3D
+// edge (one axis inside) spans 8 coarse cells, a corner one.
+template <int DIM>
+__device__ __forceinline__ int edge_entries(int d) {
+  const int inside = (d % 3 == 1) + ((d / 3) % 3 == 1) + (DIM == 3 ? (d / 9 == 1) : 0);
+  return (DIM == 3 && inside == 1) ? BS / 2 : 1;
+}
+
 // A ghost whose source is a cell of a same-level leaf (not a parent, whose cells are restricted,
 // and not a leaf part way through a longer step, whose half step is read): one load gives it.
 template <bool BINS>
@@ -122,7 +148,11 @@ __global__ void __launch_bounds__(NT, MINB) amr_assemble(const KParams* __restri
   using T = Tab<DIM>;
   __shared__ float sRed[NT / 32];
   __shared__ unsigned sPlain;  // REST: bit d set when the ghosts of neighbour direction d are plain
+  __shared__ int sEdge[27];    // REST: first edge-table entry of direction d, or -1
+  __shared__ int sEdgeN;       // REST: edge-table entries of this block
   extern __shared__ __align__(16) float sTab[];
+  float* const sEdgeTab = sTab + (size_t)2 * DIM * T::CPF * TAB_VALS;  // REST and !per_texel only
+  constexpr bool EDGES = REST && !BINS;
   for (int i = blockIdx.x; i < n; i += gridDim.x) {
     float rmax = 0.f;
     const int slot = __ldg(list + i);
@@ -142,42 +172,81 @@ __global__ void __launch_bounds__(NT, MINB) amr_assemble(const KParams* __restri
       // axis into the block whatever its ghost layer), so one texel per direction decides.
       const int d = threadIdx.x;
       bool plain = false;
+      int cnt = 0;  // edge-table entries of direction d
       if (d < (DIM == 3 ? 27 : 9) && d != (DIM == 3 ? 13 : 4)) {
         const int l[3] = {d % 3 == 0 ? -1 : d % 3 == 2 ? BS : 0, (d / 3) % 3 == 0 ? -1 : (d / 3) % 3 == 2 ? BS : 0,
                           DIM == 3 ? (d / 9 == 0 ? -1 : d / 9 == 2 ? BS : 0) : 0};
-        plain = plain_src<BINS>(bt, bins, ghost_src_any<DIM>(bt, slot, l));
+        const Src sd = ghost_src_any<DIM>(bt, slot, l);
+        plain = plain_src<BINS>(bt, bins, sd);
+        // a coarser leaf reached through another block (an edge or corner direction): its coarse
+        // cells go into the edge table, 8 along a 3D edge, one at a corner
+        if (EDGES && !per_texel && sd.kind == 1 && sd.from != slot) cnt = edge_entries<DIM>(d);
       }
       const unsigned m = __ballot_sync(0xffffffffu, plain);
       if (d == 0) sPlain = m;
+      if (EDGES) {
+        int base = cnt;  // inclusive scan of the counts over the warp
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int v = __shfl_up_sync(0xffffffffu, base, o);
+          if (d >= o) base += v;
+        }
+        if (d < 27) sEdge[d] = cnt ? base - cnt : -1;
+        if (d == 31) sEdgeN = base;
+      }
     }
-    if (cmask) {
+    if (EDGES) __syncthreads();  // the edge directions, before their table is built
+    const int nedge = EDGES ? sEdgeN : 0;
+    if (cmask || nedge) {
       // the table of this block's coarse faces (the previous block's reads of it ended at the
-      // barriers of its rate maximum)
-      const int nf = __popc(cmask);
-      for (int idx = threadIdx.x; idx < nf * T::CPF; idx += NT) {
-        const int k = idx / T::CPF, c = idx % T::CPF;
-        unsigned mk = cmask;
-        for (int q = 0; q < k; q++) mk &= mk - 1;
-        const int f = __ffs(mk) - 1;
-        const int a = f >> 1;
-        int m[3] = {0, 0, 0};
-        m[a] = (f & 1) ? BS : -1;
-        if (DIM == 3) {
-          m[(a + 1) % 3] = 2 * (c % 8);
-          m[(a + 2) % 3] = 2 * (c / 8);
+      // barriers of its rate maximum), then the edge table's entries
+      const int nface = __popc(cmask) * T::CPF;
+      for (int idx = threadIdx.x; idx < nface + nedge; idx += NT) {
+        int from = slot, m[3] = {0, 0, 0}, cs;
+        float* dst;
+        if (idx < nface) {
+          const int k = idx / T::CPF, c = idx % T::CPF;
+          unsigned mk = cmask;
+          for (int q = 0; q < k; q++) mk &= mk - 1;
+          const int f = __ffs(mk) - 1;
+          const int a = f >> 1;
+          m[a] = (f & 1) ? BS : -1;
+          if (DIM == 3) {
+            m[(a + 1) % 3] = 2 * (c % 8);
+            m[(a + 2) % 3] = 2 * (c / 8);
+          } else {
+            m[1 - a] = 2 * c;
+          }
+          cs = bt_at(bt, slot, 20 + f);
+          dst = sTab + (size_t)(f * T::CPF + c) * TAB_VALS;
         } else {
-          m[1 - a] = 2 * c;
+          const int e = idx - nface;
+          int d = 0;
+          while (d < 26 && !(sEdge[d] >= 0 && e >= sEdge[d] && e < sEdge[d] + edge_entries<DIM>(d))) d++;
+          // the direction's representative texel, at the entry's coarse cell along a 3D edge
+          int l[3] = {d % 3 == 0 ? -1 : d % 3 == 2 ? BS : 0, (d / 3) % 3 == 0 ? -1 : (d / 3) % 3 == 2 ? BS : 0,
+                      DIM == 3 ? (d / 9 == 0 ? -1 : d / 9 == 2 ? BS : 0) : 0};
+          if (DIM == 3) {
+            const int c = d % 3 == 1 ? 0 : (d / 3) % 3 == 1 ? 1 : d / 9 == 1 ? 2 : -1;
+            if (c >= 0) l[c] = 2 * (e - sEdge[d]);
+          }
+          const Src se = ghost_src_any<DIM>(bt, slot, l);
+          from = se.from;
+          m[0] = se.l[0];
+          m[1] = se.l[1];
+          m[2] = se.l[2];
+          cs = se.slot;
+          dst = sEdgeTab + (size_t)e * TAB_VALS;
         }
         Cons uc;
         Slopes sl;
         int par[3];
-        const int cs = bt_at(bt, slot, 20 + f);
-        if (BINS && mid_block(bt, bins, cs)) coarse_cell_mid<DIM, R>(P, bt, p1, p2, nr, slot, m, cs, uc, sl, par);
-        else coarse_cell<DIM, R>(bt, u1, u2, nr, slot, m, cs, P.rho_floor, uc, sl, par);
-        tab_store(sTab + (size_t)(f * T::CPF + c) * TAB_VALS, uc, sl);
+        if (BINS && mid_block(bt, bins, cs)) coarse_cell_mid<DIM, R>(P, bt, p1, p2, nr, from, m, cs, uc, sl, par);
+        else coarse_cell<DIM, R>(bt, u1, u2, nr, from, m, cs, P.rho_floor, uc, sl, par);
+        tab_store(dst, uc, sl);
       }
     }
-    if (cmask || REST) __syncthreads();
+    if (cmask || REST) __syncthreads();  // (REST: also the edge table)
     // the block's own cells (a parent's restricted from its children), with the rate maximum
 #pragma unroll 4
     for (int t = threadIdx.x; t < (REST ? 0 : BG<DIM>::CB); t += NT) {
@@ -194,27 +263,33 @@ __global__ void __launch_bounds__(NT, MINB) amr_assemble(const KParams* __restri
     for (int i = threadIdx.x; i < BG<DIM>::WN - BG<DIM>::CB; i += NT) {
       int l[3];
       shell_texel<DIM>(i, l);
-      if (REST) {
-        const int d = (l[0] < 0 ? 0 : l[0] >= BS ? 2 : 1) + 3 * (l[1] < 0 ? 0 : l[1] >= BS ? 2 : 1) +
-                      (DIM == 3 ? 9 * (l[2] < 0 ? 0 : l[2] >= BS ? 2 : 1) : 0);
-        if ((sPlain >> d) & 1u) continue;
-      }
+      if (REST && ((sPlain >> dir_code<DIM>(l)) & 1u)) continue;
       const Src s = ghost_src_any<DIM>(bt, slot, l);
       Cons u;
       if (s.kind == 0) {
         if (BINS && mid_block(bt, bins, s.slot)) u = mid_cons<DIM>(P, p1, p2, s.slot, s.l);
         else u = u_at<DIM>(bt, u1, u2, s.slot, s.l);
-      } else if (cmask && s.from == slot) {
-        // a ghost of this block's own coarse face: its coarse cell from the table
-        int a = 0;
+      } else if ((cmask && s.from == slot) || (EDGES && nedge && sEdge[dir_code<DIM>(l)] >= 0)) {
+        // a ghost beyond a coarser leaf whose coarse cell is in a table: this block's own coarse
+        // face's, or (an edge or corner ghost reached through another block) the edge table's
+        const float* ent;
+        if (cmask && s.from == slot) {
+          int a = 0;
 #pragma unroll
-        for (int q = 0; q < DIM; q++)
-          if (s.l[q] < 0 || s.l[q] >= BS) a = q;
-        const int f = 2 * a + (s.l[a] >= BS ? 1 : 0);
-        const int c = DIM == 3 ? (s.l[(a + 1) % 3] >> 1) + 8 * (s.l[(a + 2) % 3] >> 1) : (s.l[1 - a] >> 1);
+          for (int q = 0; q < DIM; q++)
+            if (s.l[q] < 0 || s.l[q] >= BS) a = q;
+          const int f = 2 * a + (s.l[a] >= BS ? 1 : 0);
+          const int c = DIM == 3 ? (s.l[(a + 1) % 3] >> 1) + 8 * (s.l[(a + 2) % 3] >> 1) : (s.l[1 - a] >> 1);
+          ent = sTab + (size_t)(f * T::CPF + c) * TAB_VALS;
+        } else {
+          // along a 3D edge, the coarse cell under the texel's position on the axis inside
+          const int d = dir_code<DIM>(l);
+          const int in = DIM == 3 ? (d % 3 == 1 ? l[0] : (d / 3) % 3 == 1 ? l[1] : d / 9 == 1 ? l[2] : 0) : 0;
+          ent = sEdgeTab + (size_t)(sEdge[d] + (in >> 1)) * TAB_VALS;
+        }
         Cons uc;
         Slopes sl;
-        tab_load(sTab + (size_t)(f * T::CPF + c) * TAB_VALS, uc, sl);
+        tab_load(ent, uc, sl);
         const int par[3] = {s.l[0] & 1, s.l[1] & 1, DIM == 3 ? (s.l[2] & 1) : 0};
         u = prolong_child(uc, sl, par);
       } else if (BINS && mid_block(bt, bins, s.slot)) {
@@ -580,11 +655,12 @@ template <int DIM, int R, int MINB, bool BINS = false, bool REST = false>
 cudaError_t assemble_t(const AmrLaunch& L, int g, const int* list, int n, const float4* u1, const float4* u2,
                        unsigned* rates, int rslot, cudaStream_t s, const int* bins = nullptr, float* brate = nullptr) {
   auto k = amrk::amr_assemble<DIM, R, MINB, BINS, REST>;
+  // the coarse-face table, and in the second pass of the split form also the edge table
+  constexpr size_t TB = amrk::Tab<DIM>::BYTES + (REST && !BINS ? amrk::EdgeTab<DIM>::BYTES : 0);
   // (set once per instantiation; not a stream operation)
-  static const cudaError_t attr =
-      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)amrk::Tab<DIM>::BYTES);
+  static const cudaError_t attr = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TB);
   if (attr != cudaSuccess) return attr;
-  const size_t smem = L.per_texel ? 0 : amrk::Tab<DIM>::BYTES;
+  const size_t smem = L.per_texel ? 0 : TB;
   k<<<g, amrk::NT, smem, s>>>(L.gp, L.bt, list, n, u1, u2, L.w1, L.w2, rates, rslot, L.per_texel ? 1 : 0, L.p1, L.p2,
                               bins, brate);
   return cudaGetLastError();
