@@ -459,7 +459,9 @@ const char* shz_version(void);
  *     pass for the blocks' own cells and same-level ghosts, then the ghosts beyond a level
  *     change over only the blocks that have them; per_sm = CTAs of the work-list grid per SM;
  *   2 AMR fused sweep: per_sm;
- *   3 AMR fine-flux pass: per_sm.
+ *   3 AMR fine-flux pass: per_sm;
+ *   4 the per-block-timestep substeps' assemble: variant 1 one pass, 3 the split form (its
+ *     second pass over every block of the substep's list); per_sm.
  */
 typedef struct shz_tune_entry {
   int32_t kernel, ndim, recon, isentropic, size_class;  /* the key; size class = floor(log2 units) */
@@ -469,7 +471,7 @@ typedef struct shz_tune_entry {
 } shz_tune_entry;
 /* Turn the tuner on (default) or off (every launch takes the default shape). Process-wide. */
 int shz_tune_enable(int32_t on);
-/* Pin one AMR kernel's choice (kernel 1-3 above; variant, per_sm with 0 for the default grid)
+/* Pin one AMR kernel's choice (kernel 1-4 above; variant, per_sm with 0 for the default grid)
  * for every key, used instead of the tuned one; variant < 0 unpins. Process-wide. */
 int shz_tune_pin(int32_t kernel, int32_t variant, int32_t per_sm);
 /* Forget every choice. */

@@ -152,7 +152,7 @@ __global__ void __launch_bounds__(NT, MINB) amr_assemble(const KParams* __restri
   __shared__ int sEdgeN;       // REST: edge-table entries of this block
   extern __shared__ __align__(16) float sTab[];
   float* const sEdgeTab = sTab + (size_t)2 * DIM * T::CPF * TAB_VALS;  // REST and !per_texel only
-  constexpr bool EDGES = REST && !BINS;
+  constexpr bool EDGES = REST;
   for (int i = blockIdx.x; i < n; i += gridDim.x) {
     float rmax = 0.f;
     const int slot = __ldg(list + i);
@@ -656,7 +656,7 @@ cudaError_t assemble_t(const AmrLaunch& L, int g, const int* list, int n, const 
                        unsigned* rates, int rslot, cudaStream_t s, const int* bins = nullptr, float* brate = nullptr) {
   auto k = amrk::amr_assemble<DIM, R, MINB, BINS, REST>;
   // the coarse-face table, and in the second pass of the split form also the edge table
-  constexpr size_t TB = amrk::Tab<DIM>::BYTES + (REST && !BINS ? amrk::EdgeTab<DIM>::BYTES : 0);
+  constexpr size_t TB = amrk::Tab<DIM>::BYTES + (REST ? amrk::EdgeTab<DIM>::BYTES : 0);
   // (set once per instantiation; not a stream operation)
   static const cudaError_t attr = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TB);
   if (attr != cudaSuccess) return attr;
@@ -776,9 +776,23 @@ void amr_rest_blocks(const int32_t* bt, int ndim, const int32_t* list, int n, st
 }
 
 cudaError_t amr_launch_assemble_bins(const AmrLaunch& L, const int* list, int n, const float4* u1, const float4* u2,
-                                     const int* bins, unsigned* rates, int rslot, float* brate, cudaStream_t s) {
+                                     const int* bins, unsigned* rates, int rslot, float* brate, cudaStream_t s,
+                                     const tune::Choice* c) {
   if (n <= 0) return cudaSuccess;
-  const int g = grid_for(n, 4);
+  const int per_sm = c && c->per_sm > 0 ? c->per_sm : 4;
+  const int g = grid_for(n, per_sm);
+  if (c && c->variant == 3) {
+    // the split form; its second pass walks the whole list, since which neighbours are part way
+    // through their step changes from substep to substep
+    cudaError_t e = assemble_plain<true>(L, list, n, u1, u2, rates, rslot, s, bins, brate);
+    if (e != cudaSuccess) return e;
+    if (L.ndim == 3) {
+      SHZ_RECON_SWITCH(L.recon, false, return (assemble_t<3, R, 2, true, true>(L, g, list, n, u1, u2, rates, rslot, s, bins, brate)))
+    } else {
+      SHZ_RECON_SWITCH(L.recon, false, return (assemble_t<2, R, 2, true, true>(L, g, list, n, u1, u2, rates, rslot, s, bins, brate)))
+    }
+    return cudaSuccess;
+  }
   if (L.ndim == 3) {
     SHZ_RECON_SWITCH(L.recon, false, return (assemble_t<3, R, 2, true>(L, g, list, n, u1, u2, rates, rslot, s, bins, brate)))
   } else {

@@ -68,8 +68,16 @@ cudaError_t amr_launch_update(const AmrLaunch& L, const int* list, int n, const 
 // The assemble of the blocks in list for a substep: as amr_launch_assemble's per-texel form, with
 // the ghosts of neighbours part way through a longer step taken from their half-step atlas; each
 // leaf's own rate / dx also goes to brate[slot] (if not null).
+// c: the launch shape (null: the one-pass kernel, 4 CTAs per SM; variant 3: the split form).
 cudaError_t amr_launch_assemble_bins(const AmrLaunch& L, const int* list, int n, const float4* u1, const float4* u2,
-                                     const int* bins, unsigned* rates, int rslot, float* brate, cudaStream_t s);
+                                     const int* bins, unsigned* rates, int rslot, float* brate, cudaStream_t s,
+                                     const tune::Choice* c = nullptr);
+// The same with the tuned shape (kernel K_AMR_ASSEMBLE_BINS), tuned in place on its first call for
+// a key (these substep launches are eager); *extra grows by the kernels launched beyond the one
+// the caller counts (the split form's second pass, the tuning launches).
+cudaError_t amr_assemble_bins_tuned(const AmrLaunch& L, const int* list, int n, const float4* u1, const float4* u2,
+                                    const int* bins, unsigned* rates, int rslot, float* brate, cudaStream_t s,
+                                    long long* extra);
 // The bins of a cycle over the blocks in list (all of them): the first guess from each leaf's rate
 // and the clock's dt into `a`, then the dilation sweep into `b` and `sweeps` (odd) relaxation
 // sweeps alternating b -> a, a -> b, ..., so that the result is in `a`.

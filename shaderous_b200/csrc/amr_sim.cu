@@ -379,7 +379,7 @@ int cycle_two(shz_amr* a) {
   const int na = n_all(a), nl = n_leaves(a);
   unsigned* scratch = a->rates + 4;  // the later substeps' assembles: rates nothing reads
   AMR_CUDA(a, shz::amr_launch_bins_tick(a->clk, A, 0, a->stream));
-  AMR_CUDA(a, shz::amr_launch_assemble_bins(a->L, a->d_all, na, u1, u2, A, a->rates, a->slot, a->d_brate, a->stream));
+  AMR_CUDA(a, shz::amr_assemble_bins_tuned(a->L, a->d_all, na, u1, u2, A, a->rates, a->slot, a->d_brate, a->stream, &a->launches));
   AMR_CUDA(a, shz::launch_clock_multi(a->clk, a->rates, a->slot, 1, a->stream, n));
   const int sweeps = (K + a->cfg.max_level + 2) | 1;
   AMR_CUDA(a, shz::amr_launch_bins(a->L, a->d_all, na, a->d_brate, a->clk, (float)a->cfg.hydro.cfl, K, sweeps, A, B,
@@ -442,7 +442,7 @@ int cycle_two(shz_amr* a) {
     const int* ll = la + na;
     const int* lu = ll + nl;
     AMR_CUDA(a, shz::amr_launch_bins_tick(a->clk, A, sub, a->stream));
-    AMR_CUDA(a, shz::amr_launch_assemble_bins(a->L, la, rec[0], u1, u2, A, scratch, 0, nullptr, a->stream));
+    AMR_CUDA(a, shz::amr_assemble_bins_tuned(a->L, la, rec[0], u1, u2, A, scratch, 0, nullptr, a->stream, &a->launches));
     AMR_CUDA(a, shz::amr_launch_predict(a->L, ll, rec[1], a->clk, a->stream, A));
     AMR_CUDA(a, shz::amr_launch_update(a->L, lu, rec[2], u1, u2, u1, u2, a->clk, a->stream, A));
     a->launches += 1 + (rec[0] > 0) + (rec[1] > 0) + (rec[2] > 0);
@@ -488,7 +488,7 @@ int cycle_fused(shz_amr* a) {
   const int na = n_all(a), nl = n_leaves(a), cap = a->cfg.cap;
   unsigned* scratch = a->rates + 4;
   AMR_CUDA(a, shz::amr_launch_bins_tick(a->clk, A, 0, a->stream));
-  AMR_CUDA(a, shz::amr_launch_assemble_bins(a->L, a->d_leaves, nl, u1, u2, A, a->rates, a->slot, a->d_brate, a->stream));
+  AMR_CUDA(a, shz::amr_assemble_bins_tuned(a->L, a->d_leaves, nl, u1, u2, A, a->rates, a->slot, a->d_brate, a->stream, &a->launches));
   AMR_CUDA(a, shz::launch_clock_multi(a->clk, a->rates, a->slot, 1, a->stream, n));
   const int sweeps = (K + a->cfg.max_level + 2) | 1;
   AMR_CUDA(a, shz::amr_launch_bins(a->L, a->d_all, na, a->d_brate, a->clk, (float)a->cfg.hydro.cfl, K, sweeps, A, B,
@@ -579,7 +579,7 @@ int cycle_fused(shz_amr* a) {
     L.fbase = a->d_cyc + q.fb;
     if (sub > 0) {
       AMR_CUDA(a, shz::amr_launch_bins_tick(a->clk, A, sub, a->stream));
-      AMR_CUDA(a, shz::amr_launch_assemble_bins(L, ll, q.nll, u1, u2, A, scratch, 0, nullptr, a->stream));
+      AMR_CUDA(a, shz::amr_assemble_bins_tuned(L, ll, q.nll, u1, u2, A, scratch, 0, nullptr, a->stream, &a->launches));
       a->launches += 1 + (q.nll > 0);
     }
     AMR_CUDA(a, shz::amr_launch_fine_flux(L, a->d_cyc + q.e, q.ne, a->clk, a->stream));

@@ -778,7 +778,7 @@ cudaError_t amr_launch_sweep(const AmrLaunch& L, const int* list, int n, const f
 namespace shz {
 
 tune::Key amr_tune_key(int kernel, const AmrLaunch& L, long long units) {
-  const int isen = (kernel == tune::K_AMR_ASSEMBLE) ? 0 : (L.isen ? 1 : 0);
+  const int isen = (kernel == tune::K_AMR_ASSEMBLE || kernel == tune::K_AMR_ASSEMBLE_BINS) ? 0 : (L.isen ? 1 : 0);
   return tune::Key{kernel, L.ndim, L.recon, isen, tune::size_class(units)};
 }
 
@@ -815,9 +815,31 @@ cudaError_t amr_assemble_tuned(const AmrLaunch& L, const int* list, int n, const
   // the split form (variants 3, 4): the plain pass, then the rest at 2 or 3 CTAs' register budget
   for (int v : {3, 4})
     for (int p : {2, 4}) cands.push_back(mk(v, p));
-  return run_tuned(amr_tune_key(tune::K_AMR_ASSEMBLE, L, n), cands, tune_now, s,
-                   [&](const tune::Choice* c) { return amr_launch_assemble(L, list, n, u1, u2, rates, rslot, s, c); },
-                   launches);
+  long long second = 0;  // the split form's second kernels (when the host listed blocks for them)
+  const cudaError_t e = run_tuned(amr_tune_key(tune::K_AMR_ASSEMBLE, L, n), cands, tune_now, s,
+                                  [&](const tune::Choice* c) {
+                                    if (c && c->variant >= 3 && L.nrest != 0) second++;
+                                    return amr_launch_assemble(L, list, n, u1, u2, rates, rslot, s, c);
+                                  },
+                                  launches);
+  *launches += second;
+  return e;
+}
+
+cudaError_t amr_assemble_bins_tuned(const AmrLaunch& L, const int* list, int n, const float4* u1, const float4* u2,
+                                    const int* bins, unsigned* rates, int rslot, float* brate, cudaStream_t s,
+                                    long long* extra) {
+  if (n <= 0) return cudaSuccess;
+  const std::vector<tune::Choice> cands = {mk(1, 4), mk(3, 4), mk(3, 2)};
+  long long launched = 0, second = 0;
+  const cudaError_t e = run_tuned(amr_tune_key(tune::K_AMR_ASSEMBLE_BINS, L, n), cands, true, s,
+                                  [&](const tune::Choice* c) {
+                                    if (c && c->variant == 3) second++;
+                                    return amr_launch_assemble_bins(L, list, n, u1, u2, bins, rates, rslot, brate, s, c);
+                                  },
+                                  &launched);
+  *extra += launched - 1 + second;
+  return e;
 }
 
 cudaError_t amr_fine_flux_tuned(const AmrLaunch& L, const int* flist, int nf, const DevClock* clks, cudaStream_t s,

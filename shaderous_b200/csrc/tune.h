@@ -20,7 +20,8 @@ enum Kernel : int {
   K_AMR_ASSEMBLE = 1,   // variant: register budget (CTAs per SM the compiler plans for); per_sm: grid
   K_AMR_SWEEP = 2,      // per_sm: grid
   K_AMR_FINE_FLUX = 3,  // per_sm: grid
-  K_COUNT = 4
+  K_AMR_ASSEMBLE_BINS = 4,  // the per-block-timestep substeps' assemble: variant 1 one pass, 3 split
+  K_COUNT = 5
 };
 
 struct Key {

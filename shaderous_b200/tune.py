@@ -11,7 +11,7 @@ import ctypes as C
 
 from . import _abi
 
-KERNELS = {0: "uniform_sweep", 1: "amr_assemble", 2: "amr_sweep", 3: "amr_fine_flux"}
+KERNELS = {0: "uniform_sweep", 1: "amr_assemble", 2: "amr_sweep", 3: "amr_fine_flux", 4: "amr_assemble_bins"}
 
 
 def enable(on: bool = True) -> None:
