@@ -67,6 +67,9 @@ def parse():
     ap.add_argument("--amr-cap", type=int, default=26000, help="block slots of the AMR runs")
     ap.add_argument("--profile-window", action="store_true",
                     help="AMR section: bracket one step after the warm-up with cudaProfilerStart/Stop")
+    ap.add_argument("--pin-assemble", type=int, default=None, metavar="V",
+                    help="AMR section: fix the assemble's launch shape to variant V (0-2 one pass, 3-4 split) "
+                         "instead of the tuned one, e.g. to profile one form")
     ap.add_argument("--slabs", action="store_true",
                     help="the z-slab driver also at N = 1 (one periodic slab exchanging with itself)")
     return ap.parse_args()
@@ -503,6 +506,10 @@ def main():
         return
     if args.section != "all":
         out = {}
+        if args.section == "amr" and args.pin_assemble is not None:
+            from shaderous_b200 import tune
+
+            tune.pin("amr_assemble", args.pin_assemble, 2)
         if args.section == "amr":
             if args.amr_variant in ("both", "spec"):
                 out["spec"] = amr_sedov(steps=max(args.steps, 8), cap=args.amr_cap, profile_window=args.profile_window)
