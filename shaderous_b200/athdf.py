@@ -73,23 +73,27 @@ def max_level(s: Snapshot) -> int:
     return int(max((int(v) for v in s.levels), default=0))
 
 
-def primitives_from(gamma: float, u1: np.ndarray, u2: np.ndarray) -> dict:
+def primitives_from(gamma: float, u1: np.ndarray, u2: np.ndarray, chunk: int = 1 << 22) -> dict:
     """Primitive variables from interleaved conserved state (snapshot.ts:121-137): the pressure
     from the ideal-gas equation of state on the stored internal energy, (gamma - 1) e_int
-    (eos.ts:398-400), each value formed in float64 and stored as float32."""
-    u1 = np.asarray(u1, np.float32).reshape(-1, 4).astype(np.float64)
-    u2 = np.asarray(u2, np.float32).reshape(-1, 4).astype(np.float64)
-    rho = u1[:, 0]
-    with np.errstate(divide="ignore", invalid="ignore"):
-        out = {
-            "rho": rho,
-            "press": (gamma - 1) * u2[:, 1],
-            "vel1": u1[:, 1] / rho,
-            "vel2": u1[:, 2] / rho,
-            "vel3": u1[:, 3] / rho,
-            "r0": u2[:, 2] / rho,
-        }
-    return {k: np.ascontiguousarray(v, dtype=np.float32) for k, v in out.items()}
+    (eos.ts:398-400), each value formed in float64 and stored as float32. The cells are taken
+    `chunk` at a time, so the float64 work arrays stay small for a state of billions of cells."""
+    u1 = np.asarray(u1, np.float32).reshape(-1, 4)
+    u2 = np.asarray(u2, np.float32).reshape(-1, 4)
+    n = u1.shape[0]
+    out = {k: np.empty(n, np.float32) for k in VARIABLES}
+    for i in range(0, n, max(1, int(chunk))):
+        a = u1[i:i + chunk].astype(np.float64)
+        b = u2[i:i + chunk].astype(np.float64)
+        rho = a[:, 0]
+        with np.errstate(divide="ignore", invalid="ignore"):
+            out["rho"][i:i + chunk] = rho
+            out["press"][i:i + chunk] = (gamma - 1) * b[:, 1]
+            out["vel1"][i:i + chunk] = a[:, 1] / rho
+            out["vel2"][i:i + chunk] = a[:, 2] / rho
+            out["vel3"][i:i + chunk] = a[:, 3] / rho
+            out["r0"][i:i + chunk] = b[:, 2] / rho
+    return out
 
 
 def _swap_axes23(s: Snapshot, to_file: bool) -> Snapshot:

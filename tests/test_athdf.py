@@ -226,3 +226,21 @@ def test_file_round_trip_through_a_path(tmp_path):
         assert np.array_equal(r.read("press", 1, 3), s.data["press"][16:48])
         # block 0, cells z 0, y [1, 3), x [2, 4)
         assert r.read_slab("rho", 0, [0, 1], [1, 3], [2, 4]).tolist() == [6.25, 7.25, 10.25, 11.25]
+
+
+def test_primitives_in_chunks_equal_the_whole():
+    """The primitives of a state taken a chunk of cells at a time are those formed all at once, and
+    each is the float32 rounding of the float64 value (snapshot.ts primitivesFrom)."""
+    from shaderous_b200.athdf import primitives_from
+
+    rng = np.random.default_rng(3)
+    n = 10007
+    u1 = np.column_stack([rng.uniform(0.1, 3, n), rng.normal(size=(n, 3))]).astype(np.float32)
+    u2 = np.column_stack([rng.uniform(1, 5, n), rng.uniform(0.5, 2, n), rng.uniform(0, 1, n), np.zeros(n)]).astype(np.float32)
+    whole = primitives_from(1.4, u1, u2, chunk=n)
+    parts = primitives_from(1.4, u1, u2, chunk=1000)
+    for k in VARIABLES:
+        assert parts[k].dtype == np.float32 and np.array_equal(parts[k], whole[k])
+    rho = u1[:, 0].astype(np.float64)
+    assert np.array_equal(whole["vel2"], (u1[:, 2].astype(np.float64) / rho).astype(np.float32))
+    assert np.array_equal(whole["press"], (0.4 * u2[:, 1].astype(np.float64)).astype(np.float32))
