@@ -65,9 +65,10 @@ cudaError_t amr_launch_predict(const AmrLaunch& L, const int* list, int n, const
 cudaError_t amr_launch_update(const AmrLaunch& L, const int* list, int n, const float4* u1, const float4* u2, float4* o1,
                               float4* o2, const DevClock* clks, cudaStream_t s, const int* bins = nullptr);
 // Per-block timesteps (amr_bins.cu).
-// The assemble of the blocks in list for a substep: as amr_launch_assemble's per-texel form, with
-// the ghosts of neighbours part way through a longer step taken from their half-step atlas; each
-// leaf's own rate / dx also goes to brate[slot] (if not null).
+// The assemble of the blocks in list for a substep: as amr_launch_assemble (coarse ghosts from the
+// block's tables, or each formed by itself in the two-pass form), with the ghosts of neighbours
+// part way through a longer step taken from their half-step atlas; each leaf's own rate / dx also
+// goes to brate[slot] (if not null).
 // c: the launch shape (null: the one-pass kernel, 4 CTAs per SM; variant 3: the split form).
 cudaError_t amr_launch_assemble_bins(const AmrLaunch& L, const int* list, int n, const float4* u1, const float4* u2,
                                      const int* bins, unsigned* rates, int rslot, float* brate, cudaStream_t s,
