@@ -130,7 +130,7 @@ def amr_sedov(levels=4, nr=8, radius_cells=3.5, steps=24, cap=26000, grown=False
             "note": "time includes the refinement checks (flag, host adapt, regrid) every 8 steps"}
 
 
-# The reference's published throughputs (WebGPU, zone-updates/s) for the same
+# The reference's published throughputs (WebGPU in Chrome, zone-updates/s) for the same
 # configurations, for context: other hardware and another implementation.
 PUBLISHED = {
     "kh_2d_1024": {"H200 NVL": 2.339e9, "RTX 3080": 1.633e9},
@@ -351,19 +351,34 @@ def cpu_extra() -> list:
     return out
 
 
+def tgv_prims(n: int) -> np.ndarray:
+    """The Taylor-Green initial primitives (rho, vx, vy, vz, p, s) at the cell centres of an n^3
+    grid on [0, 2 pi]^3, x fastest: rho = 1, p = 100, u = sin x cos y cos z, v = -cos x sin y cos z,
+    w = 0. Built here with numpy alone (cell centres at (i + 1/2) 2 pi / n, the reference's
+    cell-centre rule, src/reference/hydro.ts:195-214), so the reference arm loads no product code."""
+    c = (np.arange(n) + 0.5) * (2 * math.pi / n)
+    sx, cx = np.sin(c), np.cos(c)
+    w = np.zeros((n, n, n, 6))  # [z][y][x]
+    w[..., 0] = 1.0
+    w[..., 1] = sx[None, None, :] * cx[None, :, None] * cx[:, None, None]
+    w[..., 2] = -cx[None, None, :] * sx[None, :, None] * cx[:, None, None]
+    w[..., 4] = 100.0
+    return w.reshape(-1, 6)
+
+
 def run_reference(args, rank, world):
-    """The reference arm: the CPU oracle on the host's cores, one bounded sample step per bench step."""
+    """The reference arm: the CPU oracle on the host's cores, one bounded sample step per bench
+    step. It imports only the oracle and numpy (no product library is loaded in this process)."""
     if rank != 0:
         return
     from oracle.oracle import RefHydro
-    from shaderous_b200 import problem_prims
 
     n = 128
-    cfg, prob = workload(n, args.recon)
     threads = os.cpu_count() or 1
-    h = RefHydro(n=cfg.n, dx=cfg.dx, gamma=cfg.gamma, bc_lo=(0, 0, 0), bc_hi=(0, 0, 0), cfl=cfg.cfl,
-                 limiter=args.recon, isentropic=cfg.isentropic and args.recon != "ppm", threads=threads)
-    h.init_prims(problem_prims(cfg, prob))
+    recon = args.recon
+    h = RefHydro(n=(n, n, n), dx=2 * math.pi / n, gamma=5 / 3, bc_lo=(0, 0, 0), bc_hi=(0, 0, 0), cfl=0.4,
+                 limiter=recon, isentropic=recon != "ppm", threads=threads)
+    h.init_prims(tgv_prims(n))
     for _ in range(args.warmup):
         h.step()
     t0 = time.perf_counter()
@@ -371,14 +386,15 @@ def run_reference(args, rank, world):
         h.step()
     dt = time.perf_counter() - t0
     v = n ** 3 * args.steps / dt
-    sample = (f"TGV {n}^3 {args.recon.upper()}+HLLC per step (bounded sample of the {args.n}^3 workload), float64 "
+    sample = (f"TGV {n}^3 {recon.upper()}+HLLC per step (bounded sample of the {args.n}^3 workload), float64 "
               f"C++ oracle ported from src/reference/hydro.ts (the TypeScript original has no runtime here), "
               f"{threads} threads")
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000 * dt / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"taylor-green {args.n}^3 periodic, {args.recon}+hllc, cfl 0.4",
-                       "sample_cells": n ** 3},
+            "config": {"workload": f"taylor-green {n}^3 periodic (a bounded sample of the {args.n}^3 workload: the "
+                                   f"float64 oracle at {args.n}^3 needs tens of GB), {recon}+hllc, cfl 0.4",
+                       "sample_cells": n ** 3, "workload_cells": args.n ** 3},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)

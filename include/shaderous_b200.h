@@ -506,10 +506,14 @@ int shz_tune_entries(shz_tune_entry* out, int32_t max, int32_t* n);
  *         work is enqueued, and `out` is ready when the stream reaches it.
  *
  * The first call on a device looks up the array's device address (cudaGetSymbolAddress) with
- * that device current; make that first call before any stream capture. All calls share the one
- * array: calls whose work overlaps on the GPU race on it, so serialise them (one stream, or
- * events between streams). Each call overwrites every row it reads, so nothing left by an
- * earlier call matters. On failure, shz_totals_noalloc_error() gives the message.
+ * that device current; make that first call before any stream capture. The address is kept per
+ * device together with the id of the context it was found in: after a device reset
+ * (cudaDeviceReset) the next call finds the new context and looks the address up again. The call
+ * makes `device` current for its own work and puts the caller's current device back before it
+ * returns. All calls share the one array: calls whose work overlaps on the GPU race on it, so
+ * serialise them (one stream, or events between streams). Each call overwrites every row it
+ * reads, so nothing left by an earlier call matters. On failure, shz_totals_noalloc_error() gives
+ * the message of the calling thread's last failure.
  */
 #define SHZ_DIAG_VALUES 9
 #define SHZ_TOTALS_MAX_BLOCKS 8192

@@ -78,11 +78,14 @@ def primitives_from(gamma: float, u1: np.ndarray, u2: np.ndarray, chunk: int = 1
     from the ideal-gas equation of state on the stored internal energy, (gamma - 1) e_int
     (eos.ts:398-400), each value formed in float64 and stored as float32. The cells are taken
     `chunk` at a time, so the float64 work arrays stay small for a state of billions of cells."""
+    chunk = int(chunk)
+    if chunk < 1:
+        raise ValueError(f"chunk must be at least 1 cell, got {chunk}")
     u1 = np.asarray(u1, np.float32).reshape(-1, 4)
     u2 = np.asarray(u2, np.float32).reshape(-1, 4)
     n = u1.shape[0]
     out = {k: np.empty(n, np.float32) for k in VARIABLES}
-    for i in range(0, n, max(1, int(chunk))):
+    for i in range(0, n, chunk):
         a = u1[i:i + chunk].astype(np.float64)
         b = u2[i:i + chunk].astype(np.float64)
         rho = a[:, 0]

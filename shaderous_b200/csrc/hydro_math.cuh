@@ -18,7 +18,7 @@ struct KParams {
   float rho_floor, p_floor, e_floor;
   float eta_dual, shock_thresh, signal;
   int hll;
-  float dv;  // cell volume dx^ndim (diagnostics)
+  double dv;  // cell volume dx^ndim in float64 (the float64 totals are scaled by it)
 };
 
 // The clock on the device (the reference's Clock, src/hydro/common.wgsl:84-96), advanced by

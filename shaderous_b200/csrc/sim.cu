@@ -87,7 +87,7 @@ struct DeviceScope {
   }
 };
 
-int ndim_of(const shz_config& c) { return c.n[2] > 1 ? 3 : (c.n[1] > 1 ? 2 : 1); }
+int ndim_of(const shz_config& c) { return shz::ndim_of_size(c.n); }
 // Ghost planes a halo face stores: the z march reads 1 + 2 planes beyond the slab with PPM's
 // five-cell stencil, 1 + 1 with the three-cell limiters.
 int halo_planes(const shz_config& c) { return c.recon == SHZ_RECON_PPM ? 3 : 2; }
@@ -144,7 +144,7 @@ void fill_kparams(shz_sim* s) {
   k.shock_thresh = (float)c.shock_thresh;
   k.signal = (float)c.signal_dims;
   k.hll = c.riemann == SHZ_RIEMANN_HLL ? 1 : 0;
-  k.dv = (float)std::pow(c.dx, s->ndim);
+  k.dv = std::pow(c.dx, s->ndim);
 }
 
 int write_clock(shz_sim* s, double t, long long steps) {

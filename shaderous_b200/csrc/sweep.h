@@ -11,6 +11,9 @@ namespace shz {
 
 constexpr int DIAG_VALUES = 9;  // mass, momentum x3, e_kin, e_int, e_tot, floored, max Mach
 
+// A grid's dimensionality from its size: the highest axis with more than one cell.
+inline int ndim_of_size(const int n[3]) { return n[2] > 1 ? 3 : (n[1] > 1 ? 2 : 1); }
+
 // Tensor maps of one parity of a 3D state, for the sweep's TMA staging of its planes.
 struct SweepMaps {
   CUtensorMap u1, u2;

@@ -145,8 +145,7 @@ class SlabSim:
                 if self.prev is not None or self.next is not None:
                     exchange_halos(self._faces(), self.prev, self.next, self.rank, self.group)
                 if self.world > 1:
-                    rate = _view(self.sim.rate_device(), 4, torch.int32, self.device)
-                    dist.all_reduce(rate, op=dist.ReduceOp.MAX, group=self.group)
+                    allreduce_rate_word(_view(self.sim.rate_device(), 4, torch.int32, self.device), self.group)
                 self.sim.step(1)
 
     def sync(self) -> None:
@@ -161,14 +160,39 @@ class SlabSim:
     def diagnostics(self) -> Diagnostics:
         """Totals over the whole grid (float64 sums over the slabs; the largest Mach number)."""
         d = self.sim.diagnostics()
-        sums = torch.tensor([d.mass, *d.momentum, d.e_kin, d.e_int, d.e_tot, d.floored], dtype=torch.float64,
-                            device=self.device)
-        mach = torch.tensor([d.max_mach], dtype=torch.float64, device=self.device)
-        if self.world > 1:
-            dist.all_reduce(sums, group=self.group)
-            dist.all_reduce(mach, op=dist.ReduceOp.MAX, group=self.group)
-        s = sums.tolist()
-        return Diagnostics(d.t, d.dt, d.steps, s[0], tuple(s[1:4]), s[4], s[5], s[6], float(mach.item()), s[7])
+        mine = [d.mass, *d.momentum, d.e_kin, d.e_int, d.e_tot, d.floored]
+        s = sum_over_ranks(mine, self.group, self.device)
+        mach = max_over_ranks(d.max_mach, self.group, self.device)
+        return Diagnostics(d.t, d.dt, d.steps, s[0], tuple(s[1:4]), s[4], s[5], s[6], mach, s[7])
+
+
+_SIGN_BIT = -(2 ** 31)  # an int32 word with only its sign bit set
+
+
+def allreduce_rate_word(word: torch.Tensor, group=None) -> None:
+    """Make a slab's rate word (the float bits of its signal-rate maximum, which the sweep folds
+    with an unsigned atomicMax) the unsigned maximum over all ranks, in place.
+
+    Collectives have no unsigned 32-bit MAX, so the word is reduced as int32 with its sign bit
+    flipped before and after: that maps unsigned order onto signed order exactly. A NaN rate with
+    its sign bit set (0xffc00000) therefore wins over every healthy rank's rate, as it does inside
+    one GPU's atomicMax, and the clock of every rank sees it."""
+    word.bitwise_xor_(_SIGN_BIT)
+    dist.all_reduce(word, op=dist.ReduceOp.MAX, group=group)
+    word.bitwise_xor_(_SIGN_BIT)
+
+
+def sum_over_ranks(values: list[float], group=None, device=None) -> list[float]:
+    """Each value's sum over the ranks, correctly rounded (math.fsum of every rank's float64
+    value, gathered), so the cross-rank step keeps the compensated totals' accuracy."""
+    if not dist.is_initialized() or dist.get_world_size(group) == 1:
+        return [float(v) for v in values]
+    mine = torch.tensor(values, dtype=torch.float64, device=device)
+    world = dist.get_world_size(group)
+    every = torch.empty(world * len(values), dtype=torch.float64, device=device)
+    dist.all_gather_into_tensor(every, mine, group=group)
+    rows = every.view(world, len(values)).cpu().tolist()
+    return [math.fsum(r[i] for r in rows) for i in range(len(values))]
 
 
 def max_over_ranks(x: float, group=None, device=None) -> float:

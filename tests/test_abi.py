@@ -102,3 +102,15 @@ def test_refuses_bad_configs_without_gpu():
         assert rc in (_abi.SHZ_E_CONFIG, _abi.SHZ_E_NODEV)
         if rc == _abi.SHZ_E_CONFIG:
             assert b"refused" in lib.shz_last_error(None)
+
+
+def test_reference_arm_tgv_init_equals_the_library_init():
+    """bench.py's reference arm builds the Taylor-Green init with numpy alone; it is the library's
+    init of the same grid (both float64 at the cell centres)."""
+    import bench
+
+    n = 12
+    cfg = Config(n=(n, n, n), dx=2 * math.pi / n, gamma=5 / 3)
+    want = problem_prims(cfg, Problem("tgv", a=(1.0, 100.0, 1.0)))
+    got = bench.tgv_prims(n)
+    np.testing.assert_allclose(got, np.asarray(want).reshape(-1, 6), rtol=0, atol=1e-14)

@@ -120,3 +120,56 @@ def test_halo_exchange_matches_whole_field(world, periodic):
     for rank, ok1, ok2, slow in got:
         assert ok1 and ok2, (rank, ok1, ok2)
         assert slow == world - 1 + 0.5
+
+
+def _word_worker(rank: int, world: int, port: int, q):
+    from shaderous_b200.dist import allreduce_rate_word, sum_over_ranks
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        def bits(x):
+            return int(np.array([x], dtype=np.float32).view(np.int32)[0])
+
+        neg_nan = int(np.array([0xFFC00000], dtype=np.uint32).view(np.int32)[0])
+        cases = {
+            "finite": [bits(3.0), bits(7.5), bits(0.25)],
+            "neg_nan": [bits(3.0), neg_nan, bits(1e30)],
+            "pos_nan": [bits(np.inf), bits(2.0), 0x7FC00000],
+            "inf": [bits(np.inf), bits(2.0), bits(5.0)],
+        }
+        out = {}
+        for name, per_rank in cases.items():
+            w = torch.tensor([per_rank[rank]], dtype=torch.int32)
+            allreduce_rate_word(w)
+            out[name] = int(w.item())
+        # correctly rounded sums: one rank's large value and others' small ones that plain
+        # float64 addition in rank order would lose
+        vals = [[1e16, 1.0, -3.0], [1.0, 1e-3, 2.0], [1.0, 1e-3, 1.0]][rank]
+        out["sums"] = sum_over_ranks(vals)
+        q.put((rank, out))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_rate_word_reduces_as_unsigned_and_sums_are_correctly_rounded():
+    """The rate word's maximum over ranks is the unsigned maximum the sweep's atomicMax takes: a
+    NaN whose sign bit is set wins over the healthy ranks (so every rank's clock reports NaN);
+    the totals' cross-rank sum is math.fsum of the ranks' values."""
+    import math
+
+    world = 3
+    ctx = mp.get_context("spawn")
+    q = ctx.SimpleQueue()
+    mp.start_processes(_word_worker, args=(world, _free_port(), q), nprocs=world, start_method="spawn")
+    got = dict(q.get() for _ in range(world))
+    u = lambda x: int(np.array([x], dtype=np.int32).view(np.uint32)[0])  # noqa: E731
+    f = lambda x: float(np.array([x], dtype=np.int32).view(np.float32)[0])  # noqa: E731
+    for rank, out in got.items():
+        assert f(out["finite"]) == 7.5
+        assert u(out["neg_nan"]) == 0xFFC00000, hex(u(out["neg_nan"]))
+        assert u(out["pos_nan"]) == 0x7FC00000
+        assert f(out["inf"]) == np.inf
+        want = [math.fsum([1e16, 1.0, 1.0]), math.fsum([1.0, 1e-3, 1e-3]), 0.0]
+        assert out["sums"] == want, (rank, out["sums"], want)
