@@ -339,6 +339,15 @@ int shz_amr_table(shz_amr* a, int32_t* out);
 int shz_amr_get_leaves_state(shz_amr* a, float* u1, float* u2);
 /* The last refinement indicators per slot (cap floats). */
 int shz_amr_flags(shz_amr* a, float* out);
+/* The primitive region of block `slot` as the last assemble left it (a step's first pass, or a
+ * refinement check's): 20^ndim texels, x fastest, w1 = (rho, vx, vy, vz) and w2 = (p, s, cs, 0)
+ * as float4 each (AmrSim's W1/W2 atlas texels, amr/assemble.wgsl:78-154; this build keeps the
+ * sound speed where the reference keeps the internal energy). For checks against an oracle. */
+int shz_amr_prims(shz_amr* a, int32_t slot, float* w1, float* w2);
+/* The regrid table of the last re-mesh (cap * 12 ints, BlockTree.regridTable,
+ * src/amr/tree.ts:681-693: kind 1 copy / 2 prolong / 3 restrict, source slot, octant, children);
+ * zero before the first. */
+int shz_amr_regrid_table(shz_amr* a, int32_t* out);
 /* The device's ghost classification of block `slot`: (kind, source slot, l0, l1, l2) for each of
  * the 20^ndim texels of its primitive region, x fastest (amr/grid.wgsl ghost_src). */
 int shz_amr_ghost_map(shz_amr* a, int32_t slot, int32_t* out);

@@ -230,6 +230,8 @@ SIGNATURES = [
     ("shz_amr_get_leaves_state", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("shz_amr_flags", C.c_int, [C.c_void_p, C.c_void_p]),
     ("shz_amr_ghost_map", C.c_int, [C.c_void_p, C.c_int32, C.c_void_p]),
+    ("shz_amr_prims", C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
+    ("shz_amr_regrid_table", C.c_int, [C.c_void_p, C.c_void_p]),
     ("shz_amr_profile", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(shz_profile_result)]),
     ("shz_amr_kernel_launches", C.c_int64, [C.c_void_p]),
     ("shz_amr_bins", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),

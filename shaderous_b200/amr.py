@@ -150,6 +150,21 @@ class AmrSim:
         self._ok(self._lib.shz_amr_ghost_map(self._h, int(slot), out.ctypes.data))
         return out
 
+    def prims(self, slot: int) -> np.ndarray:
+        """Block `slot`'s primitive region as the last assemble left it: (20^ndim, 8) floats per
+        texel, x fastest: rho, vx, vy, vz, p, s, cs, 0."""
+        wn = 20 ** self.cfg.ndim
+        w1 = np.zeros((wn, 4), np.float32)
+        w2 = np.zeros((wn, 4), np.float32)
+        self._ok(self._lib.shz_amr_prims(self._h, int(slot), w1.ctypes.data, w2.ctypes.data))
+        return np.concatenate([w1, w2], axis=1)
+
+    def regrid_table(self) -> np.ndarray:
+        """The last re-mesh's regrid table (cap x 12 ints: kind, source, octant, _, children)."""
+        t = np.zeros((self.cfg.cap, 12), np.int32)
+        self._ok(self._lib.shz_amr_regrid_table(self._h, t.ctypes.data))
+        return t
+
     def profile(self, n: int) -> dict:
         r = _abi.shz_profile_result()
         self._ok(self._lib.shz_amr_profile(self._h, int(n), C.byref(r)))

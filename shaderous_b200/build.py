@@ -72,11 +72,12 @@ def build_library(force: bool = False, verbose: bool = False) -> Path:
 
 
 def build_oracle(force: bool = False) -> Path:
-    src = ORACLE_DIR / "ref_hydro.cpp"
-    if not force and not _stale(ORACLE_LIB, [src, Path(__file__)]):
+    srcs = [ORACLE_DIR / "ref_hydro.cpp", ORACLE_DIR / "amr_ref.cpp"]
+    if not force and not _stale(ORACLE_LIB, srcs + [ORACLE_DIR / "hydro_ref.h", Path(__file__)]):
         return ORACLE_LIB
     tmp = ORACLE_LIB.with_suffix(".so.tmp")
-    subprocess.run(["g++", "-O2", "-std=c++17", "-fopenmp", "-fPIC", "-shared", "-o", str(tmp), str(src)], check=True)
+    subprocess.run(["g++", "-O2", "-std=c++17", "-fopenmp", "-fPIC", "-shared", "-o", str(tmp), *map(str, srcs)],
+                   check=True)
     os.replace(tmp, ORACLE_LIB)
     return ORACLE_LIB
 

@@ -1178,6 +1178,24 @@ int shz_amr_flags(shz_amr* a, float* out) {
   return 0;
 }
 
+int shz_amr_prims(shz_amr* a, int32_t slot, float* w1, float* w2) {
+  if (!a || !w1 || !w2 || slot < 0 || slot >= a->cfg.cap) return SHZ_E_CONFIG;
+  Dev dv(a->device);
+  const size_t n = (size_t)a->WN, o = (size_t)slot * n;
+  AMR_CUDA(a, cudaMemcpyAsync(w1, a->L.w1 + o, n * sizeof(float4), cudaMemcpyDeviceToHost, a->stream));
+  AMR_CUDA(a, cudaMemcpyAsync(w2, a->L.w2 + o, n * sizeof(float4), cudaMemcpyDeviceToHost, a->stream));
+  AMR_CUDA(a, cudaStreamSynchronize(a->stream));
+  return 0;
+}
+
+int shz_amr_regrid_table(shz_amr* a, int32_t* out) {
+  if (!a || !out) return SHZ_E_CONFIG;
+  const size_t n = (size_t)a->cfg.cap * shz::amr::RG_STRIDE;
+  std::memset(out, 0, n * sizeof(int32_t));
+  std::memcpy(out, a->h_rg.data(), std::min(n, a->h_rg.size()) * sizeof(int32_t));
+  return 0;
+}
+
 int shz_amr_ghost_map(shz_amr* a, int32_t slot, int32_t* out) {
   if (!a || !out || slot < 0 || slot >= a->cfg.cap) return SHZ_E_CONFIG;
   Dev dv(a->device);
