@@ -8,7 +8,8 @@ pinned on the CPU by tests/test_amr_oracle.py), from the same float32 state on t
 - one step, and several, of the block sweep (fused, and the reference's two passes): relative L1
   per conserved variable <= 1e-5 against the oracle's predict and update with fine-flux matching
   (amr/predict.wgsl:184-221, amr/update.wgsl:207-560), L-inf <= 1e-4;
-- the Löhner indicators (amr/flag.wgsl:66-155) within float32 rounding (relative 2e-5), and the
+- the Löhner indicators (amr/flag.wgsl:66-155) within float32 rounding (2e-5 relative plus 1e-6),
+  and the
   block tree's decisions from the oracle's indicators equal the ones the GPU run made;
 - the regrid fill of the new leaves (amr/regrid.wgsl:41-139): relative L-inf per variable <= 1e-6.
 Meshes: 2D and 3D, levels 0-2, with reflecting, outflow and periodic faces.
@@ -127,6 +128,20 @@ def test_assemble_and_steps_match_oracle(case):
         check_state(g1, g2, o.state(slots), 1e-5, 1e-4, f"step {n + 1}")
 
 
+def leaf_positions(cfg, level, c):
+    """Cell centres (CB, 3) of the leaf at `level`, block coordinates c; box centred on 0."""
+    dx = cfg.box / (cfg.nr * BS * 2 ** level)
+    i = np.arange(BS)
+    if cfg.ndim == 3:
+        z, y, x = np.meshgrid(i, i, i, indexing="ij")
+    else:
+        y, x = np.meshgrid(i, i, indexing="ij")
+        z = np.zeros_like(x)
+    pos = np.stack([(c[0] * BS + x + 0.5) * dx, (c[1] * BS + y + 0.5) * dx,
+                    (c[2] * BS + z + 0.5) * dx if cfg.ndim == 3 else 0.0 * x], axis=-1).reshape(-1, 3)
+    return pos - cfg.box / 2 * np.array([1, 1, 1 if cfg.ndim == 3 else 0])
+
+
 def tree_like(cfg, tab):
     """A host block tree with the same leaves as `tab` (the same parents split, coarsest first)."""
     t = BlockTree(cfg.ndim, cfg.nr, cfg.max_level, cfg.cap, cfg.hydro.bc_lo, cfg.hydro.bc_hi)
@@ -150,7 +165,23 @@ def test_flags_decisions_and_regrid_match_oracle(case):
     ndim, bc_lo, bc_hi, recon, isen, two_pass = case
     cfg, a = make(*case)
     with a:
-        a.step(10 if ndim == 3 else 30)  # the blast moves out: some leaves refine, some merge
+        # a new state on the blast's mesh: a density jump off the centre, so that leaves at the
+        # jump refine and the refined blocks about the centre merge
+        slots, levels, coords = a.leaves()
+        u1s, u2s = [], []
+        for lv, c in zip(levels, coords):
+            x = leaf_positions(cfg, int(lv), c)
+            w = np.zeros((len(x), 6))
+            w[:, 0] = 1.0 + 2.0 * (x[:, 0] > 0.2) + 0.05 * np.sin(6.0 * x[:, 1])
+            w[:, 1] = 0.1
+            w[:, 4] = 1.0
+            w[:, 5] = (x[:, 0] > 0.2).astype(float)
+            e = w[:, 4] / (cfg.hydro.gamma - 1)
+            r = w[:, 0]
+            u1s.append(np.stack([r, r * w[:, 1], 0 * r, 0 * r], axis=1))
+            u2s.append(np.stack([e + 0.5 * r * w[:, 1] ** 2, e, r * w[:, 5], 0 * r], axis=1))
+        a.set_leaves_state(np.stack(u1s).astype(np.float32), np.stack(u2s).astype(np.float32))
+        a.step(2)
         slots, _, _ = a.leaves()
         tab = a.table()
         u1, u2 = a.leaves_state()
@@ -167,8 +198,11 @@ def test_flags_decisions_and_regrid_match_oracle(case):
         o.assemble(active_blocks(tab))
         ind = o.flags(slots)
         got = flags[slots].astype(np.float64)
-        err = np.abs(got - ind) / np.maximum(ind, 1e-3)
-        assert err.max() <= 2e-5, (err.max(), slots[err.argmax()], got[err.argmax()], ind[err.argmax()])
+        # (the indicator is dimensionless, about 1 at a jump; in smooth gas it is a small
+        # difference of float32 values, so the bound has an absolute part far below the
+        # thresholds the decisions use)
+        err = np.abs(got - ind) - 2e-5 * ind
+        assert err.max() <= 1e-6, (err.max(), slots[err.argmax()], got[err.argmax()], ind[err.argmax()])
         # no indicator so close to a threshold that float32 rounding could tip it
         for thr in (cfg.refine_hi, cfg.refine_lo):
             assert (np.abs(ind - thr) > 1e-4 * thr).all()
