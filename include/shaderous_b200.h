@@ -441,6 +441,12 @@ int shz_server_drain(shz_server* s, int32_t max_rounds);
 int shz_server_run_stream(shz_server* s, const shz_request* reqs, int32_t n, shz_server_stats* out);
 /* The conservation totals of a finished request, and (keep_states) its final state as uniform
  * arrays of n^ndim cells, x fastest. */
+/* Cancel request `id` (called between other server calls, with no round in flight): a queued
+ * request leaves the queue; a running one gives its block slots and clock back at once, and the
+ * others go on as they would have. Its result and state then return SHZ_E_CANCELLED. Returns
+ * SHZ_E_CONFIG for an unknown id or a request that has finished or was cancelled already. No
+ * counterpart in the reference (whose runs stop by their RunOptions timeoutMs). */
+int shz_server_cancel(shz_server* s, int64_t id);
 int shz_server_result(shz_server* s, int64_t id, shz_diag* diag);
 int shz_server_state(shz_server* s, int64_t id, float* u1, float* u2);
 /* The same stream run one request after another, each through the plain uniform-grid step

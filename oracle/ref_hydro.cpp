@@ -299,8 +299,12 @@ struct Hydro {
           for (int f = 0; f < 6; f++) {
             const int axis = f >> 1;
             const bool upper = (f & 1) == 1;
-            Pred nb;
-            predict(i + OFF[f][0], j + OFF[f][1], k + OFF[f][2], &nb);
+            // an in-range neighbour's memoised prediction is read in place; a ghost's is formed
+            const int ni = i + OFF[f][0], nj = j + OFF[f][1], nk = k + OFF[f][2];
+            Pred ghost;
+            const bool inside = ni >= 0 && nj >= 0 && nk >= 0 && ni < c.n[0] && nj < c.n[1] && nk < c.n[2];
+            if (!inside) predict(ni, nj, nk, &ghost);
+            const Pred& nb = inside ? preds[index(ni, nj, nk)] : ghost;
             const Side L = upper ? side(self, axis, 1) : side(nb, axis, 1);
             const Side R = upper ? side(nb, axis, -1) : side(self, axis, -1);
             const double w = std::max(self.flag, nb.flag);

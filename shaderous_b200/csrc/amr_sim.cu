@@ -1049,6 +1049,7 @@ int shz_amr_run(shz_amr* a, const shz_run_opts* o, shz_run_result* r) {
   if (stop != t_end_was) AMR_CUDA(a, cudaMemcpyAsync(&a->clk->t_end, &stop, sizeof(double), cudaMemcpyHostToDevice, a->stream));
   int stopped = SHZ_STOP_STEPS;
   int grow = 1;
+  double ms_per_step = 0;  // the batches' pace
   for (;;) {
     const long long taken = c.steps - start;
     const long long left = o->steps < 0 ? std::numeric_limits<long long>::max() : o->steps - taken;
@@ -1057,11 +1058,15 @@ int shz_amr_run(shz_amr* a, const shz_run_opts* o, shz_run_result* r) {
     if (std::isfinite(t_end_was) && c.t >= t_end_was * (1 - 1e-12)) { stopped = SHZ_STOP_END; break; }
     if (o->timeout_ms > 0 && ms() > o->timeout_ms) { stopped = SHZ_STOP_TIMEOUT; break; }
     long long batch = std::min<long long>(left, grow);
+    // batches of about 100 ms on blocks (api.ts run: BATCH_MS for an adaptive mesh)
+    if (ms_per_step > 0) batch = std::min<long long>(batch, std::max(1.0, std::floor(100.0 / ms_per_step)));
     if (std::isfinite(stop) && last_dt > 0) {
       const double ahead = std::ceil((stop - c.t) / last_dt - 1e-6);
       if (ahead >= 1 && ahead < (double)batch) batch = (long long)ahead;
     }
-    if ((rc = shz_amr_step(a, (int)std::max<long long>(batch, 1)))) break;
+    batch = std::max<long long>(batch, 1);
+    const double b0 = ms();
+    if ((rc = shz_amr_step(a, (int)batch))) break;
     if ((rc = read_clock(a, &c))) break;
     if (c.bad) { rc = fail(a, SHZ_E_NAN, "the clock is NaN after %lld steps", c.steps); break; }
     if (c.last_dt > 0) last_dt = c.last_dt;
@@ -1069,6 +1074,8 @@ int shz_amr_run(shz_amr* a, const shz_run_opts* o, shz_run_result* r) {
       stopped = has_until && c.t >= o->until * (1 - 1e-9) ? SHZ_STOP_TIME : SHZ_STOP_END;
       break;
     }
+    const double m = (ms() - b0) / (double)batch;
+    ms_per_step = ms_per_step > 0 ? 0.7 * ms_per_step + 0.3 * m : m;
     grow = std::min(grow * 2, 64);
   }
   if (stop != t_end_was) {

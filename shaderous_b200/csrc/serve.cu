@@ -48,6 +48,7 @@ struct Grid {
   bool staged = false;
   double arrival = 0, finished = 0;
   bool done = false;
+  bool cancelled = false;  // shz_server_cancel took it off the queue or the device
   shz_diag diag{};
   std::vector<float> out1, out2;      // final state (keep_states), uniform layout
 };
@@ -689,10 +690,43 @@ int shz_server_run_stream(shz_server* s, const shz_request* reqs, int32_t n, shz
   return 0;
 }
 
+int shz_server_cancel(shz_server* s, int64_t id) {
+  if (!s) return SHZ_E_CONFIG;
+  auto it = s->grids.find(id);
+  if (it == s->grids.end()) return fail(s, SHZ_E_CONFIG, "no request %lld", (long long)id);
+  Grid& G = *it->second;
+  if (G.done) return fail(s, SHZ_E_CONFIG, "request %lld has %s", (long long)id, G.cancelled ? "been cancelled" : "finished");
+  Dev dv(s->device);
+  auto q = std::find(s->pending.begin(), s->pending.end(), &G);
+  if (q != s->pending.end()) {
+    s->pending.erase(q);
+  } else {
+    // admitted: no round is in flight between calls, so its slots and clock go back at once
+    Engine& e = s->e[G.eng];
+    shz::DevClock idle;
+    std::memset(&idle, 0, sizeof idle);
+    idle.t_end = HUGE_VAL;
+    idle.dt_max = HUGE_VAL;
+    idle.cfl_dx = 1.0;
+    SV_CUDA(s, cudaMemcpyAsync(e.d_clk + G.g, &idle, sizeof idle, cudaMemcpyHostToDevice, e.stream));
+    SV_CUDA(s, cudaStreamSynchronize(e.stream));
+    for (int b = G.nblocks - 1; b >= 0; b--) e.free_slots.push_back(G.slots[b]);
+    e.free_g.push_back(G.g);
+    G.g = -1;
+    e.active.erase(std::find(e.active.begin(), e.active.end(), &G));
+    e.dirty = true;
+  }
+  G.cancelled = true;
+  G.done = true;
+  G.finished = now_s(s);
+  return 0;
+}
+
 int shz_server_result(shz_server* s, int64_t id, shz_diag* d) {
   if (!s || !d) return SHZ_E_CONFIG;
   auto it = s->grids.find(id);
   if (it == s->grids.end()) return fail(s, SHZ_E_CONFIG, "no request %lld", (long long)id);
+  if (it->second->cancelled) return fail(s, SHZ_E_CANCELLED, "request %lld was cancelled", (long long)id);
   if (!it->second->done) return fail(s, SHZ_E_CONFIG, "request %lld has not finished", (long long)id);
   *d = it->second->diag;
   return 0;
@@ -701,6 +735,8 @@ int shz_server_result(shz_server* s, int64_t id, shz_diag* d) {
 int shz_server_state(shz_server* s, int64_t id, float* u1, float* u2) {
   if (!s || !u1 || !u2) return SHZ_E_CONFIG;
   auto it = s->grids.find(id);
+  if (it != s->grids.end() && it->second->cancelled)
+    return fail(s, SHZ_E_CANCELLED, "request %lld was cancelled", (long long)id);
   if (it == s->grids.end() || !it->second->done) return fail(s, SHZ_E_CONFIG, "request %lld has not finished", (long long)id);
   if (it->second->out1.empty()) return fail(s, SHZ_E_CONFIG, "states are kept only with keep_states");
   std::memcpy(u1, it->second->out1.data(), it->second->out1.size() * sizeof(float));

@@ -524,6 +524,7 @@ int shz_run(shz_sim* s, const shz_run_opts* o, shz_run_result* r) {
   }
   int stopped = -1;
   int grow = 1;
+  double ms_per_step = 0;  // the batches' pace (api.ts run: batches of about BATCH_MS = 50 ms)
   for (;;) {
     const long long taken = c.steps - start;
     const long long left = o->steps < 0 ? std::numeric_limits<long long>::max() : o->steps - taken;
@@ -532,11 +533,13 @@ int shz_run(shz_sim* s, const shz_run_opts* o, shz_run_result* r) {
     if (std::isfinite(t_end_was) && c.t >= t_end_was * (1 - 1e-12)) { stopped = SHZ_STOP_END; break; }
     if (o->timeout_ms > 0 && elapsed_ms() > o->timeout_ms) { stopped = SHZ_STOP_TIMEOUT; break; }
     long long batch = std::min<long long>(left, grow);
+    if (ms_per_step > 0) batch = std::min<long long>(batch, std::max(1.0, std::floor(50.0 / ms_per_step)));
     if (std::isfinite(stop) && last_dt > 0) {
       const double ahead = std::ceil((stop - c.t) / last_dt - 1e-6);
       if (ahead >= 1 && ahead < (double)batch) batch = (long long)ahead;
     }
     if (batch < 1) batch = 1;
+    const double b0 = elapsed_ms();
     if ((rc = enqueue_steps(s, (int)batch))) break;
     if ((rc = read_clock(s, &c))) break;
     if (c.bad) { rc = fail(s, SHZ_E_NAN, "the clock is NaN after %lld steps", c.steps); break; }
@@ -546,6 +549,8 @@ int shz_run(shz_sim* s, const shz_run_opts* o, shz_run_result* r) {
       stopped = has_until && c.t >= o->until * (1 - 1e-9) ? SHZ_STOP_TIME : SHZ_STOP_END;
       break;
     }
+    const double m = (elapsed_ms() - b0) / (double)batch;
+    ms_per_step = ms_per_step > 0 ? 0.7 * ms_per_step + 0.3 * m : m;
     grow = std::min(grow * 2, 256);
   }
   if (stop != t_end_was) {

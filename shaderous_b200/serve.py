@@ -106,6 +106,10 @@ class Server:
         self._ok(self._lib.shz_server_run_stream(self._h, _array(reqs), len(reqs), C.byref(st)))
         return _stats(st)
 
+    def cancel(self, rid: int) -> None:
+        """Take request `rid` off the queue or the device; its result then raises SHZ_E_CANCELLED."""
+        self._ok(self._lib.shz_server_cancel(self._h, int(rid)))
+
     def result(self, rid: int) -> Diagnostics:
         d = _abi.shz_diag()
         self._ok(self._lib.shz_server_result(self._h, rid, C.byref(d)))
