@@ -278,6 +278,14 @@ int shz_tree_lists(const shz_tree* t, int32_t* all, int32_t* leaves, int32_t* pe
 int64_t shz_tree_index_grid_size(const shz_tree* t);
 int shz_tree_index_grid(const shz_tree* t, uint32_t* out);             /* leaf slot per finest block cell */
 /* count, free slots, leaves, deepest level, highest slot used */
+/* indexGrid(boxes) (tree.ts:721-803): the index grid (as shz_tree_index_grid) and the boxes that
+ * changed since the last call of this function, 6 ints each (origin x, y, z, size x, y, z): the
+ * whole grid on the first call, else runs of changed rows; a copy updated only inside them stays
+ * equal to the grid. *n_boxes = the boxes found (at most max_boxes are written). */
+int shz_tree_index_grid_boxes(shz_tree* t, uint32_t* out, int32_t* boxes, int32_t max_boxes, int32_t* n_boxes);
+/* The bcLo / bcHi setters (tree.ts:193-199): boundary types of a built tree; tables read after it
+ * show them. */
+int shz_tree_set_bc(shz_tree* t, const int32_t bc_lo[3], const int32_t bc_hi[3]);
 int shz_tree_stats(const shz_tree* t, int32_t* blocks, int32_t* free_slots, int32_t* leaves, int32_t* deepest, int32_t* high_slot);
 
 /*

@@ -213,6 +213,8 @@ SIGNATURES = [
                                  C.POINTER(C.c_int32)]),
     ("shz_tree_index_grid_size", C.c_int64, [C.c_void_p]),
     ("shz_tree_index_grid", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("shz_tree_index_grid_boxes", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]),
+    ("shz_tree_set_bc", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("shz_tree_stats", C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                  C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     ("shz_amr_create", C.c_int, [C.POINTER(shz_amr_config), C.POINTER(C.c_void_p)]),

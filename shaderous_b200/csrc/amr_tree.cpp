@@ -64,6 +64,7 @@ Block* BlockTree::create(int level, const int c[3], Block* parent) {
   ++version_;
   slots_[slot] = b;
   blocks_[key(level, c[0], c[1], c[2])] = b;
+  new_leaves_.push_back(b);  // tree.ts:234
   return b;
 }
 
@@ -227,6 +228,7 @@ bool BlockTree::can_coarsen(const Block* p) const {
 void BlockTree::coarsen(Block* p) {
   for (Block* ch : p->children) remove(ch);
   p->children.clear();
+  new_leaves_.push_back(p);  // tree.ts:417
 }
 
 // tree.ts:420-430 evictable: parents with only leaf children, scored by their most strongly
@@ -547,21 +549,100 @@ int64_t BlockTree::index_grid_size() const {
   return ndim == 1 ? m : (ndim == 2 ? m * m : m * m * m);
 }
 
+// tree.ts:805-812 fillLeaf: a leaf's cells of the index grid.
+void BlockTree::fill_leaf(uint32_t* g, const Block* b) const {
+  const int64_t m = (int64_t)nr << max_level;
+  const int64_t span = (int64_t)1 << (max_level - b->level);
+  if (ndim == 1) {
+    for (int64_t x = b->c[0] * span; x < (b->c[0] + 1) * span; x++) g[x] = b->slot;
+    return;
+  }
+  const int64_t z0 = ndim == 3 ? b->c[2] * span : 0;
+  for (int64_t k = z0; k < z0 + (ndim == 3 ? span : 1); k++)
+    for (int64_t j = b->c[1] * span; j < (b->c[1] + 1) * span; j++)
+      for (int64_t x = b->c[0] * span; x < (b->c[0] + 1) * span; x++) g[(k * m + j) * m + x] = b->slot;
+}
+
 // tree.ts:721-816 indexGrid (the whole grid; every cell lies in exactly one leaf).
 void BlockTree::index_grid(uint32_t* g) const {
-  const int64_t m = (int64_t)nr << max_level;
-  for (const Block* b : slots_) {
-    if (!b || !b->leaf()) continue;
-    const int64_t span = (int64_t)1 << (max_level - b->level);
-    if (ndim == 1) {
-      for (int64_t x = b->c[0] * span; x < (b->c[0] + 1) * span; x++) g[x] = b->slot;
+  for (const Block* b : slots_)
+    if (b && b->leaf()) fill_leaf(g, b);
+}
+
+// tree.ts:721-803 indexGrid with boxes: filling the leaves made since the last read covers
+// whatever changed (every cell lies in exactly one leaf). The boxes: per row of the outer axis (y
+// in 2D, z in 3D) the extent filled along the inner ones, merged into runs of rows that bridge
+// gaps of up to GAP = 4 unchanged rows (each box costs the caller a copy call).
+const std::vector<uint32_t>& BlockTree::index_grid_tracked(std::vector<std::array<int, 6>>* boxes) {
+  const int m = nr << max_level;
+  const bool d3 = ndim == 3;
+  const int mz = d3 ? m : 1;
+  const size_t n = (size_t)index_grid_size();
+  if (grid_.size() != n) {
+    grid_.assign(n, 0u);
+    index_grid(grid_.data());
+    new_leaves_.clear();
+    if (boxes) boxes->push_back({0, 0, 0, m, ndim >= 2 ? m : 1, mz});
+    return grid_;
+  }
+  if (ndim == 1) {
+    int lo = m, hi = 0;
+    for (Block* b : new_leaves_) {
+      if (!b->leaf() || slots_[b->slot] != b) continue;
+      fill_leaf(grid_.data(), b);
+      const int span = 1 << (max_level - b->level);
+      lo = std::min(lo, b->c[0] * span);
+      hi = std::max(hi, (b->c[0] + 1) * span);
+    }
+    new_leaves_.clear();
+    if (boxes && hi > lo) boxes->push_back({lo, 0, 0, hi - lo, 1, 1});
+    return grid_;
+  }
+  std::vector<int> lo0(m, m), hi0(m, 0), lo1(m, m), hi1(m, 0);
+  for (Block* b : new_leaves_) {
+    if (!b->leaf() || slots_[b->slot] != b) continue;
+    fill_leaf(grid_.data(), b);
+    const int span = 1 << (max_level - b->level);
+    const int x0 = b->c[0] * span, y0 = b->c[1] * span, o0 = (d3 ? b->c[2] : b->c[1]) * span;
+    for (int o = o0; o < o0 + span; o++) {
+      lo0[o] = std::min(lo0[o], x0);
+      hi0[o] = std::max(hi0[o], x0 + span);
+      if (d3) {
+        lo1[o] = std::min(lo1[o], y0);
+        hi1[o] = std::max(hi1[o], y0 + span);
+      }
+    }
+  }
+  new_leaves_.clear();
+  if (!boxes) return grid_;
+  constexpr int GAP = 4;
+  for (int o = 0; o < m;) {
+    if (hi0[o] == 0) {
+      o++;
       continue;
     }
-    const int64_t z0 = ndim == 3 ? b->c[2] * span : 0;
-    for (int64_t k = z0; k < z0 + (ndim == 3 ? span : 1); k++)
-      for (int64_t j = b->c[1] * span; j < (b->c[1] + 1) * span; j++)
-        for (int64_t x = b->c[0] * span; x < (b->c[0] + 1) * span; x++) g[(k * m + j) * m + x] = b->slot;
+    int a0 = m, b0 = 0, a1 = m, b1 = 0, end = o;
+    for (int k = o; k < m && k <= end + GAP; k++) {
+      if (hi0[k] == 0) continue;
+      a0 = std::min(a0, lo0[k]);
+      b0 = std::max(b0, hi0[k]);
+      a1 = std::min(a1, lo1[k]);
+      b1 = std::max(b1, hi1[k]);
+      end = k;
+    }
+    if (d3) boxes->push_back({a0, a1, o, b0 - a0, b1 - a1, end + 1 - o});
+    else boxes->push_back({a0, o, 0, b0 - a0, end + 1 - o, 1});
+    o = end + 1;
   }
+  return grid_;
+}
+
+void BlockTree::set_bc(const int lo[3], const int hi[3]) {
+  for (int a = 0; a < 3; a++) {
+    bc_lo[a] = lo[a];
+    bc_hi[a] = hi[a];
+  }
+  ++version_;  // cached neighbour tests see a new tree
 }
 
 }  // namespace amr

@@ -119,8 +119,18 @@ class BlockTree {
   void lists(std::vector<int32_t>& all, std::vector<int32_t>& leaves, std::vector<int32_t>& per_level) const;
   void index_grid(uint32_t* out) const;  // (nr << max_level)^ndim leaf slots (tree.ts:721)
   int64_t index_grid_size() const;
+  // tree.ts:721-803 indexGrid(boxes): the index grid kept between reads, updated from the leaves
+  // made since the last read, and the boxes (origin, size; 6 ints each) that cover what changed:
+  // the whole grid on the first read, else runs of changed rows of the outer axis.
+  const std::vector<uint32_t>& index_grid_tracked(std::vector<std::array<int, 6>>* boxes);
+  // tree.ts:193-199 the bcLo / bcHi setters: boundary types of a tree already built (every table
+  // read after the change shows them).
+  void set_bc(const int lo[3], const int hi[3]);
 
  private:
+  std::vector<uint32_t> grid_;       // the index grid as last read (empty: not read yet)
+  std::vector<Block*> new_leaves_;   // blocks that became leaves since the last read (tree.ts:129)
+  void fill_leaf(uint32_t* g, const Block* b) const;
   int64_t key(int level, int c0, int c1, int c2) const;
   Block* create(int level, const int c[3], Block* parent);
   void remove(Block* b);

@@ -1,4 +1,5 @@
 // C ABI of the host block tree (amr_tree.h): the shz_tree_* entry points.
+#include <array>
 #include <cstring>
 #include <exception>
 #include <mutex>
@@ -153,6 +154,25 @@ int64_t shz_tree_index_grid_size(const shz_tree* t) { return t ? t->t->index_gri
 int shz_tree_index_grid(const shz_tree* t, uint32_t* out) {
   if (!t || !out) return fail("shz_tree_index_grid: null argument");
   t->t->index_grid(out);
+  return SHZ_OK;
+}
+
+int shz_tree_index_grid_boxes(shz_tree* t, uint32_t* out, int32_t* boxes, int32_t max_boxes, int32_t* n_boxes) {
+  if (!t || !out || !n_boxes || (max_boxes > 0 && !boxes)) return fail("shz_tree_index_grid_boxes: null argument");
+  std::vector<std::array<int, 6>> bx;
+  const std::vector<uint32_t>& g = t->t->index_grid_tracked(&bx);
+  std::memcpy(out, g.data(), g.size() * sizeof(uint32_t));
+  *n_boxes = (int32_t)bx.size();
+  for (int32_t i = 0; i < (int32_t)bx.size() && i < max_boxes; i++)
+    for (int q = 0; q < 6; q++) boxes[6 * i + q] = bx[i][q];
+  return SHZ_OK;
+}
+
+int shz_tree_set_bc(shz_tree* t, const int32_t bc_lo[3], const int32_t bc_hi[3]) {
+  if (!t || !bc_lo || !bc_hi) return fail("shz_tree_set_bc: null argument");
+  int lo[3], hi[3];
+  for (int a = 0; a < 3; a++) { lo[a] = bc_lo[a]; hi[a] = bc_hi[a]; }
+  t->t->set_bc(lo, hi);
   return SHZ_OK;
 }
 

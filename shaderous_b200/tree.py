@@ -39,6 +39,7 @@ class BlockTree:
         self._ok(self._lib.shz_tree_create(ndim, nr, max_level, cap, _i3(bc_lo), _i3(bc_hi), 1 if edge_balance else 0,
                                            C.byref(h)))
         self._h = h
+        self._bc = (tuple(bc_lo), tuple(bc_hi))
 
     def _ok(self, rc):
         if rc != 0:
@@ -107,6 +108,22 @@ class BlockTree:
         g = np.zeros(n, dtype=np.uint32)
         self._ok(self._lib.shz_tree_index_grid(self._h, g.ctypes.data))
         return g
+
+    def index_grid_boxes(self):
+        """indexGrid(boxes): the grid and the boxes (origin, size) that changed since the last call."""
+        n = self._lib.shz_tree_index_grid_size(self._h)
+        g = np.zeros(n, dtype=np.uint32)
+        cap = 4096
+        bx = np.zeros((cap, 6), dtype=np.int32)
+        k = C.c_int32()
+        self._ok(self._lib.shz_tree_index_grid_boxes(self._h, g.ctypes.data, bx.ctypes.data, cap, C.byref(k)))
+        assert k.value <= cap
+        return g, [(tuple(map(int, b[:3])), tuple(map(int, b[3:]))) for b in bx[:k.value]]
+
+    def set_bc(self, bc_lo, bc_hi):
+        """The bcLo / bcHi setters: boundary types of a built tree (tree.ts:193-199)."""
+        self._ok(self._lib.shz_tree_set_bc(self._h, _i3(bc_lo), _i3(bc_hi)))
+        self._bc = (tuple(bc_lo), tuple(bc_hi))
 
     def stats(self) -> dict:
         v = [C.c_int32() for _ in range(5)]

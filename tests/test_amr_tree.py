@@ -2,8 +2,8 @@
 case (same trees, budgets and thresholds). The reference ships no golden tables; its pins are
 these properties plus the concrete slots and codes the individual cases assert.
 
-Not ported: the incremental index-grid boxes ("reports the index-grid boxes that changed") and a
-boundary change after creation; this tree rebuilds its tables whole on each read.
+Every case is ported, including the index-grid boxes that changed between reads and a change of
+boundaries after the tree was built.
 """
 import math
 
@@ -146,6 +146,65 @@ def test_tables_equal_for_equal_remeshes():
         assert np.array_equal(a.table(), b.table())
         assert np.array_equal(a.index_grid(), b.index_grid())
         covers(a)
+        # A change of boundaries reaches the table read after it: b2 takes the same re-meshes under
+        # the old boundaries and is switched only before its table is read.
+        flipped = tuple(0 if x else 1 for x in bc)
+        a.set_bc(flipped, bc)
+        b2 = make()
+        seed2 = [7]
+
+        def rnd2():
+            seed2[0] = (seed2[0] * 16807) % 2147483647
+            return seed2[0] / 2147483647
+
+        for _ in range(10):
+            ind = np.array([rnd2() * 1.2 for _ in range(3000)])
+            b2.set_bc(bc, bc)
+            b2.adapt(ind, 0.8, 0.3)
+        b2.set_bc(flipped, bc)
+        assert np.array_equal(a.table(), b2.table())
+        # and the boundary codes in it are the new ones (-1 - type at a lower face of the domain)
+        t = a.table()
+        for s, lv, c in a.leaves():
+            for axis in range(ndim):
+                if c[axis] == 0 and flipped[axis] != 0:
+                    assert t[s, 6 + 2 * axis] == -1 - flipped[axis]
+
+
+def test_reports_the_index_grid_boxes_that_changed():
+    """A copy updated only inside the reported boxes, as the GPU texture is, stays equal; and not
+    every re-mesh re-sends the whole grid (tree.test.ts 'reports the index-grid boxes that
+    changed')."""
+    for ndim in (2, 3):
+        t = BlockTree(ndim, 2, 4 if ndim == 2 else 3, 3000, PERIODIC, PERIODIC)
+        m = t.nr << t.max_level
+        mz = m if ndim == 3 else 1
+        copy = np.zeros((mz, m, m), np.uint32)
+        seed = [11]
+
+        def rnd():
+            seed[0] = (seed[0] * 16807) % 2147483647
+            return seed[0] / 2147483647
+
+        partial = 0
+        for rnd_i in range(12):
+            if rnd_i:
+                ind = np.array([rnd() * 1.2 for _ in range(3000)])
+                t.adapt(ind, 0.8, 0.3)
+            g, boxes = t.index_grid_boxes()
+            g3 = g.reshape(mz, m, m)
+            cells = 0
+            for o, sz in boxes:
+                cells += sz[0] * sz[1] * sz[2]
+                # each box packed on its own, as gridBox packs it, then written at its origin
+                data = g3[o[2]:o[2] + sz[2], o[1]:o[1] + sz[1], o[0]:o[0] + sz[0]].copy()
+                assert data.size == sz[0] * sz[1] * sz[2]
+                copy[o[2]:o[2] + sz[2], o[1]:o[1] + sz[1], o[0]:o[0] + sz[0]] = data
+            if rnd_i and cells < g.size:
+                partial += 1
+            assert np.array_equal(copy.reshape(-1), g)
+            assert np.array_equal(g, t.index_grid())
+        assert partial > 0  # not every re-mesh re-sends the whole grid
 
 
 def test_starts_as_uniform_root_grid():
