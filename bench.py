@@ -60,7 +60,9 @@ def parse():
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-comparable", action="store_true",
                     help="skip the configurations the reference publishes throughputs for")
-    ap.add_argument("--serve-requests", type=int, default=200)
+    ap.add_argument("--serve-requests", type=int, default=100)
+    ap.add_argument("--serve-sizes", choices=["config", "small"], default="config",
+                    help="the serving stream's size and step distributions")
     ap.add_argument("--section", choices=["all", "amr", "serving", "comparable"], default="all",
                     help="amr / serving: only that measurement, printed as its own JSON line")
     ap.add_argument("--amr-variant", choices=["both", "spec", "developed", "bins"], default="both")
@@ -75,59 +77,103 @@ def parse():
     return ap.parse_args()
 
 
-def amr_sedov(levels=4, nr=8, radius_cells=3.5, steps=24, cap=26000, grown=False, profile_window=False, time_bins=0,
-              two_pass=False):
-    """3D Sedov blast on the block grid: 16^3-cell blocks, levels 0-levels above nr^3 roots (finest
-    nr * 16 << levels cells per side), E = 1 spread over the finest cells within radius_cells of
-    the centre, Löhner refinement above 0.1 (below 0.05 merges), a refinement check every 8 steps.
-    Zone-updates are leaf cells x steps, the leaves counted at the start and end of the timed run.
-    With per-block timesteps (time_bins) a step is a substep of the cycles (the fastest block's
-    step), so the same figure counts the single-step work the cycles stand for."""
-    from shaderous_b200 import Config, Problem
-    from shaderous_b200.amr import AmrConfig, AmrSim
+def _amr_cfg(levels, nr, cap, time_bins=0, two_pass=False):
+    from shaderous_b200 import Config
+    from shaderous_b200.amr import AmrConfig
 
     hyd = Config(gamma=5 / 3, bc_lo=(1, 1, 1), bc_hi=(1, 1, 1), recon="koren", isentropic=True, cfl=0.5, p_floor=1e-12)
-    cfg = AmrConfig(hydro=hyd, ndim=3, nr=nr, max_level=levels, cap=cap, refine_hi=0.1, refine_lo=0.05, regrid_every=8,
-                    two_pass=two_pass, time_bins=time_bins, time_bins_always=time_bins > 0)
-    t0 = time.perf_counter()
-    with AmrSim(cfg) as a:
-        if grown:
-            # the same energy (E = 1, gamma = 5/3) as a uniform hot sphere of radius 0.2
-            r = 0.2
-            prob = Problem("blast", a=(1.0, (2.0 / 3.0) / (4.0 / 3.0 * math.pi * r ** 3), 1.0, 1e-5, r))
-        else:
-            prob = Problem("sedov", a=(1.0, 1e-5, 1.0, radius_cells))
-        a.reset(prob)
-        t_init = time.perf_counter() - t0
-        # warm-up, including one refinement check (and, with bins, the run's first single steps)
-        a.profile(8 if not time_bins else 16 + (1 << time_bins))
-        if profile_window:
-            # one graph-replayed step between cudaProfilerStart/Stop, for `ncu --profile-from-start off`
-            import torch
+    return AmrConfig(hydro=hyd, ndim=3, nr=nr, max_level=levels, cap=cap, refine_hi=0.1, refine_lo=0.05,
+                     regrid_every=8, two_pass=two_pass, time_bins=time_bins, time_bins_always=time_bins > 0)
 
-            torch.cuda.synchronize()
-            torch.cuda.profiler.start()
-            a.step(1)
-            a.diagnostics()
-            torch.cuda.synchronize()
-            torch.cuda.profiler.stop()
-        n0 = len(a.leaves()[0])
-        l0 = a.kernel_launches
-        prof = a.profile(steps)
-        steps = prof["steps"]
-        n1 = len(a.leaves()[0])
-        _, lv, _ = a.leaves()
-        launches = a.kernel_launches - l0
-        work = a.bin_work() if time_bins else None
+
+def _time_amr(a, steps, time_bins=0, profile_window=False):
+    """Warm-up (one refinement check; with bins the run's first single steps), then `steps` steps
+    timed by CUDA events on the handle's stream. Zone-updates are leaf cells x steps, the leaves
+    counted at the start and end of the timed run; with per-block timesteps a step is a substep
+    of the cycles (the fastest block's step), so the same figure counts the single-step work the
+    cycles stand for."""
+    a.profile(8 if not time_bins else 16 + (1 << time_bins))
+    if profile_window:
+        # one graph-replayed step between cudaProfilerStart/Stop, for `ncu --profile-from-start off`
+        import torch
+
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        a.step(1)
+        a.diagnostics()
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+    n0 = len(a.leaves()[0])
+    l0 = a.kernel_launches
+    prof = a.profile(steps)
+    steps = prof["steps"]
+    _, lv, _ = a.leaves()
+    n1 = len(lv)
+    work = a.bin_work() if time_bins else None
     leaf_cells = 0.5 * (n0 + n1) * 4096
-    extra = {}
-    if work:
-        extra = {"time_bins": time_bins, "block_update_share": work["updates"] / max(work["single"], 1)}
+    extra = {"time_bins": time_bins, "block_update_share": work["updates"] / max(work["single"], 1)} if work else {}
     return {"value": leaf_cells * steps / (prof["total_ms"] / 1000.0), "unit": UNIT, "steps": steps, **extra,
             "ms_per_step": prof["total_ms"] / steps, "leaf_blocks": [n0, n1], "levels": int(lv.max()) + 1,
-            "finest_cells_per_side": nr * 16 << levels, "radius_finest_cells": 0.2 * (nr * 16 << levels) if grown else radius_cells,
-            "init_s": t_init, "gpu_launches": launches,
+            "gpu_launches": a.kernel_launches - l0,
             "note": "time includes the refinement checks (flag, host adapt, regrid) every 8 steps"}
+
+
+def amr_sedov(levels=4, nr=8, radius_cells=3.5, steps=24, cap=26000, profile_window=False, time_bins=0,
+              two_pass=False):
+    """3D Sedov blast on the block grid as configured: 16^3-cell blocks, levels 0-levels above nr^3
+    roots (finest nr * 16 << levels cells per side), E = 1 spread over the finest cells within
+    radius_cells of the centre, Löhner refinement above 0.1 (below 0.05 merges), a refinement
+    check every 8 steps; timed on its initial mesh."""
+    from shaderous_b200 import Problem
+    from shaderous_b200.amr import AmrSim
+
+    t0 = time.perf_counter()
+    with AmrSim(_amr_cfg(levels, nr, cap, time_bins, two_pass)) as a:
+        a.reset(Problem("sedov", a=(1.0, 1e-5, 1.0, radius_cells)))
+        t_init = time.perf_counter() - t0
+        out = _time_amr(a, steps, time_bins, profile_window)
+    out.update({"finest_cells_per_side": nr * 16 << levels, "radius_finest_cells": radius_cells, "init_s": t_init})
+    return out
+
+
+def amr_sedov_developed(levels=4, nr=8, radius_cells=3.5, steps=16, bins_steps=64, cap=26000, target_leaves=20000,
+                        advance_s=330.0, profile_window=False, bins=True):
+    """The same configured Sedov run advanced (untimed) until its mesh holds about `target_leaves`
+    leaves (the blast's shell, refined to the finest level, grows with its radius; about 34,000
+    steps), then timed with one timestep for every block and, restarted on the same mesh, state
+    and clock (shz_amr_reset_mesh), with per-block timesteps (5 bins)."""
+    import numpy as np
+
+    from shaderous_b200 import Problem
+    from shaderous_b200.amr import AmrSim
+
+    out = {}
+    with AmrSim(_amr_cfg(levels, nr, cap)) as a:
+        a.reset(Problem("sedov", a=(1.0, 1e-5, 1.0, radius_cells)))
+        t1 = time.perf_counter()
+        taken = 0
+        while len(a.leaves()[0]) < target_leaves and time.perf_counter() - t1 < advance_s:
+            taken += a.run(steps=256).taken
+        t_sim, _, st = a.clock()
+        advanced = {"steps": taken, "t": t_sim, "leaves": int(len(a.leaves()[0])), "target_leaves": target_leaves,
+                    "seconds": time.perf_counter() - t1}
+        slots, levels_l, coords = a.leaves()
+        u1, u2 = a.leaves_state()
+        t_sim, _, st = a.clock()
+        out["developed"] = _time_amr(a, steps, 0, profile_window)
+        out["developed"]["advanced_before_timing"] = advanced
+    if bins:
+        with AmrSim(_amr_cfg(levels, nr, cap, time_bins=5)) as b:
+            n = nr * 16
+            b.reset_mesh(levels_l, coords, (n, n, n), (16, 16, 16), (-0.5,) * 3, (0.5,) * 3, 0)
+            _, lv2, co2 = b.leaves()
+            where = {(int(l), *map(int, c)): i for i, (l, c) in enumerate(zip(levels_l, coords))}
+            order = np.array([where[(int(l), *map(int, c))] for l, c in zip(lv2, co2)])
+            b.set_leaves_state(u1[order], u2[order])
+            b.set_clock(t_sim, st)
+            out["developed_time_bins"] = _time_amr(b, bins_steps, 5)
+            out["developed_time_bins"]["advanced_before_timing"] = dict(advanced, restarted=True)
+    return out
 
 
 # The reference's published throughputs (WebGPU in Chrome, zone-updates/s) for the same
@@ -161,39 +207,68 @@ def comparable(steps=40):
         v = cfg.ncell * steps / (prof["total_ms"] / 1000.0)
         out[name] = {"value": v, "unit": UNIT, "ms_per_step": prof["total_ms"] / steps, "steps": steps,
                      "scheme": "koren+isentropic+hllc, cfl 0.8", "published_reference": PUBLISHED[name]}
+    # the second configuration as stated: Kelvin-Helmholtz 1024^2, MC + HLLC, CFL 0.4, its 1000
+    # steps timed whole (the run the parity tests hold to the oracle)
+    cfg = Config(n=(1024, 1024, 1), dx=1.0 / 1024, gamma=1.4, cfl=0.4, recon="mc", riemann="hllc", isentropic=False)
+    prob = Problem("kh", a=(2, 1, 0.5, 2.5, 0.01, 1e-3), seed=20240601)
+    with Sim(cfg) as s:
+        s.reset(prob)
+        s.profile(5)  # warm-up (tunes)
+        s.reset(prob)
+        prof = s.profile(1000)
+    out["kh_2d_1024_1000"] = {"value": cfg.ncell * 1000 / (prof["total_ms"] / 1000.0), "unit": UNIT,
+                              "ms_per_step": prof["total_ms"] / 1000, "steps": 1000,
+                              "scheme": "mc+hllc, cfl 0.4 (the configuration as stated)"}
     return out
 
 
-def serving(n_requests=200, seed=2024, budget=150e9):
+SERVE_SIZES = {
+    # the configuration's stream: 64^2-1024^2 (2D) and 32^3-256^3 (3D), 100-2000 steps
+    "config": {"sizes2": (64, 1024), "sizes3": (32, 256), "steps": (100, 2000)},
+    # a reduced stream of small grids, where the plain loop is launch-bound
+    "small": {"sizes2": (64, 512), "sizes3": (32, 128), "steps": (100, 500)},
+}
+
+
+def serving(n_requests=100, seed=2024, budget=150e9, sizes="config"):
     """A seeded stream of Sod / Kelvin-Helmholtz / blast requests with Poisson arrivals, served with
     continuous batching, and the same stream run one request after another through the plain
-    uniform-grid step."""
+    uniform-grid step. Each arm's GPU-busy share (CUDA-event spans over the makespan) says how
+    much of its time the device was working."""
+    from dataclasses import replace
+
     from shaderous_b200.serve import Server, ServerConfig, plain_run_stream, request_stream
 
-    reqs = request_stream(n_requests, seed=seed, rate=100.0, sizes2=(64, 512), sizes3=(32, 128), steps=(100, 500))
+    sz = SERVE_SIZES[sizes]
+    reqs = request_stream(n_requests, seed=seed, rate=100.0, **sz)
     cfg = ServerConfig(budget_bytes=budget, max_grids=512, round_steps=8)
     try:
         srv = Server(cfg)
     except Exception:
         cfg.budget_bytes = budget / 3
         srv = Server(cfg)
-    # warm-up: one untimed pass of the same stream on this server, which fills the launch-shape
-    # tuner's process-wide table for every work-list size the stream reaches (a running server
-    # tunes once, not per stream); the timed pass runs on a fresh server
+    # warm-up: one untimed pass of the same requests, 16 steps each, on this server, which fills
+    # the launch-shape tuner's process-wide table for the work-list sizes the stream reaches (a
+    # running server tunes once, not per stream); the timed pass runs on a fresh server
     with srv:
-        srv.run_stream(reqs)
+        srv.run_stream([replace(r, steps=16) for r in reqs])
     with Server(cfg) as srv:
         batched = srv.run_stream(reqs)
     plain = plain_run_stream(cfg, reqs)
     keep = ["completed", "makespan_s", "p50_s", "p99_s", "mean_s", "zone_updates", "zu_per_s", "max_concurrent",
-            "kernel_launches"]
-    return {"requests": n_requests,
-            "stream": f"seeded (seed {seed}) Poisson arrivals at 100/s; Sod, KH or blast; 2D 64^2-512^2 and 3D "
-                      f"32^3-128^3 log-uniform; 100-500 steps; rho ratio U[1,10], p ratio log-U[1,1000], gamma "
-                      f"1.4 or 5/3; koren+HLLC; budget {cfg.budget_bytes / 1e9:.0f} GB",
-            "warmup": "one untimed pass of the same stream on another server (the launch-shape tuner's table filled)",
-            "batched": {k: batched[k] for k in keep}, "plain": {k: plain[k] for k in keep},
-            "aggregate_speedup": batched["zu_per_s"] / plain["zu_per_s"] if plain["zu_per_s"] else None}
+            "kernel_launches", "busy_s"]
+    out = {"requests": n_requests,
+           "stream": f"seeded (seed {seed}) Poisson arrivals at 100/s; Sod, KH or blast; 2D {sz['sizes2'][0]}^2-"
+                     f"{sz['sizes2'][1]}^2 and 3D {sz['sizes3'][0]}^3-{sz['sizes3'][1]}^3 log-uniform; "
+                     f"{sz['steps'][0]}-{sz['steps'][1]} steps; rho ratio U[1,10], p ratio log-U[1,1000], gamma "
+                     f"1.4 or 5/3; koren+HLLC; budget {cfg.budget_bytes / 1e9:.0f} GB",
+           "sizes": sizes,
+           "warmup": "one untimed pass of the same requests at 16 steps each on another server (the tuner's table)",
+           "batched": {k: batched[k] for k in keep}, "plain": {k: plain[k] for k in keep},
+           "aggregate_speedup": batched["zu_per_s"] / plain["zu_per_s"] if plain["zu_per_s"] else None}
+    for arm in ("batched", "plain"):
+        out[arm]["gpu_busy_share"] = out[arm]["busy_s"] / out[arm]["makespan_s"] if out[arm]["makespan_s"] else None
+    return out
 
 
 def workload(n: int, recon: str):
@@ -529,15 +604,13 @@ def main():
         if args.section == "amr":
             if args.amr_variant in ("both", "spec"):
                 out["spec"] = amr_sedov(steps=max(args.steps, 8), cap=args.amr_cap, profile_window=args.profile_window)
-            if args.amr_variant in ("both", "developed"):
-                out["developed"] = amr_sedov(steps=max(args.steps, 8), grown=True, cap=args.amr_cap,
-                                             profile_window=args.profile_window)
-            if args.amr_variant in ("both", "bins"):
-                out["developed_time_bins"] = amr_sedov(steps=64, grown=True, cap=args.amr_cap, time_bins=5)
+            if args.amr_variant in ("both", "developed", "bins"):
+                out.update(amr_sedov_developed(steps=max(args.steps, 8), cap=args.amr_cap,
+                                               profile_window=args.profile_window, bins=args.amr_variant != "developed"))
         elif args.section == "comparable":
             out = comparable()
         else:
-            out = serving(args.serve_requests)
+            out = serving(args.serve_requests, sizes=args.serve_sizes)
         print(json.dumps({"section": args.section, "result": out}), flush=True)
         return
 
@@ -620,13 +693,12 @@ def main():
     del h_in1, h_in2, h_out1, h_out2
     amr = serve = None
     if rank == 0 and not args.no_amr:
-        amr = {"spec": amr_sedov(), "developed": amr_sedov(steps=16, grown=True)}
-        amr["developed"]["note"] += ("; the same blast with the energy spread within 0.2 of the box, the mesh of the "
-                                     "grown blast (about 20k blocks) that the spec's run reaches later")
-        # per-block timesteps (cycles of 32 substeps): zone-updates counted as single steps would make them
-        amr["developed_time_bins"] = amr_sedov(steps=64, grown=True, time_bins=5)
+        amr = {"spec": amr_sedov()}
+        # the same run advanced to about 20k leaves; then per-block timesteps (cycles of 32
+        # substeps) on that mesh, zone-updates counted as single steps would make them
+        amr.update(amr_sedov_developed(steps=16, bins_steps=64))
     if rank == 0 and not args.no_serving:
-        serve = serving(args.serve_requests)
+        serve = serving(args.serve_requests, sizes=args.serve_sizes)
     comp = comparable() if rank == 0 and not args.no_comparable else None
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:

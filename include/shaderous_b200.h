@@ -434,6 +434,9 @@ typedef struct shz_server_stats {
   int64_t max_concurrent;  /* requests in flight at once, at most */
   int64_t rounds;
   int64_t kernel_launches;
+  double busy_s;           /* GPU-busy seconds (CUDA events): the batched server's rounds (per
+                              round, the longer of its two engines' spans), or the plain loop's
+                              runs; busy_s / makespan_s is the device's busy share */
 } shz_server_stats;
 
 typedef struct shz_server shz_server;

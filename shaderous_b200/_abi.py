@@ -154,6 +154,7 @@ class shz_server_stats(C.Structure):
         ("max_concurrent", C.c_int64),
         ("rounds", C.c_int64),
         ("kernel_launches", C.c_int64),
+        ("busy_s", C.c_double),
     ]
 
 

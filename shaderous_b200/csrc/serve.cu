@@ -77,6 +77,7 @@ struct Engine {
   cudaGraphExec_t graphs[4] = {nullptr, nullptr, nullptr, nullptr};
   long long graph_launches[4] = {0, 0, 0, 0};  // kernels one replay of each graph launches
   cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // a round's span on this engine's stream
   shz::AmrLaunch L{};
   long long launches = 0;
   int64_t slot_bytes() const { return (int64_t)(4 * CB + 2 * WN) * 16; }
@@ -95,6 +96,7 @@ struct shz_server {
   Clock::time_point t0 = Clock::now();
   long long rounds = 0;
   long long max_concurrent = 0;
+  double busy_s = 0;  // GPU seconds of the rounds: per round the longer engine's event span
 };
 
 namespace {
@@ -203,6 +205,8 @@ void engine_free(Engine& e) {
   for (void* x : b)
     if (x) cudaFree(x);
   if (e.stream) cudaStreamDestroy(e.stream);
+  if (e.ev0) cudaEventDestroy(e.ev0);
+  if (e.ev1) cudaEventDestroy(e.ev1);
   if (e.h_clk) cudaFreeHost(e.h_clk);
   e = Engine();
 }
@@ -469,8 +473,17 @@ int finish(shz_server* s, Engine& e, Grid& G) {
 // admit.
 int round_once(shz_server* s) {
   int rc = 0;
-  for (Engine& e : s->e)
+  bool timed[2] = {false, false};
+  for (int k = 0; k < 2; k++) {
+    Engine& e = s->e[k];
+    if (!e.stream || e.active.empty()) continue;
+    if (!e.ev0) SV_CUDA(s, cudaEventCreate(&e.ev0));
+    if (!e.ev1) SV_CUDA(s, cudaEventCreate(&e.ev1));
+    SV_CUDA(s, cudaEventRecord(e.ev0, e.stream));
     if ((rc = launch_round(s, e))) return rc;
+    SV_CUDA(s, cudaEventRecord(e.ev1, e.stream));
+    timed[k] = true;
+  }
   // stage queued requests (host work overlapping the round)
   for (Grid* G : s->pending)
     if (!G->staged) {
@@ -488,6 +501,12 @@ int round_once(shz_server* s) {
     }
   }
   s->rounds++;
+  float span = 0.f;
+  for (int k = 0; k < 2; k++) {
+    float ms = 0.f;
+    if (timed[k] && cudaEventElapsedTime(&ms, s->e[k].ev0, s->e[k].ev1) == cudaSuccess) span = std::max(span, ms);
+  }
+  s->busy_s += span / 1000.0;
   for (Engine& e : s->e) {
     std::vector<Grid*> done;
     for (Grid* G : e.active) {
@@ -540,7 +559,7 @@ Grid* enqueue(shz_server* s, const shz_request& r, double arrival) {
 }
 
 void fill_stats(const std::vector<Grid*>& gs, double t_first, long long rounds, long long maxc, long long launches,
-                shz_server_stats* out) {
+                double busy_s, shz_server_stats* out) {
   std::vector<double> lat;
   double zu = 0, last = t_first;
   for (const Grid* G : gs) {
@@ -568,6 +587,7 @@ void fill_stats(const std::vector<Grid*>& gs, double t_first, long long rounds, 
   out->max_concurrent = maxc;
   out->rounds = rounds;
   out->kernel_launches = launches;
+  out->busy_s = busy_s;
 }
 
 }  // namespace
@@ -657,6 +677,7 @@ int shz_server_run_stream(shz_server* s, const shz_request* reqs, int32_t n, shz
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return reqs[a].arrival < reqs[b].arrival; });
   const double base = now_s(s);
   const long long r0 = s->rounds;
+  const double busy0 = s->busy_s;
   long long l0 = s->e[0].launches + s->e[1].launches;
   s->max_concurrent = 0;
   std::vector<Grid*> mine;
@@ -686,7 +707,7 @@ int shz_server_run_stream(shz_server* s, const shz_request* reqs, int32_t n, shz
     if (rc) return rc;
   }
   fill_stats(mine, base + (n ? reqs[order[0]].arrival : 0.0), s->rounds - r0, s->max_concurrent,
-             s->e[0].launches + s->e[1].launches - l0, out);
+             s->e[0].launches + s->e[1].launches - l0, s->busy_s - busy0, out);
   return 0;
 }
 
@@ -754,6 +775,7 @@ int shz_plain_run_stream(const shz_server_config* cfg, const shz_request* reqs, 
   std::vector<std::unique_ptr<Grid>> gs;
   std::vector<Grid*> ptrs;
   long long launches = 0;
+  double busy = 0;
   for (int i : order) {
     const shz_request& r = reqs[i];
     const double wait = r.arrival - now();
@@ -777,7 +799,20 @@ int shz_plain_run_stream(const shz_server_config* cfg, const shz_request* reqs, 
     }
     shz_run_opts o{r.steps, std::numeric_limits<double>::quiet_NaN(), 0.0};
     shz_run_result res;
+    // the run's span on the handle's stream: the GPU-busy part of this request
+    void* sv = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    const bool timed = shz_stream(sim, &sv) == 0 && cudaEventCreate(&e0) == cudaSuccess &&
+                       cudaEventCreate(&e1) == cudaSuccess;
+    if (timed) cudaEventRecord(e0, static_cast<cudaStream_t>(sv));
     rc = shz_run(sim, &o, &res);
+    if (timed) {
+      cudaEventRecord(e1, static_cast<cudaStream_t>(sv));
+      float ms = 0.f;
+      if (cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess) busy += ms / 1000.0;
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
     launches += shz_kernel_launches(sim);
     shz_destroy(sim);
     if (rc) return rc;
@@ -788,7 +823,7 @@ int shz_plain_run_stream(const shz_server_config* cfg, const shz_request* reqs, 
     ptrs.push_back(G.get());
     gs.push_back(std::move(G));
   }
-  fill_stats(ptrs, n ? reqs[order[0]].arrival : 0.0, 0, 1, launches, out);
+  fill_stats(ptrs, n ? reqs[order[0]].arrival : 0.0, 0, 1, launches, busy, out);
   return 0;
 }
 
