@@ -422,6 +422,10 @@ typedef struct shz_server_config {
   int32_t max_grids;     /* requests in flight at most */
   int32_t round_steps;   /* steps between admission and completion checks */
   int32_t keep_states;   /* 1: keep each finished request's state for shz_server_state */
+  int32_t direct_large;  /* 1: a request of at least 2^18 cells (2D) or 2^21 (3D) runs as a uniform
+                            grid (the fused sweep) on a stream of its own, its steps enqueued in the
+                            same rounds as the batched blocks, within a quarter of the budget; 0:
+                            every request on the block passes */
 } shz_server_config;
 
 typedef struct shz_server_stats {

@@ -139,6 +139,7 @@ class shz_server_config(C.Structure):
         ("max_grids", C.c_int32),
         ("round_steps", C.c_int32),
         ("keep_states", C.c_int32),
+        ("direct_large", C.c_int32),
     ]
 
 

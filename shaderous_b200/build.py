@@ -40,7 +40,14 @@ def _stale(target: Path, deps: list[Path]) -> bool:
     return any(d.stat().st_mtime > t for d in deps)
 
 
-def _compile(src: Path, obj: Path, verbose: bool) -> None:
+def _newest(paths: list[Path]) -> float:
+    return max(p.stat().st_mtime for p in paths)
+
+
+def _compile(src: Path, obj: Path, verbose: bool, deps: list[Path] = ()) -> None:
+    # the object is stamped with the newest input's time as read before compiling, so an input
+    # edited while the compiler runs still makes the object stale
+    stamp = _newest([src, *deps])
     cmd = [NVCC, "-O3", "-std=c++17", *ARCH, "-lineinfo", "--use_fast_math", "-Xcompiler", "-fPIC,-fopenmp,-O3",
            "-I", str(ROOT / "include"), "-c", str(src), "-o", str(obj)]
     if src.suffix == ".cu":
@@ -48,6 +55,7 @@ def _compile(src: Path, obj: Path, verbose: bool) -> None:
     else:
         cmd[1:1] = ["-x", "cu"]
     subprocess.run(cmd, check=True)
+    os.utime(obj, (stamp, stamp))
 
 
 def build_library(force: bool = False, verbose: bool = False) -> Path:
@@ -61,7 +69,7 @@ def build_library(force: bool = False, verbose: bool = False) -> Path:
     todo = [(s, o) for s, o in zip(srcs, objs) if force or _stale(o, [s] + deps)]
     if todo:
         with ThreadPoolExecutor(max_workers=max(1, os.cpu_count() or 1)) as pool:
-            for f in [pool.submit(_compile, s, o, verbose) for s, o in todo]:
+            for f in [pool.submit(_compile, s, o, verbose, deps) for s, o in todo]:
                 f.result()
     if todo or force or _stale(LIB, objs):
         tmp = LIB.with_suffix(".so.tmp")

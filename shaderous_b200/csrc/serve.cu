@@ -49,6 +49,13 @@ struct Grid {
   double arrival = 0, finished = 0;
   bool done = false;
   bool cancelled = false;  // shz_server_cancel took it off the queue or the device
+  // A large request run as a uniform grid (direct_large): its handle, the steps enqueued so far,
+  // its device bytes, and its span's events for the busy time.
+  bool direct = false;
+  shz_sim* sim = nullptr;
+  int enq = 0;
+  double bytes = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   shz_diag diag{};
   std::vector<float> out1, out2;      // final state (keep_states), uniform layout
 };
@@ -96,7 +103,12 @@ struct shz_server {
   Clock::time_point t0 = Clock::now();
   long long rounds = 0;
   long long max_concurrent = 0;
-  double busy_s = 0;  // GPU seconds of the rounds: per round the longer engine's event span
+  double busy_s = 0;  // GPU seconds of the rounds: per round the longest stream's event span
+  // large requests run as uniform grids (direct_large): the running ones, their device bytes
+  // against their share of the budget, and the kernels their handles launched
+  std::vector<Grid*> direct;
+  double direct_budget = 0, direct_used = 0;
+  long long direct_launches = 0;
 };
 
 namespace {
@@ -132,6 +144,18 @@ struct Dev {
 };
 
 double now_s(const shz_server* s) { return std::chrono::duration<double>(Clock::now() - s->t0).count(); }
+
+// Requests this large run as uniform grids when the server has direct_large: the fused sweep of a
+// whole grid fills the GPU at these sizes, where the block passes' ghost-filled atlases cost more.
+constexpr int DIRECT_MAX = 8;  // uniform grids running at once
+bool direct_size(const shz_request& r) {
+  const double cells = std::pow((double)r.n, r.ndim);
+  return cells >= (r.ndim == 3 ? (double)(1 << 21) : (double)(1 << 18));
+}
+// Device bytes of a request run as a uniform grid: two parities of (u1, u2), and the handle's rest.
+double direct_bytes(const shz_request& r) { return std::pow((double)r.n, r.ndim) * 64.0 + (16 << 20); }
+
+bool running(const shz_server* s) { return !s->e[0].active.empty() || !s->e[1].active.empty() || !s->direct.empty(); }
 
 void drop_graphs(Engine& e) {
   for (auto& g : e.graphs)
@@ -225,7 +249,9 @@ void grid_rows(const shz_request& r, Grid& G) {
 // Sample the initial condition into the staging buffers, local block order; the cell numbering
 // of the seeded noise is the uniform grid's, so a request starts from the state the plain
 // uniform-grid step would.
+void stage_uniform(const shz_server* s, Grid& G);
 void stage_grid(const shz_server* s, Grid& G) {
+  if (G.direct) return stage_uniform(s, G);
   const shz_request& r = G.req;
   const int n = r.n, nd = r.ndim, nr = n / BS, CB = nd == 3 ? 4096 : 256;
   shz_config c = s->cfg.hydro;
@@ -255,6 +281,38 @@ void stage_grid(const shz_server* s, Grid& G) {
   G.staged = true;
 }
 
+// A direct request's initial state in the uniform grid's layout (x fastest), sampled as
+// stage_grid samples it.
+void stage_uniform(const shz_server* s, Grid& G) {
+  const shz_request& r = G.req;
+  const int n = r.n, nd = r.ndim;
+  shz_config c = s->cfg.hydro;
+  c.n[0] = n;
+  c.n[1] = n;
+  c.n[2] = nd == 3 ? n : 1;
+  c.dx = 1.0 / n;
+  c.gamma = r.gamma;
+  const shz::ProblemCtx q = shz::prepare_problem(c, r.problem);
+  const size_t cells = (size_t)n * n * (nd == 3 ? n : 1);
+  G.s1.resize(cells);
+  G.s2.resize(cells);
+  const double dx = 1.0 / n;
+#pragma omp parallel for schedule(static)
+  for (long long row = 0; row < (long long)n * (nd == 3 ? n : 1); row++) {
+    const int j = (int)(row % n), k = (int)(row / n);
+    for (int i = 0; i < n; i++) {
+      const double x = (i + 0.5 - n / 2.0) * dx, y = (j + 0.5 - n / 2.0) * dx, z = nd == 3 ? (k + 0.5 - n / 2.0) * dx : 0.0;
+      const uint64_t cell = ((uint64_t)k * n + j) * n + i;
+      double w[6];
+      shz::sample_problem(q, x, y, z, cell, w);
+      const double rho = w[0], eint = w[4] / (r.gamma - 1), ke = 0.5 * rho * (w[1] * w[1] + w[2] * w[2] + w[3] * w[3]);
+      G.s1[cell] = make_float4((float)rho, (float)(rho * w[1]), (float)(rho * w[2]), (float)(rho * w[3]));
+      G.s2[cell] = make_float4((float)(eint + ke), (float)eint, (float)(rho * w[5]), 0.f);
+    }
+  }
+  G.staged = true;
+}
+
 // Copy runs of consecutive global slots in one call each.
 int upload_blocks(shz_server* s, Engine& e, Grid& G, float4* d1, float4* d2) {
   int b = 0;
@@ -270,7 +328,79 @@ int upload_blocks(shz_server* s, Engine& e, Grid& G, float4* d1, float4* d2) {
 }
 
 // Admit a staged request: slots, parameters, clock, state.
+// A direct request onto the GPU: its handle (the scheme of the server's config, the request's
+// size, gamma and boundaries), its staged state uploaded.
+int admit_direct(shz_server* s, Grid& G) {
+  const shz_request& r = G.req;
+  shz_config c = s->cfg.hydro;
+  c.n[0] = r.n;
+  c.n[1] = r.n;
+  c.n[2] = r.ndim == 3 ? r.n : 1;
+  c.dx = 1.0 / r.n;
+  c.gamma = r.gamma;
+  c.t_end = HUGE_VAL;
+  for (int a = 0; a < 3; a++) {
+    c.bc_lo[a] = a < r.ndim ? r.bc : 0;
+    c.bc_hi[a] = a < r.ndim ? r.bc : 0;
+  }
+  c.device = s->device;
+  int rc = shz_create(&c, &G.sim);
+  if (rc) return fail(s, rc, "request %lld: %s", (long long)G.id, shz_last_error(nullptr));
+  const size_t cells = G.s1.size();
+  if ((rc = shz_set_state(G.sim, reinterpret_cast<const float*>(G.s1.data()), reinterpret_cast<const float*>(G.s2.data()),
+                          cells)))
+    return fail(s, rc, "request %lld: %s", (long long)G.id, shz_last_error(G.sim));
+  SV_CUDA(s, cudaEventCreate(&G.ev0));
+  SV_CUDA(s, cudaEventCreate(&G.ev1));
+  G.s1.clear();
+  G.s1.shrink_to_fit();
+  G.s2.clear();
+  G.s2.shrink_to_fit();
+  G.enq = 0;
+  s->direct_used += G.bytes;
+  s->direct.push_back(&G);
+  return 0;
+}
+
+// Whether the request fits what is free now.
+bool fits(const shz_server* s, const Grid& G) {
+  if (G.direct) return (int)s->direct.size() < DIRECT_MAX && s->direct_used + G.bytes <= s->direct_budget;
+  const Engine& e = s->e[G.eng];
+  return (int)e.free_slots.size() >= G.nblocks && !e.free_g.empty();
+}
+
+void release_direct(shz_server* s, Grid& G) {
+  if (G.sim) {
+    s->direct_launches += shz_kernel_launches(G.sim);
+    shz_destroy(G.sim);
+    G.sim = nullptr;
+  }
+  if (G.ev0) cudaEventDestroy(G.ev0);
+  if (G.ev1) cudaEventDestroy(G.ev1);
+  G.ev0 = G.ev1 = nullptr;
+  s->direct_used -= G.bytes;
+  s->direct.erase(std::find(s->direct.begin(), s->direct.end(), &G));
+}
+
+// A direct request that took its steps: its totals (and state), then its handle freed.
+int finish_direct(shz_server* s, Grid& G) {
+  int rc = shz_diagnostics(G.sim, &G.diag);
+  if (rc) return fail(s, rc, "request %lld: %s", (long long)G.id, shz_last_error(G.sim));
+  if (s->cfg.keep_states) {
+    const size_t cells = (size_t)G.req.n * G.req.n * (G.req.ndim == 3 ? G.req.n : 1);
+    G.out1.resize(cells * 4);
+    G.out2.resize(cells * 4);
+    if ((rc = shz_get_state(G.sim, G.out1.data(), G.out2.data(), cells)))
+      return fail(s, rc, "request %lld: %s", (long long)G.id, shz_last_error(G.sim));
+  }
+  release_direct(s, G);
+  G.done = true;
+  G.finished = now_s(s);
+  return 0;
+}
+
 int admit(shz_server* s, Grid& G) {
+  if (G.direct) return admit_direct(s, G);
   Engine& e = s->e[G.eng];
   const shz_request& r = G.req;
   for (int b = 0; b < G.nblocks; b++) {
@@ -473,6 +603,17 @@ int finish(shz_server* s, Engine& e, Grid& G) {
 // admit.
 int round_once(shz_server* s) {
   int rc = 0;
+  // the direct requests' steps first, each on its handle's stream, so that they overlap the
+  // batched blocks' round
+  for (Grid* G : s->direct) {
+    const int k = std::min(s->cfg.round_steps, G->req.steps - G->enq);
+    void* sv = nullptr;
+    shz_stream(G->sim, &sv);
+    SV_CUDA(s, cudaEventRecord(G->ev0, static_cast<cudaStream_t>(sv)));
+    if (k > 0 && (rc = shz_step(G->sim, k))) return fail(s, rc, "request %lld: %s", (long long)G->id, shz_last_error(G->sim));
+    SV_CUDA(s, cudaEventRecord(G->ev1, static_cast<cudaStream_t>(sv)));
+    G->enq += std::max(k, 0);
+  }
   bool timed[2] = {false, false};
   for (int k = 0; k < 2; k++) {
     Engine& e = s->e[k];
@@ -506,6 +647,17 @@ int round_once(shz_server* s) {
     float ms = 0.f;
     if (timed[k] && cudaEventElapsedTime(&ms, s->e[k].ev0, s->e[k].ev1) == cudaSuccess) span = std::max(span, ms);
   }
+  {
+    std::vector<Grid*> done;
+    for (Grid* G : s->direct) {
+      float ms = 0.f;
+      SV_CUDA(s, cudaEventSynchronize(G->ev1));
+      if (cudaEventElapsedTime(&ms, G->ev0, G->ev1) == cudaSuccess) span = std::max(span, ms);
+      if (G->enq >= G->req.steps) done.push_back(G);
+    }
+    for (Grid* G : done)
+      if ((rc = finish_direct(s, *G))) return rc;
+  }
   s->busy_s += span / 1000.0;
   for (Engine& e : s->e) {
     std::vector<Grid*> done;
@@ -520,13 +672,12 @@ int round_once(shz_server* s) {
   // admit in arrival order while the head of the queue fits
   while (!s->pending.empty()) {
     Grid* G = s->pending.front();
-    Engine& e = s->e[G->eng];
-    if ((int)e.free_slots.size() < G->nblocks || e.free_g.empty()) break;
+    if (!fits(s, *G)) break;
     if (!G->staged) stage_grid(s, *G);
     if ((rc = admit(s, *G))) return rc;
     s->pending.pop_front();
   }
-  long long live = (long long)(s->e[0].active.size() + s->e[1].active.size());
+  long long live = (long long)(s->e[0].active.size() + s->e[1].active.size() + s->direct.size());
   s->max_concurrent = std::max(s->max_concurrent, live);
   return 0;
 }
@@ -538,6 +689,10 @@ int validate_request(const shz_server* s, const shz_request& r, std::string& why
   if (r.bc < 0 || r.bc > 2) { why = "bc must be 0, 1 or 2"; return -1; }
   if (!(r.gamma > 1)) { why = "gamma must exceed 1"; return -1; }
   if (!shz::problem_known(r.problem.kind)) { why = "unknown problem"; return -1; }
+  if (s->cfg.direct_large && direct_size(r)) {
+    if (direct_bytes(r) > s->direct_budget) { why = "the request is larger than the budget for large requests"; return -1; }
+    return 0;
+  }
   const Engine& e = s->e[r.ndim == 3 ? 1 : 0];
   const int nr = r.n / BS;
   const int64_t nb = (int64_t)nr * nr * (r.ndim == 3 ? nr : 1);
@@ -551,7 +706,9 @@ Grid* enqueue(shz_server* s, const shz_request& r, double arrival) {
   G->req = r;
   G->eng = r.ndim == 3 ? 1 : 0;
   G->arrival = arrival;
-  grid_rows(r, *G);
+  G->direct = s->cfg.direct_large && direct_size(r);
+  if (G->direct) G->bytes = direct_bytes(r);
+  else grid_rows(r, *G);
   Grid* p = G.get();
   s->grids[p->id] = std::move(G);
   s->pending.push_back(p);
@@ -616,9 +773,12 @@ int shz_server_create(const shz_server_config* cfg, shz_server** out) {
   shz_server* s = new shz_server();
   s->cfg = *cfg;
   s->device = cfg->hydro.device;
-  // a sixth of the budget for 2D requests, the rest for 3D
-  int rc = engine_init(s, s->e[0], 2, cfg->budget_bytes / 6.0);
-  if (!rc) rc = engine_init(s, s->e[1], 3, cfg->budget_bytes * 5.0 / 6.0);
+  // a sixth of the budget for 2D requests, the rest for 3D; with direct_large a quarter of it is
+  // kept for the large requests' uniform grids, the rest split so
+  const double blocks_budget = cfg->direct_large ? cfg->budget_bytes * 0.75 : cfg->budget_bytes;
+  s->direct_budget = cfg->direct_large ? cfg->budget_bytes * 0.25 : 0.0;
+  int rc = engine_init(s, s->e[0], 2, blocks_budget / 6.0);
+  if (!rc) rc = engine_init(s, s->e[1], 3, blocks_budget * 5.0 / 6.0);
   if (rc) {
     g_create_err = s->err;
     shz_server_destroy(s);
@@ -631,6 +791,7 @@ int shz_server_create(const shz_server_config* cfg, shz_server** out) {
 void shz_server_destroy(shz_server* s) {
   if (!s) return;
   Dev dv(s->device);
+  while (!s->direct.empty()) release_direct(s, *s->direct.back());
   for (Engine& e : s->e) engine_free(e);
   delete s;
 }
@@ -648,8 +809,8 @@ int shz_server_drain(shz_server* s, int32_t max_rounds) {
   if (!s) return SHZ_E_CONFIG;
   Dev dv(s->device);
   int rounds = 0;
-  while (!s->pending.empty() || !s->e[0].active.empty() || !s->e[1].active.empty()) {
-    if (s->e[0].active.empty() && s->e[1].active.empty()) {
+  while (!s->pending.empty() || running(s)) {
+    if (!running(s)) {
       // nothing running: admit the head of the queue
       Grid* G = s->pending.front();
       if (!G->staged) stage_grid(s, *G);
@@ -678,17 +839,17 @@ int shz_server_run_stream(shz_server* s, const shz_request* reqs, int32_t n, shz
   const double base = now_s(s);
   const long long r0 = s->rounds;
   const double busy0 = s->busy_s;
-  long long l0 = s->e[0].launches + s->e[1].launches;
+  long long l0 = s->e[0].launches + s->e[1].launches + s->direct_launches;
   s->max_concurrent = 0;
   std::vector<Grid*> mine;
   size_t next = 0;
-  while (next < order.size() || !s->pending.empty() || !s->e[0].active.empty() || !s->e[1].active.empty()) {
+  while (next < order.size() || !s->pending.empty() || running(s)) {
     const double t = now_s(s) - base;
     while (next < order.size() && reqs[order[next]].arrival <= t) {
       mine.push_back(enqueue(s, reqs[order[next]], base + reqs[order[next]].arrival));
       next++;
     }
-    if (s->e[0].active.empty() && s->e[1].active.empty()) {
+    if (!running(s)) {
       if (!s->pending.empty()) {
         Grid* G = s->pending.front();
         if (!G->staged) stage_grid(s, *G);
@@ -707,7 +868,7 @@ int shz_server_run_stream(shz_server* s, const shz_request* reqs, int32_t n, shz
     if (rc) return rc;
   }
   fill_stats(mine, base + (n ? reqs[order[0]].arrival : 0.0), s->rounds - r0, s->max_concurrent,
-             s->e[0].launches + s->e[1].launches - l0, s->busy_s - busy0, out);
+             s->e[0].launches + s->e[1].launches + s->direct_launches - l0, s->busy_s - busy0, out);
   return 0;
 }
 
@@ -721,6 +882,12 @@ int shz_server_cancel(shz_server* s, int64_t id) {
   auto q = std::find(s->pending.begin(), s->pending.end(), &G);
   if (q != s->pending.end()) {
     s->pending.erase(q);
+    G.s1.clear();
+    G.s1.shrink_to_fit();
+    G.s2.clear();
+    G.s2.shrink_to_fit();
+  } else if (G.direct) {
+    release_direct(s, G);  // its handle's work is done between calls: freed at once
   } else {
     // admitted: no round is in flight between calls, so its slots and clock go back at once
     Engine& e = s->e[G.eng];

@@ -42,12 +42,14 @@ class ServerConfig:
     max_grids: int = 256
     round_steps: int = 8
     keep_states: bool = False
+    direct_large: bool = True  # large requests run as uniform grids on streams of their own
 
     def to_c(self) -> _abi.shz_server_config:
         c = _abi.shz_server_config()
         c.hydro = self.hydro.to_c()
         c.budget_bytes = float(self.budget_bytes)
         c.max_grids, c.round_steps, c.keep_states = self.max_grids, self.round_steps, 1 if self.keep_states else 0
+        c.direct_large = 1 if self.direct_large else 0
         return c
 
 

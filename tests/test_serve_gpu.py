@@ -73,3 +73,38 @@ def test_refuses_bad_requests():
             s.submit(Request(ndim=3, n=40, steps=5, problem=Problem("blast", a=(1, 10, 1, 1, 0.1))))
         with pytest.raises(ShaderousError):
             s.submit(Request(ndim=3, n=512, steps=5, problem=Problem("blast", a=(1, 10, 1, 1, 0.1))))
+
+
+def test_large_requests_run_as_uniform_grids_with_the_plain_steps_bits():
+    """With direct_large (the default), requests of at least 2^18 (2D) or 2^21 (3D) cells run as
+    uniform grids on streams of their own, their steps enqueued in the same rounds as the batched
+    blocks of the small requests; each large result equals the plain uniform-grid step's bit for
+    bit, and the small ones are unchanged by the mix."""
+    big = [
+        Request(ndim=3, n=128, steps=21, problem=Problem("blast", a=(3, 50, 1, 1, 0.15)), gamma=5 / 3, bc=1),
+        Request(ndim=2, n=512, steps=33, problem=Problem("kh", a=(2, 1, 0.5, 2.5, 0.01, 1e-3), seed=9), gamma=1.4,
+                bc=0),
+    ]
+    small = _mix()[:2]
+    reqs = big + small
+    with Server(_cfg()) as s:
+        ids = [s.submit(r) for r in reqs]
+        s.drain()
+        got = {i: s.state(i, r) for r, i in zip(reqs, ids)}
+        for r, i in zip(reqs, ids):
+            assert s.result(i).steps == r.steps
+    for r, i in zip(big, ids[:2]):
+        c = Config(n=(r.n, r.n, r.n if r.ndim == 3 else 1), dx=1.0 / r.n, gamma=r.gamma, recon="koren", isentropic=True,
+                   cfl=0.4, bc_lo=tuple(r.bc if a < r.ndim else 0 for a in range(3)),
+                   bc_hi=tuple(r.bc if a < r.ndim else 0 for a in range(3)))
+        with Sim(c) as p:
+            p.reset(r.problem)
+            p.run(steps=r.steps)
+            u1, u2 = p.read_state()
+        assert np.array_equal(got[i][0], u1) and np.array_equal(got[i][1], u2), r
+    with Server(_cfg()) as s:
+        for r, i in zip(small, ids[2:]):
+            j = s.submit(r)
+            s.drain()
+            a1, a2 = s.state(j, r)
+            assert np.array_equal(a1, got[i][0]) and np.array_equal(a2, got[i][1])
