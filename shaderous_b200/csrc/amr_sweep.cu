@@ -88,7 +88,7 @@ __device__ __noinline__ void predict_texel(const KParams& P, const int* __restri
     }
   }
   float c[7], sua[DIM][6], sda[DIM][6];
-  float conv = 0.f, jump = 0.f;
+  float conv = 0.f, jump = -INFINITY;
   load_w7<DIM>(w1, w2, slot, l, c);
 #pragma unroll
   for (int a = 0; a < DIM; a++) {
@@ -100,7 +100,7 @@ __device__ __noinline__ void predict_texel(const KParams& P, const int* __restri
     load_w6<DIM>(w1, w2, slot, lp, p);
     axis_edges<R, ISEN>(m, m, c, p, p, P.inv_gamma, sua[a], sda[a]);
     conv += p[1 + a] - m[1 + a];
-    jump = fmaxf(jump, fabsf(p[4] - m[4]) / fminf(p[4], m[4]));
+    jump = fmaxf(jump, jump_excess(m[4], p[4], P.shock_thresh));
   }
   hancock_masked<DIM>(c, conv, jump, sua, sda, mask, h, P, pr);
   pr.q[1] *= flip[0];
@@ -447,27 +447,27 @@ __global__ void __maxnreg__(80)
       float c[7];
       read_w7(pj, lx, ly, c);
       float su[DIM][6], sd[DIM][6];
-      float conv = 0.f, jump = 0.f;
+      float conv = 0.f, jump = -INFINITY;
       {
         float m[7], p[7];
         read_w7(pj, lx - 1, ly, m);
         read_w7(pj, lx + 1, ly, p);
         axis_edges<R, ISEN>(m, m, c, p, p, P.inv_gamma, su[0], sd[0]);
         conv += p[1] - m[1];
-        jump = fmaxf(jump, fabsf(p[4] - m[4]) / fminf(p[4], m[4]));
+        jump = fmaxf(jump, jump_excess(m[4], p[4], P.shock_thresh));
         if constexpr (DIM >= 2) {
           read_w7(pj, lx, ly - 1, m);
           read_w7(pj, lx, ly + 1, p);
           axis_edges<R, ISEN>(m, m, c, p, p, P.inv_gamma, su[1], sd[1]);
           conv += p[2] - m[2];
-          jump = fmaxf(jump, fabsf(p[4] - m[4]) / fminf(p[4], m[4]));
+          jump = fmaxf(jump, jump_excess(m[4], p[4], P.shock_thresh));
         }
         if constexpr (DIM == 3) {
           read_w7(ring(j - 1), lx, ly, m);
           read_w7(ring(j + 1), lx, ly, p);
           axis_edges<R, ISEN>(m, m, c, p, p, P.inv_gamma, su[2], sd[2]);
           conv += p[3] - m[3];
-          jump = fmaxf(jump, fabsf(p[4] - m[4]) / fminf(p[4], m[4]));
+          jump = fmaxf(jump, jump_excess(m[4], p[4], P.shock_thresh));
         }
       }
       // a ghost beside a coarser block: the slopes along the face's transverse axes dropped at

@@ -46,7 +46,7 @@ __global__ void __launch_bounds__(NT) amr_predict(const KParams* __restrict__ gp
       float c[7];
       load_w<DIM>(w1, w2, src, c0, c);
       float su[DIM][6], sd[DIM][6];
-      float conv = 0.f, jump = 0.f;
+      float conv = 0.f, jump = -INFINITY;
 #pragma unroll
       for (int a = 0; a < DIM; a++) {
         float m[7], p[7];
@@ -57,7 +57,7 @@ __global__ void __launch_bounds__(NT) amr_predict(const KParams* __restrict__ gp
         load_w<DIM>(w1, w2, src, lp, p);
         axis_edges<R, ISEN>(m, m, c, p, p, P.inv_gamma, su[a], sd[a]);
         conv += p[1 + a] - m[1 + a];
-        jump = fmaxf(jump, fabsf(p[4] - m[4]) / fminf(p[4], m[4]));
+        jump = fmaxf(jump, jump_excess(m[4], p[4], P.shock_thresh));
       }
       Pred pr;
       hancock_masked<DIM>(c, conv, jump, su, sd, mask, h, P, pr);

@@ -13,8 +13,16 @@ struct Pred {
   bool fo;
 };
 
+// The shock detector's pressure jump along one axis (hydro.ts:300-303: |p+ - p-| / min(p+, p-)
+// above the threshold), as its excess over the threshold: |p+ - p-| - threshold min(p+, p-), which
+// is positive exactly where the ratio exceeds it (the pressures are floored, so positive), without
+// the division. The largest over the axes decides.
+__device__ __forceinline__ float jump_excess(float pm, float pp, float thresh) {
+  return fabsf(pp - pm) - thresh * fminf(pp, pm);
+}
+
 // hydro.ts:294-321: slopes -> shock flag -> Hancock half step -> positivity fallback, given the
-// edge increments su/sd per active axis and the convergence and pressure jump the neighbours give.
+// edge increments su/sd per active axis, the convergence, and the largest jump_excess over the axes.
 template <int DIM>
 __device__ __forceinline__ void hancock(const float* c, float conv, float jump, const float (*su)[6], const float (*sd)[6],
                                         float h, const KParams& P, Pred& out) {
@@ -31,7 +39,7 @@ __device__ __forceinline__ void hancock(const float* c, float conv, float jump, 
     dv += 0.5f * (su[a][1 + a] + sd[a][1 + a]);
     gradp[a] = 0.5f * (su[a][4] + sd[a][4]);
   }
-  out.flag = (conv < 0.f && jump > P.shock_thresh) ? 1.f : 0.f;
+  out.flag = ((conv < 0.f) & (jump > 0.f)) ? 1.f : 0.f;
   const float rho = c[0], cs = c[6];
   const float inv_rho = 1.f / rho;
   float qh[6];
@@ -103,7 +111,7 @@ __device__ __forceinline__ void hancock_masked(const float* c, float conv, float
     dv += k * (su[a][1 + a] + sd[a][1 + a]);
     gradp[a] = k * (su[a][4] + sd[a][4]);
   }
-  out.flag = (conv < 0.f && jump > P.shock_thresh) ? 1.f : 0.f;
+  out.flag = ((conv < 0.f) & (jump > 0.f)) ? 1.f : 0.f;
   const float rho = c[0], cs = c[6];
   const float inv_rho = 1.f / rho;
   float qh[6];

@@ -36,7 +36,8 @@ struct DevClock {
   int bad;
 };
 
-__device__ __forceinline__ bool same_sign(float a, float b) { return (a > 0.f && b > 0.f) || (a < 0.f && b < 0.f); }
+// (Bitwise & and | rather than && and ||: no short-circuit, so no branch; the same values.)
+__device__ __forceinline__ bool same_sign(float a, float b) { return ((a > 0.f) & (b > 0.f)) | ((a < 0.f) & (b < 0.f)); }
 
 // hydro.ts:30-46 LIMITERS: the edge increment from the differences (far, near) and the
 // quantity's natural scale (Koren only). The product test a*b > 0 is taken by signs, which is
@@ -112,10 +113,15 @@ __device__ __forceinline__ void isen_blend(const float* m, const float* c, const
 // Colella & Woodward (1984) parabola edges (their eqs. 1.6, 1.8 and 1.10) from five cells;
 // no counterpart in the reference. Returns twice the increments toward the upper face and
 // from the lower face, in the reference's edge-increment convention (hydro.ts:282-293).
-__device__ __forceinline__ float ppm_slope(float am, float a, float ap) {
-  const float d = 0.5f * (ap - am);
-  return same_sign(ap - a, a - am) ? copysignf(fminf(fabsf(d), fminf(2.f * fabsf(a - am), 2.f * fabsf(ap - a))), d) : 0.f;
+// The limited slope (eq. 1.8) from the differences toward the cell (dl = a - a_-) and away from
+// it (dr = a_+ - a); a cell's two differences are its neighbours' too, so they are formed once.
+// The test for an extremum is the product's sign, as the oracle's restatement forms it.
+__device__ __forceinline__ float ppm_slope_d(float dl, float dr) {
+  const float d = 0.5f * (dl + dr);
+  const float m = fminf(fabsf(d), 2.f * fminf(fabsf(dl), fabsf(dr)));
+  return (dl * dr > 0.f) ? copysignf(m, d) : 0.f;
 }
+__device__ __forceinline__ float ppm_slope(float am, float a, float ap) { return ppm_slope_d(a - am, ap - a); }
 // The edge increments of one cell from its neighbours and the limited slopes at the cells below,
 // at and above it (dm, d0, dp): a sweep that has the slopes already (carried along its march) gives
 // them here.
@@ -135,7 +141,8 @@ __device__ __forceinline__ void ppm_incs_d(float am, float a, float ap, float dm
   sd = 2.f * (a - al2);
 }
 __device__ __forceinline__ void ppm_incs(float a2m, float am, float a, float ap, float a2p, float& su, float& sd) {
-  ppm_incs_d(am, a, ap, ppm_slope(a2m, am, a), ppm_slope(am, a, ap), ppm_slope(a, ap, a2p), su, sd);
+  const float d1 = am - a2m, d2 = a - am, d3 = ap - a, d4 = a2p - ap;
+  ppm_incs_d(am, a, ap, ppm_slope_d(d1, d2), ppm_slope_d(d2, d3), ppm_slope_d(d3, d4), su, sd);
 }
 
 // The edge increments of one cell along one axis (hydro.ts:282-293; the ghost form :347-356):

@@ -360,7 +360,7 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, REC
     read_w<DIM, RECON>(sWj, wx, wy, c);
     with_cs(c, P);
     float su[DIM][6], sd[DIM][6];
-    float conv = 0.f, jump = 0.f;
+    float conv = 0.f, jump = -INFINITY;
     {
       float m[7], p[7], m2[7], p2[7];
       read_w<DIM, RECON>(sWj, wx - 1, wy, m);
@@ -371,7 +371,7 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, REC
       }
       axis_edges<RECON, ISEN>(m2, m, c, p, p2, P.inv_gamma, su[0], sd[0]);
       conv += p[1] - m[1];
-      jump = fmaxf(jump, fabsf(p[4] - m[4]) / fminf(p[4], m[4]));
+      jump = fmaxf(jump, jump_excess(m[4], p[4], P.shock_thresh));
       if constexpr (DIM >= 2) {
         read_w<DIM, RECON>(sWj, wx, wy - 1, m);
         read_w<DIM, RECON>(sWj, wx, wy + 1, p);
@@ -381,7 +381,7 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, REC
         }
         axis_edges<RECON, ISEN>(m2, m, c, p, p2, P.inv_gamma, su[1], sd[1]);
         conv += p[2] - m[2];
-        jump = fmaxf(jump, fabsf(p[4] - m[4]) / fminf(p[4], m[4]));
+        jump = fmaxf(jump, jump_excess(m[4], p[4], P.shock_thresh));
       }
       if constexpr (DIM == 3) {
         read_w<DIM, RECON>(ring(j - 1), wx, wy, m);
@@ -392,7 +392,7 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, REC
           axis_edges<RECON, ISEN>(m2, m, c, p, p2, P.inv_gamma, su[2], sd[2]);
         }
         conv += p[3] - m[3];
-        jump = fmaxf(jump, fabsf(p[4] - m[4]) / fminf(p[4], m[4]));
+        jump = fmaxf(jump, jump_excess(m[4], p[4], P.shock_thresh));
       }
     }
     (void)wo;
