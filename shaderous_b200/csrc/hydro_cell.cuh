@@ -50,7 +50,7 @@ __device__ __forceinline__ void hancock(const float* c, float conv, float jump, 
   qh[5] = c[5] - h * adv[5];
   const float rmin = qh[0] + fall;
   const float pmin = qh[4] - 0.5f * big;
-  out.fo = !(rmin > 0.f && pmin > 0.f);
+  out.fo = !((rmin > 0.f) & (pmin > 0.f));
 #pragma unroll
   for (int v = 0; v < 6; v++) out.q[v] = out.fo ? c[v] : qh[v];
 }
@@ -77,7 +77,7 @@ __device__ __forceinline__ void update_cell(const float4 a, const float4 b, cons
   const float eth = E - ke;
   const float emin = P.e_floor;
   // the dual-energy switch by selects (a warp whose cells choose differently runs one path)
-  const bool from_total = eth > P.eta_dual * E && eth >= emin;
+  const bool from_total = (eth > P.eta_dual * E) & (eth >= emin);
   const float eadv = (eint >= emin) ? eint : emin;
   eint = from_total ? eth : eadv;
   E = from_total ? E : ke + eadv;
@@ -122,7 +122,7 @@ __device__ __forceinline__ void hancock_masked(const float* c, float conv, float
   qh[5] = c[5] - h * adv[5];
   const float rmin = qh[0] + fall;
   const float pmin = qh[4] - 0.5f * big;
-  out.fo = !(rmin > 0.f && pmin > 0.f);
+  out.fo = !((rmin > 0.f) & (pmin > 0.f));
 #pragma unroll
   for (int v = 0; v < 6; v++) out.q[v] = out.fo ? c[v] : qh[v];
 }

@@ -59,14 +59,12 @@ __device__ __forceinline__ float limit(float a, float b, float scale) {
         ? copysignf(fminf(fminf(2.f * fabsf(far), 2.f * fabsf(near)), fabsf(fr)), near) : 0.f;
     const float s = 0.01f * scale;
     const float s2 = s * s;
-    const bool as_is = (s2 >= 1e-30f && s2 < 1e30f) || s == 0.f;
-    float eta;
-    if (as_is) {
-      eta = (far * far + near * near) / fmaxf(s2, 1e-30f);
-    } else {
-      const float k = 1.f / fabsf(s);
-      eta = (far * k) * (far * k) + (near * k) * (near * k);
-    }
+    const bool as_is = ((s2 >= 1e-30f) & (s2 < 1e30f)) | (s == 0.f);
+    // both forms, one kept (a select rather than a branch)
+    const float eta_as_is = (far * far + near * near) / fmaxf(s2, 1e-30f);
+    const float k = 1.f / fabsf(s);
+    const float eta_scaled = (far * k) * (far * k) + (near * k) * (near * k);
+    const float eta = as_is ? eta_as_is : eta_scaled;
     const float w = fminf(fmaxf(1.5f - eta, 0.f), 1.f);
     return lim + (fr - lim) * w;
   }
@@ -84,7 +82,9 @@ template <int R>
 __device__ __forceinline__ void isen_blend(const float* m, const float* c, const float* p, float pu, float pd,
                                            float inv_gamma, float& up, float& dn) {
   const float rl = m[0], pl = m[4], rc = c[0], pc = c[4], rr = p[0], pr = p[4];
-  if (!(rl > 0.f && pl > 0.f && rc > 0.f && pc > 0.f && rr > 0.f && pr > 0.f)) return;
+  // (hydro.ts:68: no increment unless all six are positive; the blend below is formed either way
+  // and kept only then, a select rather than a branch)
+  const bool ok = (rl > 0.f) & (pl > 0.f) & (rc > 0.f) & (pc > 0.f) & (rr > 0.f) & (pr > 0.f);
   const float gi = inv_gamma;
   const float tl = rl * powf(pc / pl, gi) - rc;
   const float tr = rr * powf(pc / pr, gi) - rc;
@@ -99,14 +99,14 @@ __device__ __forceinline__ void isen_blend(const float* m, const float* c, const
     const float pf = pc + 0.5f * pu;
     const float rf = fminf(fmaxf((rc + 0.5f * d) * powf(fmaxf(pf, 1e-30f) / pc, gi), fminf(rc, rr)), fmaxf(rc, rr));
     const float inc = 2.f * (rf - rc);
-    up += fminf(fmaxf(inc - up, -bound), bound);
+    up += ok ? fminf(fmaxf(inc - up, -bound), bound) : 0.f;
   }
   {
     const float d = limit<R>(tr, -tl, rc);
     const float pf = pc - 0.5f * pd;
     const float rf = fminf(fmaxf((rc - 0.5f * d) * powf(fmaxf(pf, 1e-30f) / pc, gi), fminf(rc, rl)), fmaxf(rc, rl));
     const float inc = -2.f * (rf - rc);
-    dn += fminf(fmaxf(inc - dn, -bound), bound);
+    dn += ok ? fminf(fmaxf(inc - dn, -bound), bound) : 0.f;
   }
 }
 
@@ -134,7 +134,7 @@ __device__ __forceinline__ void ppm_incs_d(float am, float a, float ap, float dm
   const bool flat = (ar - a) * (a - al) <= 0.f;
   const float da = ar - al, a6 = 6.f * (a - 0.5f * (al + ar));
   const bool pull_l = da * a6 > da * da;
-  const bool pull_r = !pull_l && -da * da > da * a6;
+  const bool pull_r = (!pull_l) & (-da * da > da * a6);
   const float al2 = flat ? a : (pull_l ? 3.f * a - 2.f * ar : al);
   const float ar2 = flat ? a : (pull_r ? 3.f * a - 2.f * al : ar);
   su = 2.f * (ar2 - a);
