@@ -43,10 +43,11 @@ def test_uniform_run_diagnostics_slice_probe_and_snapshot(tmp_path):
         u1, u2 = s.read_state()
     assert d["steps"] == 25
     assert d["mass"] == pytest.approx(want.mass, rel=1e-6) and d["eTot"] == pytest.approx(want.e_tot, rel=1e-6)
-    # a slice of density at full resolution is the state's density, cell for cell
+    # a slice of density at full resolution is the state's density, cell for cell (its values are
+    # given to 5 significant digits, as the reference's mcp.mjs gives them)
     sl = call(srv, "slice", variable="rho", axis=2, pos=0.5, res=128, include_values=True)
     rho = np.asarray(sl["values"])
-    np.testing.assert_allclose(rho, u1[:, 0].reshape(128, 128), rtol=2e-5)
+    np.testing.assert_allclose(rho, u1[:, 0].reshape(128, 128), rtol=1e-4)
     assert sl["min"] == pytest.approx(float(u1[:, 0].min()), rel=1e-6)
     # probes at cell centres
     pts = [[(5 + 0.5) / 128, (70 + 0.5) / 128, 0.5], [(100 + 0.5) / 128, (3 + 0.5) / 128, 0.5]]
