@@ -65,7 +65,8 @@ def parse():
                     help="the serving stream's size and step distributions")
     ap.add_argument("--section", choices=["all", "amr", "serving", "comparable"], default="all",
                     help="amr / serving: only that measurement, printed as its own JSON line")
-    ap.add_argument("--amr-variant", choices=["both", "spec", "developed", "bins"], default="both")
+    ap.add_argument("--amr-variant", choices=["both", "spec", "developed", "bins", "spread"], default="both",
+                    help="spread: a mesh of the developed run's size at once, for profiling")
     ap.add_argument("--amr-cap", type=int, default=26000, help="block slots of the AMR runs")
     ap.add_argument("--profile-window", action="store_true",
                     help="AMR section: bracket one step after the warm-up with cudaProfilerStart/Stop")
@@ -133,6 +134,21 @@ def amr_sedov(levels=4, nr=8, radius_cells=3.5, steps=24, cap=26000, profile_win
         t_init = time.perf_counter() - t0
         out = _time_amr(a, steps, time_bins, profile_window)
     out.update({"finest_cells_per_side": nr * 16 << levels, "radius_finest_cells": radius_cells, "init_s": t_init})
+    return out
+
+
+def amr_sedov_spread(levels=4, nr=8, steps=16, cap=30000, profile_window=False):
+    """A profiling mesh of the developed run's size at once: the same energy (E = 1, gamma = 5/3)
+    as a uniform hot sphere of radius 0.16 of the box, whose refined shell holds 22,520 leaves
+    (25,664 blocks) from the start; the configured run reaches 20k only after some 34,000 steps."""
+    from shaderous_b200 import Problem
+    from shaderous_b200.amr import AmrSim
+
+    r = 0.16
+    with AmrSim(_amr_cfg(levels, nr, cap)) as a:
+        a.reset(Problem("blast", a=(1.0, (2.0 / 3.0) / (4.0 / 3.0 * math.pi * r ** 3), 1.0, 1e-5, r)))
+        out = _time_amr(a, steps, 0, profile_window)
+    out["note"] += "; a profiling mesh: the blast's energy spread within 0.16 of the box"
     return out
 
 
@@ -604,6 +620,9 @@ def main():
         if args.section == "amr":
             if args.amr_variant in ("both", "spec"):
                 out["spec"] = amr_sedov(steps=max(args.steps, 8), cap=args.amr_cap, profile_window=args.profile_window)
+            if args.amr_variant == "spread":
+                out["spread"] = amr_sedov_spread(steps=max(args.steps, 8), cap=max(args.amr_cap, 30000),
+                                                 profile_window=args.profile_window)
             if args.amr_variant in ("both", "developed", "bins"):
                 out.update(amr_sedov_developed(steps=max(args.steps, 8), cap=args.amr_cap,
                                                profile_window=args.profile_window, bins=args.amr_variant != "developed"))

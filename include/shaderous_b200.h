@@ -462,6 +462,14 @@ int shz_server_run_stream(shz_server* s, const shz_request* reqs, int32_t n, shz
  * SHZ_E_CONFIG for an unknown id or a request that has finished or was cancelled already. No
  * counterpart in the reference (whose runs stop by their RunOptions timeoutMs). */
 int shz_server_cancel(shz_server* s, int64_t id);
+/* The state of request `id` (called between other server calls): *status one of SHZ_REQ_*, and,
+ * if steps_done is not null, the steps it has taken (its whole count once finished). No
+ * counterpart in the reference (a page runs one simulation, whose clock run() reads back). */
+#define SHZ_REQ_QUEUED 0
+#define SHZ_REQ_RUNNING 1
+#define SHZ_REQ_FINISHED 2
+#define SHZ_REQ_CANCELLED 3
+int shz_server_poll(shz_server* s, int64_t id, int32_t* status, int64_t* steps_done);
 int shz_server_result(shz_server* s, int64_t id, shz_diag* diag);
 int shz_server_state(shz_server* s, int64_t id, float* u1, float* u2);
 /* The same stream run one request after another, each through the plain uniform-grid step

@@ -252,6 +252,7 @@ SIGNATURES = [
     ("shz_server_drain", C.c_int, [C.c_void_p, C.c_int32]),
     ("shz_server_run_stream", C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(shz_server_stats)]),
     ("shz_server_cancel", C.c_int, [C.c_void_p, C.c_int64]),
+    ("shz_server_poll", C.c_int, [C.c_void_p, C.c_int64, C.POINTER(C.c_int32), C.POINTER(C.c_int64)]),
     ("shz_server_result", C.c_int, [C.c_void_p, C.c_int64, C.POINTER(shz_diag)]),
     ("shz_server_state", C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]),
     ("shz_plain_run_stream", C.c_int, [C.POINTER(shz_server_config), C.c_void_p, C.c_int32, C.POINTER(shz_server_stats)]),

@@ -910,6 +910,28 @@ int shz_server_cancel(shz_server* s, int64_t id) {
   return 0;
 }
 
+int shz_server_poll(shz_server* s, int64_t id, int32_t* status, int64_t* steps_done) {
+  if (!s || !status) return SHZ_E_CONFIG;
+  auto it = s->grids.find(id);
+  if (it == s->grids.end()) return fail(s, SHZ_E_CONFIG, "no request %lld", (long long)id);
+  const Grid& G = *it->second;
+  int64_t done = 0;
+  if (G.cancelled) {
+    *status = SHZ_REQ_CANCELLED;
+  } else if (G.done) {
+    *status = SHZ_REQ_FINISHED;
+    done = G.req.steps;
+  } else if (std::find(s->pending.begin(), s->pending.end(), &G) != s->pending.end()) {
+    *status = SHZ_REQ_QUEUED;
+  } else {
+    *status = SHZ_REQ_RUNNING;
+    // between calls no round is in flight: the clocks read back after the last round are current
+    done = G.direct ? G.enq : (G.g >= 0 ? s->e[G.eng].h_clk[G.g].steps : 0);
+  }
+  if (steps_done) *steps_done = done;
+  return 0;
+}
+
 int shz_server_result(shz_server* s, int64_t id, shz_diag* d) {
   if (!s || !d) return SHZ_E_CONFIG;
   auto it = s->grids.find(id);

@@ -112,6 +112,13 @@ class Server:
         """Take request `rid` off the queue or the device; its result then raises SHZ_E_CANCELLED."""
         self._ok(self._lib.shz_server_cancel(self._h, int(rid)))
 
+    def poll(self, rid: int) -> tuple[str, int]:
+        """(status, steps taken) of request `rid`: status "queued", "running", "finished" or
+        "cancelled"."""
+        st, n = C.c_int32(), C.c_int64()
+        self._ok(self._lib.shz_server_poll(self._h, int(rid), C.byref(st), C.byref(n)))
+        return ("queued", "running", "finished", "cancelled")[st.value], n.value
+
     def result(self, rid: int) -> Diagnostics:
         d = _abi.shz_diag()
         self._ok(self._lib.shz_server_result(self._h, rid, C.byref(d)))

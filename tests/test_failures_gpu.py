@@ -90,8 +90,11 @@ def test_cancel_running_and_queued_requests():
     with Server(_cfg(1)) as s:  # one request at a time per engine (2D, 3D): two run, two wait
         ids = [s.submit(r) for r in reqs]
         s.drain(max_rounds=2)  # 0 (2D) and 1 (3D) are running, 2 and 3 queued
+        assert [s.poll(i)[0] for i in ids] == ["running", "running", "queued", "queued"]
+        assert 0 < s.poll(ids[0])[1] < reqs[0].steps
         s.cancel(ids[1])  # running
         s.cancel(ids[3])  # queued
+        assert s.poll(ids[1])[0] == "cancelled" and s.poll(ids[3])[0] == "cancelled"
         with pytest.raises(ShaderousError) as e:
             s.cancel(ids[1])
         assert e.value.code == _abi.SHZ_E_CONFIG
@@ -106,6 +109,7 @@ def test_cancel_running_and_queued_requests():
             with pytest.raises(ShaderousError) as e:
                 s.state(ids[k], reqs[k])
             assert e.value.code == _abi.SHZ_E_CANCELLED
+        assert s.poll(ids[0]) == ("finished", reqs[0].steps) and s.poll(ids[2]) == ("finished", reqs[2].steps)
         got = {k: s.state(ids[k], reqs[k]) for k in (0, 2)}
         for k in (0, 2):
             assert s.result(ids[k]).steps == reqs[k].steps
