@@ -68,6 +68,8 @@ def parse():
     ap.add_argument("--amr-variant", choices=["both", "spec", "developed", "bins", "spread"], default="both",
                     help="spread: a mesh of the developed run's size at once, for profiling")
     ap.add_argument("--amr-cap", type=int, default=26000, help="block slots of the AMR runs")
+    ap.add_argument("--amr-levels", type=int, default=4,
+                    help="levels above the roots of the spread mesh (3: a quarter of the leaves, for full captures)")
     ap.add_argument("--profile-window", action="store_true",
                     help="AMR section: bracket one step after the warm-up with cudaProfilerStart/Stop")
     ap.add_argument("--pin-assemble", type=int, default=None, metavar="V",
@@ -621,8 +623,8 @@ def main():
             if args.amr_variant in ("both", "spec"):
                 out["spec"] = amr_sedov(steps=max(args.steps, 8), cap=args.amr_cap, profile_window=args.profile_window)
             if args.amr_variant == "spread":
-                out["spread"] = amr_sedov_spread(steps=max(args.steps, 8), cap=max(args.amr_cap, 30000),
-                                                 profile_window=args.profile_window)
+                out["spread"] = amr_sedov_spread(levels=args.amr_levels, steps=max(args.steps, 8),
+                                                 cap=max(args.amr_cap, 30000), profile_window=args.profile_window)
             if args.amr_variant in ("both", "developed", "bins"):
                 out.update(amr_sedov_developed(steps=max(args.steps, 8), cap=args.amr_cap,
                                                profile_window=args.profile_window, bins=args.amr_variant != "developed"))

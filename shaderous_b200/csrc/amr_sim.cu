@@ -63,6 +63,9 @@ struct shz_amr {
   long long since_check = 0;
   // a refinement check is due before the next single step: its assemble is that step's own
   bool flags_due = false;
+  // whether the next check takes its step ahead of the decision: after a check that kept the mesh
+  // (a step taken ahead of a check that changes it is thrown away)
+  bool check_ahead = true;
   cudaStream_t stream = nullptr;
   cudaGraphExec_t graphs[4] = {nullptr, nullptr, nullptr, nullptr};
   long long graph_launches[4] = {0, 0, 0, 0};  // kernels one replay of each graph launches
@@ -642,14 +645,19 @@ int check_and_regrid(shz_amr* a, const std::vector<double>* extra, int* changed)
 
 // A single step that begins with the refinement check due after the last (amr_sim.ts applies a
 // re-mesh decided after a step at the start of the next, applyRegrid): the step's own assemble
-// gives the primitives the Löhner pass reads, so the check needs no assemble of its own. The rest
-// of the step is launched at once, ahead of the decision (the reference's speculation behind an
-// unanswered check, amr_sim.ts:2762-2775), and BlockTree.adapt runs on the host meanwhile. The step
-// writes the other parity, so the state it started from is still there: if the mesh changes, the
-// clock is put back as it was, the new leaves are filled from that state and the step runs again
-// on the new mesh (its rate taken back); if not, the step stands. Launched eagerly, not from a graph.
+// gives the primitives the Löhner pass reads, so the check needs no assemble of its own. After a
+// check that kept the mesh, the rest of the step is launched at once, ahead of the decision (the
+// reference's speculation behind an unanswered check, amr_sim.ts:2762-2775), and BlockTree.adapt
+// runs on the host meanwhile. The step writes the other parity, so the state it started from is
+// still there: if the mesh changes, the clock is put back as it was, the new leaves are filled from
+// that state and the step runs again on the new mesh (its rate taken back); if not, the step
+// stands. After a check that changed the mesh (a moving front changes it at check after check),
+// the rest waits for the decision: the host's adapt is a few milliseconds, a step thrown away
+// several times that. Either way the same kernels run on the same data. Launched eagerly, not from
+// a graph.
 int check_step(shz_amr* a) {
   a->flags_due = false;
+  const bool ahead = a->check_ahead;
   long long n = 0;
   int rc = enqueue_assemble(a, false, &n);
   if (rc) return rc;
@@ -660,8 +668,10 @@ int check_step(shz_amr* a) {
   AMR_CUDA(a, cudaMemcpyAsync(a->h_flags_pinned, a->d_flags, sizeof(float) * a->cfg.cap, cudaMemcpyDeviceToHost,
                               a->stream));
   AMR_CUDA(a, cudaEventRecord(a->flags_ready, a->stream));
-  AMR_CUDA(a, cudaMemcpyAsync(a->clk_save, a->clk, sizeof(shz::DevClock), cudaMemcpyDeviceToDevice, a->stream));
-  if ((rc = enqueue_rest(a, false, &n))) return rc;
+  if (ahead) {
+    AMR_CUDA(a, cudaMemcpyAsync(a->clk_save, a->clk, sizeof(shz::DevClock), cudaMemcpyDeviceToDevice, a->stream));
+    if ((rc = enqueue_rest(a, false, &n))) return rc;
+  }
   a->launches += n;
   AMR_CUDA(a, cudaEventSynchronize(a->flags_ready));
   std::memcpy(a->h_flags.data(), a->h_flags_pinned, sizeof(float) * a->cfg.cap);
@@ -672,9 +682,12 @@ int check_step(shz_amr* a) {
   } catch (const std::exception& e) {
     return fail(a, SHZ_E_CONFIG, "adapt: %s", e.what());
   }
+  a->check_ahead = ops.empty();
   if (!ops.empty()) {
-    // the step taken ahead is void: the clock as it was, the rate slot empty for the new mesh
-    AMR_CUDA(a, cudaMemcpyAsync(a->clk, a->clk_save, sizeof(shz::DevClock), cudaMemcpyDeviceToDevice, a->stream));
+    // the step taken ahead (if any) is void: the clock as it was; the rate slot, which the
+    // assemble filled over the old mesh, empty for the new one
+    if (ahead)
+      AMR_CUDA(a, cudaMemcpyAsync(a->clk, a->clk_save, sizeof(shz::DevClock), cudaMemcpyDeviceToDevice, a->stream));
     AMR_CUDA(a, cudaMemsetAsync(a->rates + a->slot, 0, sizeof(unsigned), a->stream));
     a->h_rg.resize((size_t)a->cfg.cap * shz::amr::RG_STRIDE);
     BlockTree::regrid_table(ops, a->cfg.cap, a->h_rg.data());
@@ -686,6 +699,11 @@ int check_step(shz_amr* a) {
     a->launches += 1;
     a->cur ^= 1;
     return step_once(a);
+  }
+  if (!ahead) {
+    n = 0;
+    if ((rc = enqueue_rest(a, false, &n))) return rc;
+    a->launches += n;
   }
   a->cur ^= 1;
   a->slot ^= 1;

@@ -269,7 +269,8 @@ constexpr int SW_RING = RING * SW_PLANE;
 constexpr int SW_FACE = 2 * 7 * SPN;  // x and y upper face states of a plane
 constexpr int SW_FLUX = 2 * 8 * SPN;  // x and y lower-face fluxes of a plane (also the half-step exchange)
 constexpr int SW_KEEP = 8 * SPN;      // z boundary ghosts: a plane's half steps or the ghost's increments
-constexpr size_t SWEEP_SMEM = (size_t)(SW_RING + SW_FACE + SW_FLUX + SW_KEEP) * sizeof(float);
+constexpr int SW_ZUP = 7 * SPN;       // each thread's upper z face state, for the next plane's z face
+constexpr size_t SWEEP_SMEM = (size_t)(SW_RING + SW_FACE + SW_FLUX + SW_KEEP + SW_ZUP) * sizeof(float);
 constexpr uint32_t PLANE_BYTES = SWN * sizeof(float4);  // one of w1 / w2 of a plane: 6400 B
 
 // Texel (x, y) of a staged plane: its seven primitives (the sound speed as the atlas holds it).
@@ -302,6 +303,7 @@ __global__ void __maxnreg__(80)
   float* sFace = sW + SW_RING;
   float* sFlux = sFace + SW_FACE;
   float* sKeep = sFlux + SW_FLUX;
+  float* sZup = sKeep + SW_KEEP;
   // the block's grid parameters, copied once per block: the march reads them at every face
   __shared__ __align__(16) KParams sP;
   const int tid = threadIdx.x;
@@ -389,7 +391,6 @@ __global__ void __maxnreg__(80)
       p2[o] = make_float4(q.q[4], q.q[5], q.flag, q.fo ? 1.f : 0.f);
     };
 
-    float zhi_prev[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     float ph_prev = 0.f;
 
@@ -520,7 +521,10 @@ __global__ void __maxnreg__(80)
           float inc[6];
 #pragma unroll
           for (int v = 0; v < 6; v++) inc[v] = sKeep[v * SPN + tid];
-          face_state(gq, inc, 1.f, zhi_prev);
+          float zf[7];
+          face_state(gq, inc, 1.f, zf);
+#pragma unroll
+          for (int q = 0; q < 7; q++) sZup[q * SPN + tid] = zf[q];
           if (keep) keep_pred(-1, gq);  // the lower boundary ghost: plane 0's half step, mirrored
         }
         if (j == BS - 1 && zhi_nb <= -2) {
@@ -583,7 +587,10 @@ __global__ void __maxnreg__(80)
           // the z face below plane j
           float Rr[7];
           face_state(pr, sd[2], -1.f, Rr);
-          riemann<2>(zhi_prev, Rr, P, Fz);
+          float zf[7];
+#pragma unroll
+          for (int q = 0; q < 7; q++) zf[q] = sZup[q * SPN + tid];
+          riemann<2>(zf, Rr, P, Fz);
           if ((j == 0 && (fine & 16u)) || (j == BS && (fine & 32u))) matched(j == 0 ? 4 : 5, lx + BS * ly, Fz);
         }
       }
@@ -626,7 +633,12 @@ __global__ void __maxnreg__(80)
       }
       if constexpr (DIM == 3) {
         // the upper z face state of plane j (a lower boundary ghost's is set at plane 0)
-        if (!(j == -1 && zlo_nb <= -2)) face_state(pr, su[2], 1.f, zhi_prev);
+        if (!(j == -1 && zlo_nb <= -2)) {
+          float zf[7];
+          face_state(pr, su[2], 1.f, zf);
+#pragma unroll
+          for (int q = 0; q < 7; q++) sZup[q * SPN + tid] = zf[q];
+        }
       }
     }
   }
