@@ -260,17 +260,21 @@ __global__ void __launch_bounds__(NT) amr_fine_flux(const KParams* __restrict__ 
   }
 }
 
-// Shared memory of the block sweep, in floats. The primitive planes are a ring of four, each the
+// Shared memory of the block sweep, in floats. The primitive planes are a ring of three, each the
 // plane's w1 texels then its w2 texels (float4, as in the atlas), filled by bulk copies (TMA): the
-// march reads planes j - 1, j, j + 1 while plane j + 2 is in flight.
-constexpr int RING = 4;
+// predictor at plane j reads planes j - 1, j, j + 1; once every thread is past it, plane j - 1's
+// slot takes plane j + 2, in flight during the fluxes and updates of plane j. (A fourth slot, for
+// a copy issued a plane earlier, would leave no room for the flux sums held here instead of in
+// registers at two CTAs per SM.)
+constexpr int RING = 3;
 constexpr int SW_PLANE = 2 * 4 * SWN;    // floats of one staged plane (w1 and w2)
 constexpr int SW_RING = RING * SW_PLANE;
 constexpr int SW_FACE = 2 * 7 * SPN;  // x and y upper face states of a plane
 constexpr int SW_FLUX = 2 * 8 * SPN;  // x and y lower-face fluxes of a plane (also the half-step exchange)
 constexpr int SW_KEEP = 8 * SPN;      // z boundary ghosts: a plane's half steps or the ghost's increments
 constexpr int SW_ZUP = 7 * SPN;       // each thread's upper z face state, for the next plane's z face
-constexpr size_t SWEEP_SMEM = (size_t)(SW_RING + SW_FACE + SW_FLUX + SW_KEEP + SW_ZUP) * sizeof(float);
+constexpr int SW_ACC = 8 * SPN;       // each thread's flux sums of the plane below, until its upper z face
+constexpr size_t SWEEP_SMEM = (size_t)(SW_RING + SW_FACE + SW_FLUX + SW_KEEP + SW_ZUP + SW_ACC) * sizeof(float);
 constexpr uint32_t PLANE_BYTES = SWN * sizeof(float4);  // one of w1 / w2 of a plane: 6400 B
 
 // Texel (x, y) of a staged plane: its seven primitives (the sound speed as the atlas holds it).
@@ -304,6 +308,7 @@ __global__ void __maxnreg__(80)
   float* sFlux = sFace + SW_FACE;
   float* sKeep = sFlux + SW_FLUX;
   float* sZup = sKeep + SW_KEEP;
+  float* sAcc = sZup + SW_ZUP;
   // the block's grid parameters, copied once per block: the march reads them at every face
   __shared__ __align__(16) KParams sP;
   const int tid = threadIdx.x;
@@ -313,7 +318,7 @@ __global__ void __maxnreg__(80)
   const bool col_t = tx >= 1 && tx <= BS;
   const bool tile_t = row_t && col_t;
   auto ring = [&](int plane) -> const float4* {
-    return reinterpret_cast<const float4*>(sW + (size_t)((plane + 8) & (RING - 1)) * SW_PLANE);
+    return reinterpret_cast<const float4*>(sW + (size_t)((plane + 3 * RING) % RING) * SW_PLANE);
   };
   // One mbarrier per ring slot; the phase each thread expects next, per slot (uniform across the
   // CTA: every thread waits for every plane once); slots with a copy in flight.
@@ -391,13 +396,16 @@ __global__ void __maxnreg__(80)
       p2[o] = make_float4(q.q[4], q.q[5], q.flag, q.fo ? 1.f : 0.f);
     };
 
-    float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     float ph_prev = 0.f;
+    // CTA-uniform: a predicted cell of plane j - 1 (block and ghost ring) is shock-flagged. The
+    // faces of plane j see the flags of planes j - 1 and j only; without any, the solver skips the
+    // HLL flux.
+    bool flagged_prev = true;
 
     // Plane pl (-2 .. 17) of this block's atlas into its ring slot: issued by one thread, after a
-    // barrier that follows every thread's last read of the slot (the plane four before).
+    // barrier that follows every thread's last read of the slot (the plane three before).
     auto issue = [&](int pl) {
-      const int s = (pl + 8) & (RING - 1);
+      const int s = (pl + 3 * RING) % RING;
       if (tid == 0) {
         const size_t zb = (size_t)slot * BG<DIM>::WN + (DIM == 3 ? (size_t)(pl + NG) * SWN : 0);
         float4* dst = reinterpret_cast<float4*>(sW + (size_t)s * SW_PLANE);
@@ -410,7 +418,7 @@ __global__ void __maxnreg__(80)
     };
     // Wait for plane pl; CTA-uniformly false if the copy did not complete in time.
     auto arrived = [&](int pl) -> bool {
-      const int s = (pl + 8) & (RING - 1);
+      const int s = (pl + 3 * RING) % RING;
       const bool ok = tma::mbar_wait(&sBar[s], (phase >> s) & 1u, tma::WAIT_LIMIT);
       phase ^= 1u << s;
       pending &= ~(1u << s);
@@ -436,7 +444,6 @@ __global__ void __maxnreg__(80)
     // 3D: planes -1 .. 16, the first and last the z ghosts; 2D: the one plane.
     const int jb = DIM == 3 ? -1 : 0, je = DIM == 3 ? BS : 0;
     for (int j = jb; j <= je; j++) {
-      if (DIM == 3 && j + 2 <= BS + 1) issue(j + 2);
       if (!arrived(DIM == 3 ? j + 1 : 0)) {
         give_up();
         return;
@@ -553,7 +560,11 @@ __global__ void __maxnreg__(80)
           for (int v = 0; v < 7; v++) sFace[(7 + v) * SPN + tid] = f[v];
         }
       }
-      __syncthreads();
+      const bool flagged = __syncthreads_or(pr.flag != 0.f);
+      const bool hll_any = flagged || (DIM == 3 && flagged_prev);
+      flagged_prev = flagged;
+      // every thread is done with plane j - 1: its ring slot takes plane j + 2
+      if (DIM == 3 && j + 2 <= BS + 1) issue(j + 2);
 
       const int lz = DIM == 3 ? j : 0;
       if (tile_plane) {
@@ -563,7 +574,7 @@ __global__ void __maxnreg__(80)
 #pragma unroll
           for (int v = 0; v < 7; v++) L[v] = sFace[v * SPN + tid - 1];
           face_state(pr, sd[0], -1.f, Rr);
-          riemann<0>(L, Rr, P, F);
+          riemann<0>(L, Rr, P, F, hll_any);
           if ((lx == 0 && (fine & 1u)) || (lx == BS && (fine & 2u))) matched(lx == 0 ? 0 : 1, ly + BS * lz, F);
 #pragma unroll
           for (int v = 0; v < 8; v++) sFlux[v * SPN + tid] = F[v];
@@ -574,7 +585,7 @@ __global__ void __maxnreg__(80)
 #pragma unroll
             for (int v = 0; v < 7; v++) L[v] = sFace[(7 + v) * SPN + tid - SX];
             face_state(pr, sd[1], -1.f, Rr);
-            riemann<1>(L, Rr, P, F);
+            riemann<1>(L, Rr, P, F, hll_any);
             if ((ly == 0 && (fine & 4u)) || (ly == BS && (fine & 8u))) matched(ly == 0 ? 2 : 3, lx + BS * lz, F);
 #pragma unroll
             for (int v = 0; v < 8; v++) sFlux[(8 + v) * SPN + tid] = F[v];
@@ -590,18 +601,19 @@ __global__ void __maxnreg__(80)
           float zf[7];
 #pragma unroll
           for (int q = 0; q < 7; q++) zf[q] = sZup[q * SPN + tid];
-          riemann<2>(zf, Rr, P, Fz);
+          riemann<2>(zf, Rr, P, Fz, hll_any);
           if ((j == 0 && (fine & 16u)) || (j == BS && (fine & 32u))) matched(j == 0 ? 4 : 5, lx + BS * ly, Fz);
         }
       }
       __syncthreads();
 
       if (tile_t) {
+        float acc[8];
         if constexpr (DIM == 3) {
           if (j >= 1) {
             // plane j - 1 is complete: its upper z face is Fz
 #pragma unroll
-            for (int v = 0; v < 8; v++) acc[v] -= Fz[v];
+            for (int v = 0; v < 8; v++) acc[v] = sAcc[v * SPN + tid] - Fz[v];
             const size_t o = base + ((size_t)(j - 1) * BS + ly) * BS + lx;
             float4 na, nb4;
             update_cell(__ldg(u1 + o), __ldg(u2 + o), acc, ph_prev, dtdx, P, na, nb4);
@@ -618,8 +630,12 @@ __global__ void __maxnreg__(80)
               a += sFlux[(8 + v) * SPN + tid];
               a -= sFlux[(8 + v) * SPN + tid + SX];
             }
-            if constexpr (DIM == 3) a += Fz[v];
-            acc[v] = a;
+            if constexpr (DIM == 3) {
+              a += Fz[v];
+              sAcc[v * SPN + tid] = a;
+            } else {
+              acc[v] = a;
+            }
           }
           ph_prev = pr.q[4];
           if constexpr (DIM < 3) {

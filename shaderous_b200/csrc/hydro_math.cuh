@@ -172,8 +172,12 @@ __device__ __forceinline__ void axis_edges(const float* m2, const float* m, cons
 // The three regions (left-supersonic, right-supersonic, star) and the star side are chosen by
 // selects rather than branches, so that a warp whose faces fall in different regions runs one
 // path; the values computed for the regions not chosen are discarded.
+// hll_any: false when the caller knows that neither side of any face it solves is shock-flagged
+// (a CTA-uniform fact, so the branch does not diverge). The HLL flux then has weight 0 and is
+// skipped: c + (h - c) * 0 is c for a finite h, up to the sign of an exact zero.
 template <int AXIS>
-__device__ __forceinline__ void riemann(const float* L, const float* R, const KParams& P, float* F) {
+__device__ __forceinline__ void riemann(const float* L, const float* R, const KParams& P, float* F,
+                                        bool hll_any = true) {
   constexpr int A0 = 1 + AXIS, A1 = 1 + (AXIS + 1) % 3, A2 = 1 + (AXIS + 2) % 3;
   const float lr = fmaxf(L[0], P.rho_floor), rr = fmaxf(R[0], P.rho_floor);
   const float lp = fmaxf(L[4], P.p_floor), rp = fmaxf(R[4], P.p_floor);
@@ -197,13 +201,6 @@ __device__ __forceinline__ void riemann(const float* L, const float* R, const KP
   const float ql = lr * (sl - lu);
   const float qr = rr * (sr - ru);
   const float sm = (rp - lp + lu * ql - ru * qr) / (ql - qr);
-  const float inv = 1.f / (sr - sl);
-  const float slsr = sl * sr;
-  const float hm = (sr * ml0 - sl * mr0 + slsr * (rr - lr)) * inv;
-  const float hp0 = (sr * fpl0 - sl * fpr0 + slsr * (mr0 - ml0)) * inv;
-  const float hp1 = (sr * fpl1 - sl * fpr1 + slsr * (mr1 - ml1)) * inv;
-  const float hp2 = (sr * fpl2 - sl * fpr2 + slsr * (mr2 - ml2)) * inv;
-  const float he = (sr * fel - sl * fer + slsr * (er - el)) * inv;
   // HLLC star state on the side of the contact the face lies on
   const bool left = sm >= 0.f;
   const float sK = left ? sl : sr, qK = left ? ql : qr, rK = left ? lr : rr, uK = left ? lu : ru;
@@ -217,11 +214,21 @@ __device__ __forceinline__ void riemann(const float* L, const float* R, const KP
   const float c1 = fK1 + sK * (f * vK - mK1);
   const float c2 = fK2 + sK * (f * wK - mK2);
   const float ce = feK + sK * (es - eK);
-  float m = cm + (hm - cm) * w_hll;
-  float p0 = c0 + (hp0 - c0) * w_hll;
-  float p1 = c1 + (hp1 - c1) * w_hll;
-  float p2 = c2 + (hp2 - c2) * w_hll;
-  float e = ce + (he - ce) * w_hll;
+  float m = cm, p0 = c0, p1 = c1, p2 = c2, e = ce;
+  if (hll_any || P.hll) {
+    const float inv = 1.f / (sr - sl);
+    const float slsr = sl * sr;
+    const float hm = (sr * ml0 - sl * mr0 + slsr * (rr - lr)) * inv;
+    const float hp0 = (sr * fpl0 - sl * fpr0 + slsr * (mr0 - ml0)) * inv;
+    const float hp1 = (sr * fpl1 - sl * fpr1 + slsr * (mr1 - ml1)) * inv;
+    const float hp2 = (sr * fpl2 - sl * fpr2 + slsr * (mr2 - ml2)) * inv;
+    const float he = (sr * fel - sl * fer + slsr * (er - el)) * inv;
+    m = cm + (hm - cm) * w_hll;
+    p0 = c0 + (hp0 - c0) * w_hll;
+    p1 = c1 + (hp1 - c1) * w_hll;
+    p2 = c2 + (hp2 - c2) * w_hll;
+    e = ce + (he - ce) * w_hll;
+  }
   float vn = sm;
   // supersonic faces take the upwind side's flux
   const bool supl = sl >= 0.f, supr = sr <= 0.f;

@@ -210,6 +210,9 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, REC
   float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   float ph_prev = 0.f;
   float gsu[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // edges of the lower z ghost (outflow / reflect)
+  // CTA-uniform: a cell of plane j - 1 (column and halo ring) is shock-flagged. The faces of plane
+  // j see the flags of planes j - 1 and j only; without any, the solver skips the HLL flux.
+  bool flagged_prev = true;
 #pragma unroll
   for (int v = 0; v < 7; v++) zhi_prev[v] = 0.f;
 
@@ -332,6 +335,7 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, REC
         if (zg_lo) {
 #pragma unroll
           for (int v = 0; v < 6; v++) gsu[v] = su[v];
+          flagged_prev = false;  // plane 0's faces see plane 0's flags only
         } else if (tile_t) {
           Pred g;
 #pragma unroll
@@ -341,7 +345,7 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, REC
           g.fo = fo_prev;
           float zlo[7], Fz[8];
           face_state(g, sd, -1.f, zlo);
-          riemann<2>(zhi_prev, zlo, P, Fz);
+          riemann<2>(zhi_prev, zlo, P, Fz, flagged_prev);
 #pragma unroll
           for (int v = 0; v < 8; v++) acc[v] -= Fz[v];
           const size_t o = ((size_t)(j - 1) * ny + gy) * nx + gx;
@@ -436,7 +440,9 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, REC
         for (int v = 0; v < 7; v++) sFace[(7 + v) * PN + tid] = f[v];
       }
     }
-    __syncthreads();
+    const bool flagged = __syncthreads_or(pr.flag != 0.f);
+    const bool hll_any = flagged || (DIM == 3 && flagged_prev);
+    flagged_prev = flagged;
 
     // 5. fluxes: the lower x and y faces into shared memory, the lower z face in registers.
     if (tile_plane) {
@@ -445,7 +451,7 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, REC
 #pragma unroll
         for (int v = 0; v < 7; v++) L[v] = sFace[v * PN + tid - 1];
         face_state(pr, sd[0], -1.f, R);
-        riemann<0>(L, R, P, F);
+        riemann<0>(L, R, P, F, hll_any);
 #pragma unroll
         for (int v = 0; v < 8; v++) sFlux[v * PN + tid] = F[v];
       }
@@ -455,7 +461,7 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, REC
 #pragma unroll
           for (int v = 0; v < 7; v++) L[v] = sFace[(7 + v) * PN + tid - PX];
           face_state(pr, sd[1], -1.f, R);
-          riemann<1>(L, R, P, F);
+          riemann<1>(L, R, P, F, hll_any);
 #pragma unroll
           for (int v = 0; v < 8; v++) sFlux[(8 + v) * PN + tid] = F[v];
         }
@@ -466,7 +472,7 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, REC
       if (tile_t && j >= z0) {
         float R[7];
         face_state(pr, sd[2], -1.f, R);
-        riemann<2>(zhi_prev, R, P, Fz);
+        riemann<2>(zhi_prev, R, P, Fz, hll_any);
       }
     }
     __syncthreads();
