@@ -13,13 +13,15 @@
 // maximum (warp shuffles, then one atomicMax per CTA on the float's bits).
 //
 // Decomposition: a CTA owns a TX x TY column of cells and marches it along z through tz planes
-// (2.5D). Its threads are the (TX+2) x (TY+2) cells of the column plus one ring of halo cells;
-// each thread keeps the primitives of its own column for the planes the predictor reads along
-// z in registers, so z-neighbours and z-faces never touch shared memory. Per plane, the
-// primitives of the column plus the halo of the stencil go to shared memory for the x/y
-// neighbours; the face states toward the upper x and y faces go to shared memory so that the
-// next thread can solve its lower face; each face flux is computed once and used by both
-// cells, so both sides see bit-identical fluxes (the reference's flux-determinism check,
+// (2.5D). Its threads are the (TX+2) x (TY+2) cells of the column plus one ring of halo cells.
+// The primitives of the planes the predictor's z stencil reads sit in a ring of planes in shared
+// memory, each plane the column plus the stencil's halo (as pairs: rho vx, vy vz, p s, one
+// 8-byte load each), converted from the conserved state that a tiled TMA copy staged while the
+// previous plane was computed. The z face below a cell and the running flux sums stay in the
+// thread's registers; the face states toward the upper x and y faces go to shared memory so that
+// the next thread can solve its lower face, and the x and y fluxes so that both cells read them
+// (two float4 a thread and face). Each face flux is computed once and used by both cells, so both
+// sides see bit-identical fluxes (the reference's flux-determinism check,
 // src/validation/tests.ts:961).
 //
 // The arithmetic follows the reference's CPU scheme, src/reference/hydro.ts (RefHydro), in
@@ -63,7 +65,7 @@ struct Geo {
   // needs the registers more than the wider columns: at 80 it spilled, and 16 x 12 columns with
   // 128 registers ran 6 % faster than 16 x 16 with 80 (the PPM Taylor-Green vortex at 512^3).
   static constexpr int MAXREG = (DIM == 1) ? 64 : (DIM == 3) ? 128 : 80;
-  static constexpr size_t BASE_FLOATS = (size_t)NBUF * WC * WN + (size_t)NF * 7 * PN + (size_t)NF * 8 * PN + 32;
+  static constexpr size_t BASE_FLOATS = (size_t)NBUF * WC * WN + (size_t)NF * 8 * PN + (size_t)NF * 8 * PN + 32;
   // 3D: a staging area for one plane's conserved state, u1 box then u2 box (float4, x fastest),
   // filled by a tiled TMA copy; both boxes start on 128-byte boundaries.
   static constexpr size_t STAGE_OFS = (BASE_FLOATS + 31) / 32 * 32;
@@ -93,7 +95,7 @@ __device__ __forceinline__ void load_w_plane(const KParams& P, const float4* __r
     float w[6];
     prim6_from_cons(a, b, P, fx, fy, fz, w);
 #pragma unroll
-    for (int c = 0; c < 6; c++) sWb[c * G::WN + idx] = w[c];
+    for (int c = 0; c < 3; c++) reinterpret_cast<float2*>(sWb)[c * G::WN + idx] = make_float2(w[2 * c], w[2 * c + 1]);
   }
 }
 
@@ -102,7 +104,25 @@ template <int DIM, int RECON>
 __device__ __forceinline__ void read_w(const float* __restrict__ sWb, int wx, int wy, float* w) {
   using G = Geo<DIM, RECON>;
 #pragma unroll
-  for (int c = 0; c < 6; c++) w[c] = sWb[c * G::WN + wy * G::WX + wx];
+  for (int c = 0; c < 3; c++) {
+    const float2 t = reinterpret_cast<const float2*>(sWb)[c * G::WN + wy * G::WX + wx];
+    w[2 * c] = t.x;
+    w[2 * c + 1] = t.y;
+  }
+}
+
+__device__ __forceinline__ void unpack7(const float4 a, const float4 b, float* f) {
+  f[0] = a.x;
+  f[1] = a.y;
+  f[2] = a.z;
+  f[3] = a.w;
+  f[4] = b.x;
+  f[5] = b.y;
+  f[6] = b.z;
+}
+__device__ __forceinline__ void unpack8(const float4 a, const float4 b, float* f) {
+  unpack7(a, b, f);
+  f[7] = b.w;
 }
 
 __device__ __forceinline__ float warp_max(float v) {
@@ -140,9 +160,11 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, REC
   constexpr int H = G::H, ZH = G::ZH, PX = G::PX, PN = G::PN, WN = G::WN, WC = G::WC;
   extern __shared__ __align__(128) float smem[];
   float* sW = smem;
-  float* sFace = sW + G::NBUF * WC * WN;
-  float* sFlux = sFace + G::NF * 7 * PN;
-  float* sRed = sFlux + G::NF * 8 * PN;
+  // face states and fluxes as two float4 a thread per face direction (k = 0 x, 1 y): entries
+  // (2k) * PN + tid and (2k + 1) * PN + tid
+  float4* sFace = reinterpret_cast<float4*>(sW + G::NBUF * WC * WN);
+  float4* sFlux = sFace + G::NF * 2 * PN;
+  float* sRed = reinterpret_cast<float*>(sFlux + G::NF * 2 * PN);
 
   const int tid = threadIdx.x;
   const int tx = tid % PX, ty = tid / PX;
@@ -276,7 +298,7 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, REC
         float w[6];
         prim6_from_cons(stage1[idx], stage2[idx], P, 1.f, 1.f, stage_fz, w);
 #pragma unroll
-        for (int c = 0; c < 6; c++) dst[c * WN + idx] = w[c];
+        for (int c = 0; c < 3; c++) reinterpret_cast<float2*>(dst)[c * WN + idx] = make_float2(w[2 * c], w[2 * c + 1]);
       }
       __syncthreads();
       // the staging area is free again: the next plane's copy overlaps this plane's work
@@ -304,10 +326,11 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, REC
     // the z edge increments of this plane's cell (c; m, p below and above) from the carried
     // slopes and the new one at plane j + 1; the slopes then move up a plane
     auto z_edges = [&](const float* m, const float* c, const float* p, float* su_z, float* sd_z) {
-      const float* p2s = ring(j + 2) + wy * G::WX + wx;
+      float p2v[6];
+      read_w<DIM, RECON>(ring(j + 2), wx, wy, p2v);
 #pragma unroll
       for (int v = 0; v < 6; v++) {
-        const float zp = ppm_slope(c[v], p[v], p2s[v * WN]);
+        const float zp = ppm_slope(c[v], p[v], p2v[v]);
         ppm_incs_d(m[v], c[v], p[v], zs_m[v], zs_0[v], zp, su_z[v], sd_z[v]);
         zs_m[v] = zs_0[v];
         zs_0[v] = zp;
@@ -406,17 +429,20 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, REC
     const bool tile_plane = j >= z0 && j < z1;
     // 3. ghosts across outflow / reflecting x/y boundaries take the inner cell's half step.
     if (xyg && tile_plane) {
-#pragma unroll
-      for (int v = 0; v < 6; v++) sFlux[v * PN + tid] = pr.q[v];
-      sFlux[6 * PN + tid] = pr.flag;
-      sFlux[7 * PN + tid] = pr.fo ? 1.f : 0.f;
+      sFlux[tid] = make_float4(pr.q[0], pr.q[1], pr.q[2], pr.q[3]);
+      sFlux[PN + tid] = make_float4(pr.q[4], pr.q[5], pr.flag, pr.fo ? 1.f : 0.f);
       __syncthreads();
       if (g_src >= 0) {
-#pragma unroll
-        for (int v = 0; v < 6; v++) pr.q[v] = sFlux[v * PN + g_src];
+        const float4 a = sFlux[g_src], b = sFlux[PN + g_src];
+        pr.q[0] = a.x;
+        pr.q[1] = a.y;
+        pr.q[2] = a.z;
+        pr.q[3] = a.w;
+        pr.q[4] = b.x;
+        pr.q[5] = b.y;
+        pr.flag = b.z;
+        pr.fo = b.w != 0.f;
         if (g_flip) pr.q[1 + g_axis] = -pr.q[1 + g_axis];
-        pr.flag = sFlux[6 * PN + g_src];
-        pr.fo = sFlux[7 * PN + g_src] != 0.f;
       }
     }
     if constexpr (DIM == 3) {
@@ -432,12 +458,12 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, REC
     if (tile_plane) {
       float f[7];
       face_state(pr, su[0], 1.f, f);
-#pragma unroll
-      for (int v = 0; v < 7; v++) sFace[v * PN + tid] = f[v];
+      sFace[tid] = make_float4(f[0], f[1], f[2], f[3]);
+      sFace[PN + tid] = make_float4(f[4], f[5], f[6], 0.f);
       if constexpr (DIM >= 2) {
         face_state(pr, su[1], 1.f, f);
-#pragma unroll
-        for (int v = 0; v < 7; v++) sFace[(7 + v) * PN + tid] = f[v];
+        sFace[2 * PN + tid] = make_float4(f[0], f[1], f[2], f[3]);
+        sFace[3 * PN + tid] = make_float4(f[4], f[5], f[6], 0.f);
       }
     }
     const bool flagged = __syncthreads_or(pr.flag != 0.f);
@@ -448,22 +474,20 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, REC
     if (tile_plane) {
       if (xface_t) {
         float L[7], R[7], F[8];
-#pragma unroll
-        for (int v = 0; v < 7; v++) L[v] = sFace[v * PN + tid - 1];
+        unpack7(sFace[tid - 1], sFace[PN + tid - 1], L);
         face_state(pr, sd[0], -1.f, R);
         riemann<0>(L, R, P, F, hll_any);
-#pragma unroll
-        for (int v = 0; v < 8; v++) sFlux[v * PN + tid] = F[v];
+        sFlux[tid] = make_float4(F[0], F[1], F[2], F[3]);
+        sFlux[PN + tid] = make_float4(F[4], F[5], F[6], F[7]);
       }
       if constexpr (DIM >= 2) {
         if (yface_t) {
           float L[7], R[7], F[8];
-#pragma unroll
-          for (int v = 0; v < 7; v++) L[v] = sFace[(7 + v) * PN + tid - PX];
+          unpack7(sFace[2 * PN + tid - PX], sFace[3 * PN + tid - PX], L);
           face_state(pr, sd[1], -1.f, R);
           riemann<1>(L, R, P, F, hll_any);
-#pragma unroll
-          for (int v = 0; v < 8; v++) sFlux[(8 + v) * PN + tid] = F[v];
+          sFlux[2 * PN + tid] = make_float4(F[0], F[1], F[2], F[3]);
+          sFlux[3 * PN + tid] = make_float4(F[4], F[5], F[6], F[7]);
         }
       }
     }
@@ -492,13 +516,20 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, REC
         }
       }
       if (tile_plane) {
+        float xl[8], xu[8], yl[8], yu[8];
+        unpack8(sFlux[tid], sFlux[PN + tid], xl);
+        unpack8(sFlux[tid + 1], sFlux[PN + tid + 1], xu);
+        if constexpr (DIM >= 2) {
+          unpack8(sFlux[2 * PN + tid], sFlux[3 * PN + tid], yl);
+          unpack8(sFlux[2 * PN + tid + PX], sFlux[3 * PN + tid + PX], yu);
+        }
 #pragma unroll
         for (int v = 0; v < 8; v++) {
-          float a = sFlux[v * PN + tid];
-          a -= sFlux[v * PN + tid + 1];
+          float a = xl[v];
+          a -= xu[v];
           if constexpr (DIM >= 2) {
-            a += sFlux[(8 + v) * PN + tid];
-            a -= sFlux[(8 + v) * PN + tid + PX];
+            a += yl[v];
+            a -= yu[v];
           }
           if constexpr (DIM == 3) a += Fz[v];
           acc[v] = a;
