@@ -73,8 +73,8 @@ def parse():
     ap.add_argument("--profile-window", action="store_true",
                     help="AMR section: bracket one step after the warm-up with cudaProfilerStart/Stop")
     ap.add_argument("--pin-assemble", type=int, default=None, metavar="V",
-                    help="AMR section: fix the assemble's launch shape to variant V (0-2 one pass, 3-4 split) "
-                         "instead of the tuned one, e.g. to profile one form")
+                    help="AMR section: fix the assemble's launch shape to variant V (0-2 one pass, 3-4 split, "
+                         "5-6 split side by side) instead of the tuned one, e.g. to profile one form")
     ap.add_argument("--slabs", action="store_true",
                     help="the z-slab driver also at N = 1 (one periodic slab exchanging with itself)")
     return ap.parse_args()

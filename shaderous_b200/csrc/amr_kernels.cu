@@ -679,8 +679,9 @@ cudaError_t assemble_v(const AmrLaunch& L, int g, const int* list, int n, const 
 // of the ghosts with the MINB register budget.
 template <bool BINS>
 cudaError_t assemble_plain(const AmrLaunch& L, const int* list, int n, const float4* u1, const float4* u2,
-                           unsigned* rates, int rslot, cudaStream_t s, const int* bins, float* brate) {
-  const int g = grid_for(n, 4);
+                           unsigned* rates, int rslot, cudaStream_t s, const int* bins, float* brate,
+                           int per_sm = 4) {
+  const int g = grid_for(n, per_sm);
   if (L.ndim == 3)
     amrk::amr_assemble_plain<3, BINS><<<g, amrk::NT, 0, s>>>(L.gp, L.bt, list, n, u1, u2, L.w1, L.w2, rates, rslot, bins, brate);
   else
@@ -702,6 +703,32 @@ cudaError_t assemble_split(const AmrLaunch& L, int per_sm, const int* list, int 
   }
   return cudaSuccess;
 }
+// The split form with its passes side by side: the second (a latency-bound gather of coarse cells
+// and restrictions) on the side stream at per_sm CTAs an SM, beside the first (bandwidth-bound) at
+// 2 CTAs an SM, so that both are resident at once (the plain pass's 2 x 256 threads x 64 registers
+// and the second pass's per_sm x 256 x 128 at most fill one SM's register file).
+template <int MINB>
+cudaError_t assemble_split_side(const AmrLaunch& L, int per_sm, const int* list, int n, const float4* u1,
+                                const float4* u2, unsigned* rates, int rslot, cudaStream_t s) {
+  if (!L.side || !L.fork || !L.join || L.nrest == 0) return assemble_split<MINB>(L, per_sm, list, n, u1, u2, rates, rslot, s);
+  cudaError_t e = cudaEventRecord(L.fork, s);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(L.side, L.fork, 0);
+  if (e != cudaSuccess) return e;
+  const int* rl = L.nrest > 0 ? L.rest : list;
+  const int rn = L.nrest > 0 ? L.nrest : n;
+  const int g = grid_for(rn, per_sm);
+  if (L.ndim == 3) {
+    SHZ_RECON_SWITCH(L.recon, false, (e = assemble_t<3, R, MINB, false, true>(L, g, rl, rn, u1, u2, rates, rslot, L.side)))
+  } else {
+    SHZ_RECON_SWITCH(L.recon, false, (e = assemble_t<2, R, MINB, false, true>(L, g, rl, rn, u1, u2, rates, rslot, L.side)))
+  }
+  // the join is recorded and waited for whatever the launches returned, so that a capture in
+  // progress ends with the side stream joined
+  const cudaError_t e2 = assemble_plain<false>(L, list, n, u1, u2, rates, rslot, s, nullptr, nullptr, 2);
+  const cudaError_t e3 = cudaEventRecord(L.join, L.side);
+  const cudaError_t e4 = cudaStreamWaitEvent(s, L.join, 0);
+  return e != cudaSuccess ? e : e2 != cudaSuccess ? e2 : e3 != cudaSuccess ? e3 : e4;
+}
 }  // namespace
 
 cudaError_t amr_launch_assemble(const AmrLaunch& L, const int* list, int n, const float4* u1, const float4* u2,
@@ -714,6 +741,8 @@ cudaError_t amr_launch_assemble(const AmrLaunch& L, const int* list, int n, cons
     case 2: return assemble_v<3>(L, g, list, n, u1, u2, rates, rslot, s);
     case 3: return assemble_split<2>(L, per_sm, list, n, u1, u2, rates, rslot, s);
     case 4: return assemble_split<3>(L, per_sm, list, n, u1, u2, rates, rslot, s);
+    case 5: return assemble_split_side<2>(L, per_sm, list, n, u1, u2, rates, rslot, s);
+    case 6: return assemble_split_side<3>(L, per_sm, list, n, u1, u2, rates, rslot, s);
     default: return assemble_v<1>(L, g, list, n, u1, u2, rates, rslot, s);
   }
 }

@@ -41,6 +41,11 @@ struct AmrLaunch {
   // assemble is given); nrest < 0: every block of that list.
   const int* rest = nullptr;
   int nrest = -1;
+  // The owner's second stream and two events (all null: none): the split assemble's two passes
+  // write disjoint texels and read only the state, so variants 5 and 6 run the second on `side`
+  // beside the first (fork and join order it against the owner's stream, graph capture included).
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
 };
 
 // The blocks of `list` (n slots; bt the host copy of the block table, 32 ints a row) with a ghost

@@ -891,6 +891,10 @@ int shz_amr_create(const shz_amr_config* cfg, shz_amr** out) {
   };
   const size_t cap = c.cap;
   if (cudaStreamCreateWithFlags(&a->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(SHZ_E_CUDA, "stream");
+  if (cudaStreamCreateWithFlags(&a->L.side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&a->L.fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&a->L.join, cudaEventDisableTiming) != cudaSuccess)
+    return bail(SHZ_E_CUDA, "side stream");
   bool ok = true;
   for (int p = 0; p < 2; p++) {
     ok = ok && cudaMalloc(&a->u1[p], cap * a->CB * sizeof(float4)) == cudaSuccess;
@@ -977,6 +981,9 @@ void shz_amr_destroy(shz_amr* a) {
   if (a->h_cyc) cudaFreeHost(a->h_cyc);
   if (a->bins_ready) cudaEventDestroy(a->bins_ready);
   if (a->stream) cudaStreamDestroy(a->stream);
+  if (a->L.fork) cudaEventDestroy(a->L.fork);
+  if (a->L.join) cudaEventDestroy(a->L.join);
+  if (a->L.side) cudaStreamDestroy(a->L.side);
   delete a;
 }
 

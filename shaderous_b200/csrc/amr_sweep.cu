@@ -840,9 +840,14 @@ cudaError_t amr_assemble_tuned(const AmrLaunch& L, const int* list, int n, const
   std::vector<tune::Choice> cands;
   for (int v : {0, 1, 2})
     for (int p : {4, 2, 8}) cands.push_back(mk(v, p));
-  // the split form (variants 3, 4): the plain pass, then the rest at 2 or 3 CTAs' register budget
+  // the split form (variants 3, 4): the plain pass, then the rest at 2 or 3 CTAs' register budget;
+  // (5, 6) the same two passes side by side, the second at 1 CTA an SM beside the first's 2
   for (int v : {3, 4})
     for (int p : {2, 4}) cands.push_back(mk(v, p));
+  if (L.side) {
+    cands.push_back(mk(5, 1));
+    cands.push_back(mk(6, 1));
+  }
   long long second = 0;  // the split form's second kernels (when the host listed blocks for them)
   const cudaError_t e = run_tuned(amr_tune_key(tune::K_AMR_ASSEMBLE, L, n), cands, tune_now, s,
                                   [&](const tune::Choice* c) {

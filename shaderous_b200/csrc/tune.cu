@@ -141,9 +141,9 @@ int shz_tune_pin(int32_t kernel, int32_t variant, int32_t per_sm) {
     shz::tune::pin(kernel, nullptr);
     return 0;
   }
-  // the variants each kernel compiles (the assemble's 0-4, the substeps' assemble's 1 and 3; the
+  // the variants each kernel compiles (the assemble's 0-6, the substeps' assemble's 1 and 3; the
   // others' 0)
-  const bool ok = kernel == shz::tune::K_AMR_ASSEMBLE        ? variant <= 4
+  const bool ok = kernel == shz::tune::K_AMR_ASSEMBLE        ? variant <= 6
                   : kernel == shz::tune::K_AMR_ASSEMBLE_BINS ? (variant == 1 || variant == 3)
                                                              : variant == 0;
   if (!ok || per_sm < 0 || per_sm > 32) return SHZ_E_CONFIG;

@@ -96,10 +96,11 @@ def _pinned_amr(variant, ndim, two_pass, bcs):
 def test_every_assemble_variant_gives_the_same_state(ndim, two_pass, bcs):
     """The one-pass assemble at each register budget and the split form (a light pass for own cells
     and same-level ghosts, then the ghosts beyond level changes over only the blocks the host lists
-    for them) on refined meshes with walls, outflow and periodic faces: the same state bit for bit."""
+    for them; in order, or side by side on two streams) on refined meshes with walls, outflow and
+    periodic faces: the same state bit for bit."""
     ref = _pinned_amr(0, ndim, two_pass, bcs)
     assert len(set(ref[0].tolist())) > 1  # the mesh has level changes
-    for v in (1, 2, 3, 4):
+    for v in (1, 2, 3, 4, 5, 6):
         lv, co, (u1, u2) = _pinned_amr(v, ndim, two_pass, bcs)
         assert (lv == ref[0]).all() and (co == ref[1]).all()
         assert np.array_equal(u1, ref[2][0]) and np.array_equal(u2, ref[2][1]), v
