@@ -283,7 +283,16 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, REC
   constexpr bool ZCARRY = RECON == R_PPM && DIM == 3;
   float zs_m[6], zs_0[6];
   bool zs_ready = false;
-  for (int j = jb; j <= je; j++) {
+  // the ring slot of plane j, advanced with j (a plane k planes away from j is in slot sj + k,
+  // wrapped), instead of two remainders by NBUF per access
+  int sj = ((jb % G::NBUF) + G::NBUF) % G::NBUF;
+  auto ringk = [&](int k) -> float* {
+    int s = sj + k;
+    s = s >= G::NBUF ? s - G::NBUF : s;
+    s = s < 0 ? s + G::NBUF : s;
+    return sW + s * WC * WN;
+  };
+  for (int j = jb; j <= je; j++, sj = (sj + 1 == G::NBUF) ? 0 : sj + 1) {
     // 1. primitives of plane j + ZH (the plane itself when there is no march)
     const int lp = (DIM == 3) ? j + ZH : 0;
     if (tma_tile) {
@@ -293,7 +302,7 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, REC
         if (tid == 0 && err) atomicExch(err, tma::ERR_TMA_TIMEOUT);
         return;
       }
-      float* dst = ring(lp);
+      float* dst = ringk((DIM == 3) ? ZH : 0);
       for (int idx = tid; idx < WN; idx += G::NT) {
         float w[6];
         prim6_from_cons(stage1[idx], stage2[idx], P, 1.f, 1.f, stage_fz, w);
@@ -304,17 +313,17 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, REC
       // the staging area is free again: the next plane's copy overlaps this plane's work
       if (j + 1 <= je) issue_plane(j + 1 + ZH);
     } else {
-      load_w_plane<DIM, RECON>(P, u1, u2, x0, y0, lp, ring(lp));
+      load_w_plane<DIM, RECON>(P, u1, u2, x0, y0, lp, ringk((DIM == 3) ? ZH : 0));
       __syncthreads();
     }
-    const float* sWj = ring((DIM == 3) ? j : 0);
+    const float* sWj = ringk(0);
     if constexpr (ZCARRY) {
       if (!zs_ready) {
         float c2[7], c1[7], a0[7], b1[7];
-        read_w<DIM, RECON>(ring(j - 2), wx, wy, c2);
-        read_w<DIM, RECON>(ring(j - 1), wx, wy, c1);
+        read_w<DIM, RECON>(ringk(-2), wx, wy, c2);
+        read_w<DIM, RECON>(ringk(-1), wx, wy, c1);
         read_w<DIM, RECON>(sWj, wx, wy, a0);
-        read_w<DIM, RECON>(ring(j + 1), wx, wy, b1);
+        read_w<DIM, RECON>(ringk(1), wx, wy, b1);
 #pragma unroll
         for (int v = 0; v < 6; v++) {
           zs_m[v] = ppm_slope(c2[v], c1[v], a0[v]);
@@ -327,7 +336,7 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, REC
     // slopes and the new one at plane j + 1; the slopes then move up a plane
     auto z_edges = [&](const float* m, const float* c, const float* p, float* su_z, float* sd_z) {
       float p2v[6];
-      read_w<DIM, RECON>(ring(j + 2), wx, wy, p2v);
+      read_w<DIM, RECON>(ringk(2), wx, wy, p2v);
 #pragma unroll
       for (int v = 0; v < 6; v++) {
         const float zp = ppm_slope(c[v], p[v], p2v[v]);
@@ -346,8 +355,8 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, REC
         float c[7], m[7], p[7], m2[7], p2[7], su[6], sd[6];
         read_w<DIM, RECON>(sWj, wx, wy, c);
         with_cs(c, P);
-        read_w<DIM, RECON>(ring(j - 1) + 0, wx, wy, m);
-        read_w<DIM, RECON>(ring(j + 1) + 0, wx, wy, p);
+        read_w<DIM, RECON>(ringk(-1), wx, wy, m);
+        read_w<DIM, RECON>(ringk(1), wx, wy, p);
         if constexpr (ZCARRY) {
           (void)m2;
           (void)p2;
@@ -411,8 +420,8 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, REC
         jump = fmaxf(jump, jump_excess(m[4], p[4], P.shock_thresh));
       }
       if constexpr (DIM == 3) {
-        read_w<DIM, RECON>(ring(j - 1), wx, wy, m);
-        read_w<DIM, RECON>(ring(j + 1), wx, wy, p);
+        read_w<DIM, RECON>(ringk(-1), wx, wy, m);
+        read_w<DIM, RECON>(ringk(1), wx, wy, p);
         if constexpr (ZCARRY) {
           z_edges(m, c, p, su[2], sd[2]);
         } else {
