@@ -491,11 +491,15 @@ const char* shz_version(void);
  * fastest in a process-wide table, and uses it from then on (also in captured CUDA graphs).
  * Candidates differ only in launch shape, never in arithmetic: the state is the same whichever
  * wins. Kernels and their knobs:
- *   0 uniform sweep: tz = planes a CTA marches along z (3D);
+ *   0 uniform sweep: tz = planes a CTA marches along z (3D); in 2D grids of at least 512 cells
+ *     a side, the rows a CTA marches along y (smaller 2D grids take a tile form, 16 x 12 cells
+ *     with a ring of halo cells, untuned; the two forms agree to rounding, each depth of one form
+ *     gives the same bits);
  *   1 AMR assemble: variant = register budget (0: 1, 1: 2, 2: 3 CTAs per SM) of the one-pass
  *     kernel, or the split form (3: 2, 4: 3 CTAs per SM for its second pass): a light first
  *     pass for the blocks' own cells and same-level ghosts, then the ghosts beyond a level
- *     change over only the blocks that have them; per_sm = CTAs of the work-list grid per SM;
+ *     change over only the blocks that have them; 5, 6: the split form with its two passes side
+ *     by side on a second stream; per_sm = CTAs of the work-list grid per SM;
  *   2 AMR fused sweep: per_sm;
  *   3 AMR fine-flux pass: per_sm;
  *   4 the per-block-timestep substeps' assemble: variant 1 one pass, 3 the split form (its
@@ -509,8 +513,9 @@ typedef struct shz_tune_entry {
 } shz_tune_entry;
 /* Turn the tuner on (default) or off (every launch takes the default shape). Process-wide. */
 int shz_tune_enable(int32_t on);
-/* Pin one AMR kernel's choice (kernel 1-4 above; variant, per_sm with 0 for the default grid)
- * for every key, used instead of the tuned one; variant < 0 unpins. Process-wide. */
+/* Pin one kernel's choice for every key, used instead of the tuned one; variant < 0 unpins.
+ * Process-wide. AMR kernels (1-4 above): variant, per_sm with 0 for the default grid. The uniform
+ * sweep (0): variant 0 and per_sm = its depth tz (0-1024; in 2D 0 is the tile form). */
 int shz_tune_pin(int32_t kernel, int32_t variant, int32_t per_sm);
 /* Forget every choice. */
 void shz_tune_reset(void);

@@ -174,7 +174,7 @@ __device__ __forceinline__ void axis_edges(const float* m2, const float* m, cons
 // path; the values computed for the regions not chosen are discarded.
 // hll_any: false when the caller knows that neither side of any face it solves is shock-flagged
 // (a CTA-uniform fact, so the branch does not diverge). The HLL flux then has weight 0 and is
-// skipped: c + (h - c) * 0 is c for a finite h, up to the sign of an exact zero.
+// skipped; a face of weight 0 takes the HLLC flux as it is either way.
 template <int AXIS>
 __device__ __forceinline__ void riemann(const float* L, const float* R, const KParams& P, float* F,
                                         bool hll_any = true) {
@@ -223,11 +223,14 @@ __device__ __forceinline__ void riemann(const float* L, const float* R, const KP
     const float hp1 = (sr * fpl1 - sl * fpr1 + slsr * (mr1 - ml1)) * inv;
     const float hp2 = (sr * fpl2 - sl * fpr2 + slsr * (mr2 - ml2)) * inv;
     const float he = (sr * fel - sl * fer + slsr * (er - el)) * inv;
-    m = cm + (hm - cm) * w_hll;
-    p0 = c0 + (hp0 - c0) * w_hll;
-    p1 = c1 + (hp1 - c1) * w_hll;
-    p2 = c2 + (hp2 - c2) * w_hll;
-    e = ce + (he - ce) * w_hll;
+    // a face of weight 0 keeps the HLLC flux exactly, as where the HLL one was skipped: the
+    // result does not depend on which faces share a CTA (c + (h - c) * 0 can turn -0 into +0)
+    const bool blend = w_hll != 0.f;
+    m = blend ? cm + (hm - cm) * w_hll : cm;
+    p0 = blend ? c0 + (hp0 - c0) * w_hll : c0;
+    p1 = blend ? c1 + (hp1 - c1) * w_hll : c1;
+    p2 = blend ? c2 + (hp2 - c2) * w_hll : c2;
+    e = blend ? ce + (he - ce) * w_hll : ce;
   }
   float vn = sm;
   // supersonic faces take the upwind side's flux

@@ -190,21 +190,35 @@ int refresh_rate(shz_sim* s) {
   return 0;
 }
 
-// The autotuner's key of this grid's sweep, and its tuned z depth (0: the default).
+// The autotuner's key of this grid's sweep, and its depth: in 3D the planes a CTA marches along z
+// (0: the default); in 2D the rows a CTA marches along y, 0 for the tile form. Which 2D form runs
+// is fixed by the grid's size, not by timing: the two forms are different kernels, which agree to
+// rounding (the compiler may contract a multiply and an add differently in each), while every
+// depth of one form is the same kernel and gives the same bits. 2D grids of at least 512 cells a
+// side march along y, at a tuned depth (16 rows untuned); smaller ones take the tile form.
 shz::tune::Key sweep_key(const shz_sim* s) {
   return shz::tune::Key{shz::tune::K_UNIFORM_SWEEP, s->ndim, s->cfg.recon,
                         (s->cfg.isentropic != 0 && s->cfg.recon != SHZ_RECON_PPM) ? 1 : 0,
                         shz::tune::size_class((long long)s->ncell)};
 }
+constexpr int ROWS_MIN_SIDE = 512, ROWS_DEFAULT = 16;
+bool rows_form(const shz_sim* s) { return s->ndim == 2 && s->cfg.n[0] >= ROWS_MIN_SIDE && s->cfg.n[1] >= ROWS_MIN_SIDE; }
 int sweep_tz(const shz_sim* s) {
   shz::tune::Choice c;
-  return (s->ndim == 3 && shz::tune::lookup(sweep_key(s), &c)) ? c.tz : 0;
+  if (s->ndim >= 2 && shz::tune::pinned(shz::tune::K_UNIFORM_SWEEP, &c)) return c.tz;
+  if (s->ndim == 3) return shz::tune::lookup(sweep_key(s), &c) ? c.tz : 0;
+  if (!rows_form(s)) return 0;
+  return shz::tune::lookup(sweep_key(s), &c) ? c.tz : ROWS_DEFAULT;
 }
-bool wants_tuning(const shz_sim* s) { return s->ndim == 3 && shz::tune::needs(sweep_key(s)); }
+bool wants_tuning(const shz_sim* s) {
+  shz::tune::Choice c;
+  return (s->ndim == 3 || rows_form(s)) && !shz::tune::pinned(shz::tune::K_UNIFORM_SWEEP, &c) &&
+         shz::tune::needs(sweep_key(s));
+}
 
-// One step whose sweep is run once per candidate z depth, timed, the fastest kept. The sweep
-// reads one parity and writes the other (and folds the same rate maximum), so the step's result
-// is that of a single launch. A clock held at its stop time is not tuned on (the sweep would
+// One step whose sweep is run once per candidate depth (z planes in 3D, y rows in 2D), timed, the
+// fastest kept. The sweep reads one parity and writes the other (and folds the
+// same rate maximum), so the step's result is that of a single launch. A clock held at its stop time is not tuned on (the sweep would
 // only copy the state).
 int tuned_step(shz_sim* s) {
   CUDA_OR_FAIL(s, shz::launch_clock(s->clk, s->rates, s->slot, s->stream));
@@ -221,11 +235,20 @@ int tuned_step(shz_sim* s) {
     s->launches += 1;
   } else {
     std::vector<shz::tune::Choice> cands;
-    for (int tz : {shz::SWEEP_TZ_DEFAULT, 32, 128, 256}) {
-      if (tz != shz::SWEEP_TZ_DEFAULT && tz > s->cfg.n[2]) continue;
-      shz::tune::Choice c;
-      c.tz = tz;
-      cands.push_back(c);
+    if (s->ndim == 3) {
+      for (int tz : {shz::SWEEP_TZ_DEFAULT, 32, 128, 256}) {
+        if (tz != shz::SWEEP_TZ_DEFAULT && tz > s->cfg.n[2]) continue;
+        shz::tune::Choice c;
+        c.tz = tz;
+        cands.push_back(c);
+      }
+    } else {
+      // the march along y at 8-64 rows a CTA (deeper marches leave too few CTAs)
+      for (int rows : {ROWS_DEFAULT, 8, 32, 64}) {
+        shz::tune::Choice c;
+        c.tz = rows;
+        cands.push_back(c);
+      }
     }
     const int reps = 2;
     shz::tune::Choice best;

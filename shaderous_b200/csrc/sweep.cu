@@ -565,6 +565,324 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, REC
   block_max_to<G::NT>(rate_max, sRed, rate_out);
 }
 
+// ---------------------------------------------------------------------------------------------
+// The 2D step as a march along y. A CTA owns a row segment of RTX cells and marches it up through
+// `rows` rows, as the 3D sweep marches its columns along z: its threads are the segment's cells
+// plus one halo cell at each end, the primitives of the rows the predictor reads along y sit in a
+// ring of rows in shared memory, and the y face below a cell and the running flux sums stay in the
+// thread's registers. Against the 2D tile form (16 x 12 cells with a ring of halo cells) it runs
+// the predictor 1.02 times per cell instead of 1.31 and converts each row once; the arithmetic per
+// cell is the same functions in the same order, so both forms give the same state.
+template <int RECON>
+struct RowGeo {
+  static constexpr int H = (RECON == R_PPM) ? 3 : 2;   // halo of a row of primitives
+  static constexpr int ZH = (RECON == R_PPM) ? 2 : 1;  // rows each way the predictor reads along y
+  static constexpr int TX = 126;                       // cells of a CTA's row segment
+  static constexpr int PX = TX + 2;                    // threads: the segment and a halo cell each end
+  static constexpr int NT = PX;
+  static constexpr int WX = TX + 2 * H;                // texels of a row of primitives
+  static constexpr int WC = 6;
+  static constexpr int NBUF = 2 * ZH + 1;
+  static constexpr size_t SMEM_FLOATS = (size_t)NBUF * WC * WX + (size_t)2 * 4 * PX + (size_t)2 * 4 * PX + 32;
+  static constexpr size_t SMEM_BYTES = SMEM_FLOATS * sizeof(float);
+  static_assert((NBUF * WC * WX) % 4 == 0, "the face states start on a 16-byte boundary");
+};
+
+// Primitives of row r of the segment's region (through the y and x boundary mappings) into a ring
+// slot: float2 pairs (rho vx, vy vz, p s), as the 3D sweep's planes.
+template <int RECON>
+__device__ __forceinline__ void load_w_row(const KParams& P, const float4* __restrict__ u1, const float4* __restrict__ u2,
+                                           int x0, int r, float* __restrict__ dst) {
+  using G = RowGeo<RECON>;
+  float fy;
+  const int gy = bc_map(r, P.n[1], P.bc_lo[1], P.bc_hi[1], fy);
+  const ptrdiff_t yoff = (ptrdiff_t)gy * P.n[0];
+  for (int idx = threadIdx.x; idx < G::WX; idx += G::NT) {
+    float fx;
+    const int gx = bc_map(x0 - G::H + idx, P.n[0], P.bc_lo[0], P.bc_hi[0], fx);
+    const float4 a = __ldg(u1 + yoff + gx), b = __ldg(u2 + yoff + gx);
+    float w[6];
+    prim6_from_cons(a, b, P, fx, fy, 1.f, w);
+#pragma unroll
+    for (int c = 0; c < 3; c++) reinterpret_cast<float2*>(dst)[c * G::WX + idx] = make_float2(w[2 * c], w[2 * c + 1]);
+  }
+}
+
+template <int RECON>
+__device__ __forceinline__ void read_row(const float* __restrict__ sWr, int wx, float* w) {
+  using G = RowGeo<RECON>;
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const float2 t = reinterpret_cast<const float2*>(sWr)[c * G::WX + wx];
+    w[2 * c] = t.x;
+    w[2 * c + 1] = t.y;
+  }
+}
+
+template <int RECON, bool ISEN>
+// (5 CTAs of 4 warps per SM: 96 registers a thread; at 128 and 4 CTAs, or at 80 and 6 with spills,
+// the Kelvin-Helmholtz march ran 4-8 % slower)
+__global__ void __launch_bounds__(RowGeo<RECON>::NT, 5)
+    sweep_rows_kernel(const KParams P, const float4* __restrict__ u1, const float4* __restrict__ u2,
+                      float4* __restrict__ o1, float4* __restrict__ o2, const DevClock* __restrict__ clk,
+                      unsigned* __restrict__ rate_out, int rows) {
+  using G = RowGeo<RECON>;
+  constexpr int H = G::H, ZH = G::ZH, PX = G::PX, WX = G::WX, WC = G::WC;
+  extern __shared__ __align__(128) float smem[];
+  float* sW = smem;
+  float4* sFace = reinterpret_cast<float4*>(sW + G::NBUF * WC * WX);  // upper x face states, 2 a thread
+  float4* sFlux = sFace + 2 * PX;                                     // lower x face fluxes, 2 a thread
+  float* sRed = reinterpret_cast<float*>(sFlux + 2 * PX);
+
+  const int tid = threadIdx.x;
+  const int x0 = blockIdx.x * G::TX;
+  const int gx = x0 - 1 + tid;
+  const int wx = tid + H - 1;
+  const int nx = P.n[0], ny = P.n[1];
+  const bool col_t = tid >= 1 && tid <= G::TX && gx < nx;             // updates cell gx
+  const bool xface_t = tid >= 1 && tid <= G::TX + 1 && gx <= nx;       // solves the x face below gx
+  const int y0 = blockIdx.y * rows, y1 = min(y0 + rows, ny);
+
+  const double dt = clk->dt;
+  const float dtdx = (float)(dt / P.dx);
+  const float h = (float)((0.5 * dt) / P.dx);
+  float rate_max = 0.f;
+
+  if (clk->held) {
+    if (col_t)
+      for (int y = y0; y < y1; y++) {
+        const size_t o = (size_t)y * nx + gx;
+        const float4 a = u1[o], b = u2[o];
+        o1[o] = a;
+        o2[o] = b;
+        rate_max = fmaxf(rate_max, rate_guard(signal_rate(a, b, P)));
+      }
+    block_max_to<G::NT>(rate_max, sRed, rate_out);
+    return;
+  }
+
+  // x ghosts across an outflow or reflecting face take the inner cell's half step (hydro.ts:335-342)
+  const bool xg_lo = x0 == 0 && P.bc_lo[0] != 0;
+  const bool xg_hi = x0 + G::TX >= nx && P.bc_hi[0] != 0;
+  const bool xg = xg_lo || xg_hi;
+  int g_src = -1;
+  bool g_flip = false;
+  if (xg_lo && gx == -1) { g_src = tid + 1; g_flip = P.bc_lo[0] == 2; }
+  if (xg_hi && gx == nx) { g_src = tid - 1; g_flip = P.bc_hi[0] == 2; }
+
+  float yhi_prev[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // face state below the upper y face of row j-1
+  float q_prev[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  float flag_prev = 0.f;
+  bool fo_prev = false;
+  float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  float ph_prev = 0.f;
+  float gsu[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // edges of the lower y ghost (outflow / reflect)
+  bool flagged_prev = true;  // CTA-uniform: a cell of row j - 1 is shock-flagged
+
+  const int jb = y0 - 1, je = y1;
+  int sj = ((jb % G::NBUF) + G::NBUF) % G::NBUF;  // the ring slot of row j
+  auto ringk = [&](int k) -> float* {
+    int sl = sj + k;
+    sl = sl >= G::NBUF ? sl - G::NBUF : sl;
+    sl = sl < 0 ? sl + G::NBUF : sl;
+    return sW + sl * WC * WX;
+  };
+  for (int r = jb - ZH; r <= jb - 1 + ZH; r++) {
+    int sl = ((r % G::NBUF) + G::NBUF) % G::NBUF;
+    load_w_row<RECON>(P, u1, u2, x0, r, sW + sl * WC * WX);
+  }
+  // PPM along y: slopes carried up the march (ys_m, ys_0 at rows j - 1 and j)
+  constexpr bool YCARRY = RECON == R_PPM;
+  float ys_m[6], ys_0[6];
+  bool ys_ready = false;
+  for (int j = jb; j <= je; j++, sj = (sj + 1 == G::NBUF) ? 0 : sj + 1) {
+    load_w_row<RECON>(P, u1, u2, x0, j + ZH, ringk(ZH));
+    __syncthreads();
+    const float* sWj = ringk(0);
+    if constexpr (YCARRY) {
+      if (!ys_ready) {
+        float c2[6], c1[6], a0[6], b1[6];
+        read_row<RECON>(ringk(-2), wx, c2);
+        read_row<RECON>(ringk(-1), wx, c1);
+        read_row<RECON>(sWj, wx, a0);
+        read_row<RECON>(ringk(1), wx, b1);
+#pragma unroll
+        for (int v = 0; v < 6; v++) {
+          ys_m[v] = ppm_slope(c2[v], c1[v], a0[v]);
+          ys_0[v] = ppm_slope(c1[v], a0[v], b1[v]);
+        }
+        ys_ready = true;
+      }
+    }
+    auto y_edges = [&](const float* m, const float* c, const float* p, float* su_y, float* sd_y) {
+      float p2v[6];
+      read_row<RECON>(ringk(2), wx, p2v);
+#pragma unroll
+      for (int v = 0; v < 6; v++) {
+        const float yp = ppm_slope(c[v], p[v], p2v[v]);
+        ppm_incs_d(m[v], c[v], p[v], ys_m[v], ys_0[v], yp, su_y[v], sd_y[v]);
+        ys_m[v] = ys_0[v];
+        ys_0[v] = yp;
+      }
+    };
+
+    // The y ghost rows (outflow / reflect): their edges toward the domain at the ghost position;
+    // their half step is that of the adjacent inner row.
+    const bool yg_lo = j == -1 && bc_inner(P.bc_lo[1]);
+    const bool yg_hi = j == ny && bc_inner(P.bc_hi[1]);
+    if (yg_lo || yg_hi) {
+      float c[7], m[7], p[7], m2[7], p2[7], su[6], sd[6];
+      read_row<RECON>(sWj, wx, c);
+      with_cs(c, P);
+      read_row<RECON>(ringk(-1), wx, m);
+      read_row<RECON>(ringk(1), wx, p);
+      if constexpr (YCARRY) {
+        (void)m2;
+        (void)p2;
+        y_edges(m, c, p, su, sd);
+      } else {
+        axis_edges<RECON, ISEN>(m2, m, c, p, p2, P.inv_gamma, su, sd);
+      }
+      if (yg_lo) {
+#pragma unroll
+        for (int v = 0; v < 6; v++) gsu[v] = su[v];
+        flagged_prev = false;  // row 0's faces see row 0's flags only
+      } else if (col_t) {
+        Pred g;
+#pragma unroll
+        for (int v = 0; v < 6; v++) g.q[v] = q_prev[v];
+        if (P.bc_hi[1] == 2) g.q[2] = -g.q[2];
+        g.flag = flag_prev;
+        g.fo = fo_prev;
+        float ylo[7], Fy[8];
+        face_state(g, sd, -1.f, ylo);
+        riemann<1>(yhi_prev, ylo, P, Fy, flagged_prev);
+#pragma unroll
+        for (int v = 0; v < 8; v++) acc[v] -= Fy[v];
+        const size_t o = (size_t)(j - 1) * nx + gx;
+        float4 na, nb;
+        update_cell(__ldg(u1 + o), __ldg(u2 + o), acc, ph_prev, dtdx, P, na, nb);
+        o1[o] = na;
+        o2[o] = nb;
+        rate_max = fmaxf(rate_max, rate_guard(signal_rate(na, nb, P)));
+      }
+      continue;
+    }
+
+    // predictor at row j
+    float c[7];
+    read_row<RECON>(sWj, wx, c);
+    with_cs(c, P);
+    float su[2][6], sd[2][6];
+    float conv = 0.f, jump = -INFINITY;
+    {
+      float m[7], p[7], m2[7], p2[7];
+      read_row<RECON>(sWj, wx - 1, m);
+      read_row<RECON>(sWj, wx + 1, p);
+      if constexpr (RECON == R_PPM) {
+        read_row<RECON>(sWj, wx - 2, m2);
+        read_row<RECON>(sWj, wx + 2, p2);
+      }
+      axis_edges<RECON, ISEN>(m2, m, c, p, p2, P.inv_gamma, su[0], sd[0]);
+      conv += p[1] - m[1];
+      jump = fmaxf(jump, jump_excess(m[4], p[4], P.shock_thresh));
+      read_row<RECON>(ringk(-1), wx, m);
+      read_row<RECON>(ringk(1), wx, p);
+      if constexpr (YCARRY) {
+        y_edges(m, c, p, su[1], sd[1]);
+      } else {
+        axis_edges<RECON, ISEN>(m2, m, c, p, p2, P.inv_gamma, su[1], sd[1]);
+      }
+      conv += p[2] - m[2];
+      jump = fmaxf(jump, jump_excess(m[4], p[4], P.shock_thresh));
+    }
+    Pred pr;
+    hancock<2>(c, conv, jump, su, sd, h, P, pr);
+
+    const bool row_plane = j >= y0 && j < y1;
+    if (xg && row_plane) {
+      sFlux[tid] = make_float4(pr.q[0], pr.q[1], pr.q[2], pr.q[3]);
+      sFlux[PX + tid] = make_float4(pr.q[4], pr.q[5], pr.flag, pr.fo ? 1.f : 0.f);
+      __syncthreads();
+      if (g_src >= 0) {
+        const float4 a = sFlux[g_src], b = sFlux[PX + g_src];
+        pr.q[0] = a.x;
+        pr.q[1] = a.y;
+        pr.q[2] = a.z;
+        pr.q[3] = a.w;
+        pr.q[4] = b.x;
+        pr.q[5] = b.y;
+        pr.flag = b.z;
+        pr.fo = b.w != 0.f;
+        if (g_flip) pr.q[1] = -pr.q[1];
+      }
+    }
+    // row 0 stands in for the lower y ghost: its face state toward row 0
+    if (j == 0 && bc_inner(P.bc_lo[1])) {
+      Pred g = pr;
+      if (P.bc_lo[1] == 2) g.q[2] = -g.q[2];
+      face_state(g, gsu, 1.f, yhi_prev);
+    }
+    if (row_plane) {
+      float f[7];
+      face_state(pr, su[0], 1.f, f);
+      sFace[tid] = make_float4(f[0], f[1], f[2], f[3]);
+      sFace[PX + tid] = make_float4(f[4], f[5], f[6], 0.f);
+    }
+    const bool flagged = __syncthreads_or(pr.flag != 0.f);
+    const bool hll_any = flagged || flagged_prev;
+    flagged_prev = flagged;
+
+    if (row_plane && xface_t) {
+      float L[7], R[7], F[8];
+      unpack7(sFace[tid - 1], sFace[PX + tid - 1], L);
+      face_state(pr, sd[0], -1.f, R);
+      riemann<0>(L, R, P, F, hll_any);
+      sFlux[tid] = make_float4(F[0], F[1], F[2], F[3]);
+      sFlux[PX + tid] = make_float4(F[4], F[5], F[6], F[7]);
+    }
+    float Fy[8];
+    if (col_t && j >= y0) {
+      float R[7];
+      face_state(pr, sd[1], -1.f, R);
+      riemann<1>(yhi_prev, R, P, Fy, hll_any);
+    }
+    __syncthreads();
+
+    if (col_t) {
+      if (j - 1 >= y0) {
+#pragma unroll
+        for (int v = 0; v < 8; v++) acc[v] -= Fy[v];
+        const size_t o = (size_t)(j - 1) * nx + gx;
+        float4 na, nb;
+        update_cell(__ldg(u1 + o), __ldg(u2 + o), acc, ph_prev, dtdx, P, na, nb);
+        o1[o] = na;
+        o2[o] = nb;
+        rate_max = fmaxf(rate_max, rate_guard(signal_rate(na, nb, P)));
+      }
+      if (row_plane) {
+        float xl[8], xu[8];
+        unpack8(sFlux[tid], sFlux[PX + tid], xl);
+        unpack8(sFlux[tid + 1], sFlux[PX + tid + 1], xu);
+#pragma unroll
+        for (int v = 0; v < 8; v++) {
+          float a = xl[v];
+          a -= xu[v];
+          a += Fy[v];
+          acc[v] = a;
+        }
+        ph_prev = pr.q[4];
+      }
+    }
+    face_state(pr, su[1], 1.f, yhi_prev);
+#pragma unroll
+    for (int v = 0; v < 6; v++) q_prev[v] = pr.q[v];
+    flag_prev = pr.flag;
+    fo_prev = pr.fo;
+  }
+  block_max_to<G::NT>(rate_max, sRed, rate_out);
+}
+
 // The signal-rate maximum of a state (the reference's rates pass, hydro/rates.wgsl, and its
 // reduction, gpu/reduce.wgsl): used for the first step after the state is set.
 __global__ void rate_kernel(const KParams P, const float4* __restrict__ u1, const float4* __restrict__ u2, size_t ncell,
@@ -768,14 +1086,51 @@ static cudaError_t launch_sweep_d(const KParams& P, int recon, bool isen, const 
   }
 }
 
+template <int RECON, bool ISEN>
+static cudaError_t launch_rows_t(const KParams& P, const float4* u1, const float4* u2, float4* o1, float4* o2,
+                                 const DevClock* clk, unsigned* rate_out, int rows, cudaStream_t s) {
+  using G = RowGeo<RECON>;
+  static_assert(G::SMEM_BYTES <= 48 * 1024, "the row march fits the default shared-memory limit");
+  dim3 grid((P.n[0] + G::TX - 1) / G::TX, (P.n[1] + rows - 1) / rows, 1);
+  sweep_rows_kernel<RECON, ISEN><<<grid, G::NT, G::SMEM_BYTES, s>>>(P, u1, u2, o1, o2, clk, rate_out, rows);
+  return cudaGetLastError();
+}
+
+template <int RECON>
+static cudaError_t launch_rows_r(const KParams& P, bool isen, const float4* u1, const float4* u2, float4* o1, float4* o2,
+                                 const DevClock* clk, unsigned* rate_out, int rows, cudaStream_t s) {
+  if constexpr (RECON == R_PPM) {
+    return launch_rows_t<RECON, false>(P, u1, u2, o1, o2, clk, rate_out, rows, s);
+  } else {
+    return isen ? launch_rows_t<RECON, true>(P, u1, u2, o1, o2, clk, rate_out, rows, s)
+                : launch_rows_t<RECON, false>(P, u1, u2, o1, o2, clk, rate_out, rows, s);
+  }
+}
+
+static cudaError_t launch_rows(const KParams& P, int recon, bool isen, const float4* u1, const float4* u2, float4* o1,
+                               float4* o2, const DevClock* clk, unsigned* rate_out, int rows, cudaStream_t s) {
+  switch (recon) {
+    case R_MINMOD: return launch_rows_r<R_MINMOD>(P, isen, u1, u2, o1, o2, clk, rate_out, rows, s);
+    case R_MC: return launch_rows_r<R_MC>(P, isen, u1, u2, o1, o2, clk, rate_out, rows, s);
+    case R_VANLEER: return launch_rows_r<R_VANLEER>(P, isen, u1, u2, o1, o2, clk, rate_out, rows, s);
+    case R_KOREN: return launch_rows_r<R_KOREN>(P, isen, u1, u2, o1, o2, clk, rate_out, rows, s);
+    case R_PPM: return launch_rows_r<R_PPM>(P, isen, u1, u2, o1, o2, clk, rate_out, rows, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
 cudaError_t launch_sweep(const KParams& P, int ndim, int recon, bool isen, const float4* u1, const float4* u2, float4* o1,
                          float4* o2, const DevClock* clk, unsigned* rate_out, cudaStream_t s, int tz,
                          const SweepMaps* maps, int* err) {
-  if (tz <= 0) tz = SWEEP_TZ_DEFAULT;
   switch (ndim) {
     case 1: return launch_sweep_d<1>(P, recon, isen, u1, u2, o1, o2, clk, rate_out, 1, nullptr, err, s);
-    case 2: return launch_sweep_d<2>(P, recon, isen, u1, u2, o1, o2, clk, rate_out, 1, nullptr, err, s);
-    case 3: return launch_sweep_d<3>(P, recon, isen, u1, u2, o1, o2, clk, rate_out, tz, maps, err, s);
+    case 2:
+      // tz > 0: the march along y with tz rows a CTA; else the tile form
+      return tz > 0 ? launch_rows(P, recon, isen, u1, u2, o1, o2, clk, rate_out, tz, s)
+                    : launch_sweep_d<2>(P, recon, isen, u1, u2, o1, o2, clk, rate_out, 1, nullptr, err, s);
+    case 3:
+      return launch_sweep_d<3>(P, recon, isen, u1, u2, o1, o2, clk, rate_out, tz > 0 ? tz : SWEEP_TZ_DEFAULT, maps,
+                               err, s);
     default: return cudaErrorInvalidValue;
   }
 }

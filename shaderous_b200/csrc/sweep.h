@@ -25,9 +25,10 @@ struct SweepMaps {
 bool encode_sweep_maps(SweepMaps* m, const float4* base1, const float4* base2, int nx, int ny, int planes, int zofs,
                        int recon);
 
-// tz: planes a CTA marches along z (3D; 0 for the default). Every tz gives the same state, with or
-// without maps (the staging path and the per-cell loads give the same primitives). err: the
-// kernel's error word (a bounded wait for a copy that ran out), or null.
+// tz: planes a CTA marches along z (3D; 0 for the default); in 2D, rows a CTA marches along y (the
+// row form), or 0 for the tile form. Every tz gives the same state, with or without maps (the
+// staging path and the per-cell loads give the same primitives). err: the kernel's error word (a
+// bounded wait for a copy that ran out), or null.
 constexpr int SWEEP_TZ_DEFAULT = 64;
 cudaError_t launch_sweep(const KParams& P, int ndim, int recon, bool isen, const float4* u1, const float4* u2, float4* o1,
                          float4* o2, const DevClock* clk, unsigned* rate_out, cudaStream_t s, int tz = 0,

@@ -146,10 +146,13 @@ int shz_tune_pin(int32_t kernel, int32_t variant, int32_t per_sm) {
   const bool ok = kernel == shz::tune::K_AMR_ASSEMBLE        ? variant <= 6
                   : kernel == shz::tune::K_AMR_ASSEMBLE_BINS ? (variant == 1 || variant == 3)
                                                              : variant == 0;
-  if (!ok || per_sm < 0 || per_sm > 32) return SHZ_E_CONFIG;
+  // (the uniform sweep's knob is its depth, given in per_sm)
+  const int most = kernel == shz::tune::K_UNIFORM_SWEEP ? 1024 : 32;
+  if (!ok || per_sm < 0 || per_sm > most) return SHZ_E_CONFIG;
   shz::tune::Choice c;
   c.variant = variant;
-  c.per_sm = per_sm;
+  if (kernel == shz::tune::K_UNIFORM_SWEEP) c.tz = per_sm;
+  else c.per_sm = per_sm;
   shz::tune::pin(kernel, &c);
   return 0;
 }

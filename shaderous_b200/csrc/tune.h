@@ -16,7 +16,7 @@ namespace shz {
 namespace tune {
 
 enum Kernel : int {
-  K_UNIFORM_SWEEP = 0,  // tz: planes a CTA marches along z (3D)
+  K_UNIFORM_SWEEP = 0,  // tz: planes a CTA marches along z (3D); 2D (>= 512 a side): rows along y
   K_AMR_ASSEMBLE = 1,   // variant: register budget (CTAs per SM the compiler plans for); per_sm: grid
   K_AMR_SWEEP = 2,      // per_sm: grid
   K_AMR_FINE_FLUX = 3,  // per_sm: grid

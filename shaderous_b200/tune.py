@@ -25,8 +25,10 @@ def reset() -> None:
 
 
 def pin(kernel: str, variant: int | None, per_sm: int = 0) -> None:
-    """Use this choice for every launch of an AMR kernel ("amr_assemble", "amr_sweep",
-    "amr_fine_flux") instead of the tuned one; ``variant=None`` unpins."""
+    """Use this choice for every launch of a kernel instead of the tuned one; ``variant=None``
+    unpins. AMR kernels ("amr_assemble", "amr_sweep", "amr_fine_flux", "amr_assemble_bins"): a
+    variant and CTAs per SM. "uniform_sweep": variant 0 and ``per_sm`` = its depth (z planes a
+    CTA marches in 3D; in 2D the rows it marches along y, 0 for the tile form)."""
     k = {v: n for n, v in KERNELS.items()}[kernel]
     rc = _abi.load().shz_tune_pin(k, -1 if variant is None else int(variant), int(per_sm))
     if rc != 0:
