@@ -566,13 +566,15 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, REC
 }
 
 // ---------------------------------------------------------------------------------------------
-// The 2D step as a march along y. A CTA owns a row segment of RTX cells and marches it up through
+// The 2D step as a march along y. A CTA owns a row segment of TX cells and marches it up through
 // `rows` rows, as the 3D sweep marches its columns along z: its threads are the segment's cells
 // plus one halo cell at each end, the primitives of the rows the predictor reads along y sit in a
-// ring of rows in shared memory, and the y face below a cell and the running flux sums stay in the
-// thread's registers. Against the 2D tile form (16 x 12 cells with a ring of halo cells) it runs
-// the predictor 1.02 times per cell instead of 1.31 and converts each row once; the arithmetic per
-// cell is the same functions in the same order, so both forms give the same state.
+// ring of rows in shared memory, the state of the row after the next is in flight into a staging
+// row (asynchronous copies, a row ahead of its conversion), and the y face below a cell and the
+// running flux sums stay in the thread's registers. Against the 2D tile form (16 x 12 cells with a
+// ring of halo cells) it runs the predictor 1.02 times per cell instead of 1.31 and converts each
+// row once. The arithmetic per cell is the same functions in the same order; the two kernels agree
+// to rounding (the compiler may contract a multiply and an add differently in each).
 template <int RECON>
 struct RowGeo {
   static constexpr int H = (RECON == R_PPM) ? 3 : 2;   // halo of a row of primitives
@@ -583,7 +585,9 @@ struct RowGeo {
   static constexpr int WX = TX + 2 * H;                // texels of a row of primitives
   static constexpr int WC = 6;
   static constexpr int NBUF = 2 * ZH + 1;
-  static constexpr size_t SMEM_FLOATS = (size_t)NBUF * WC * WX + (size_t)2 * 4 * PX + (size_t)2 * 4 * PX + 32;
+  // the ring, the x face states and fluxes, the staging row (u1 then u2 of WX texels), the reduction
+  static constexpr size_t STAGE_OFS = (size_t)NBUF * WC * WX + (size_t)2 * 4 * PX + (size_t)2 * 4 * PX;
+  static constexpr size_t SMEM_FLOATS = STAGE_OFS + (size_t)2 * 4 * WX + 32;
   static constexpr size_t SMEM_BYTES = SMEM_FLOATS * sizeof(float);
   static_assert((NBUF * WC * WX) % 4 == 0, "the face states start on a 16-byte boundary");
 };
@@ -632,7 +636,8 @@ __global__ void __launch_bounds__(RowGeo<RECON>::NT, 5)
   float* sW = smem;
   float4* sFace = reinterpret_cast<float4*>(sW + G::NBUF * WC * WX);  // upper x face states, 2 a thread
   float4* sFlux = sFace + 2 * PX;                                     // lower x face fluxes, 2 a thread
-  float* sRed = reinterpret_cast<float*>(sFlux + 2 * PX);
+  float4* sStage = reinterpret_cast<float4*>(smem + G::STAGE_OFS);  // the next row's state, in flight
+  float* sRed = smem + G::STAGE_OFS + 2 * 4 * WX;
 
   const int tid = threadIdx.x;
   const int x0 = blockIdx.x * G::TX;
@@ -691,12 +696,43 @@ __global__ void __launch_bounds__(RowGeo<RECON>::NT, 5)
     int sl = ((r % G::NBUF) + G::NBUF) % G::NBUF;
     load_w_row<RECON>(P, u1, u2, x0, r, sW + sl * WC * WX);
   }
+  // Row r's state into the staging row by asynchronous copies (each thread its own texels), a row
+  // ahead of its conversion, so that the loads are in flight during a row's work.
+  auto stage_row = [&](int r) {
+    float fy;
+    const int gy = bc_map(r, ny, P.bc_lo[1], P.bc_hi[1], fy);
+    for (int idx = tid; idx < WX; idx += G::NT) {
+      float fx;
+      const int gxx = bc_map(x0 - H + idx, nx, P.bc_lo[0], P.bc_hi[0], fx);
+      const size_t o = (size_t)gy * nx + gxx;
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(tma::smem_u32(sStage + idx)), "l"(u1 + o) : "memory");
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(tma::smem_u32(sStage + WX + idx)), "l"(u2 + o)
+                   : "memory");
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  // the staged row r (this thread's copies landed) converted into a ring slot
+  auto land_row = [&](int r, float* dst) {
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    float fy;
+    bc_map(r, ny, P.bc_lo[1], P.bc_hi[1], fy);
+    for (int idx = tid; idx < WX; idx += G::NT) {
+      float fx;
+      bc_map(x0 - H + idx, nx, P.bc_lo[0], P.bc_hi[0], fx);
+      float w[6];
+      prim6_from_cons(sStage[idx], sStage[WX + idx], P, fx, fy, 1.f, w);
+#pragma unroll
+      for (int c = 0; c < 3; c++) reinterpret_cast<float2*>(dst)[c * WX + idx] = make_float2(w[2 * c], w[2 * c + 1]);
+    }
+  };
+  stage_row(jb + ZH);
   // PPM along y: slopes carried up the march (ys_m, ys_0 at rows j - 1 and j)
   constexpr bool YCARRY = RECON == R_PPM;
   float ys_m[6], ys_0[6];
   bool ys_ready = false;
   for (int j = jb; j <= je; j++, sj = (sj + 1 == G::NBUF) ? 0 : sj + 1) {
-    load_w_row<RECON>(P, u1, u2, x0, j + ZH, ringk(ZH));
+    land_row(j + ZH, ringk(ZH));
+    if (j + 1 <= je) stage_row(j + 1 + ZH);
     __syncthreads();
     const float* sWj = ringk(0);
     if constexpr (YCARRY) {
