@@ -262,6 +262,42 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, REC
       tma::tile3d_g2s(smem + G::STAGE_OFS + G::STAGE_BOX, &tm2, 4 * (x0 - H), y0 - H, gz + zofs, &sBarU);
     }
   };
+  // Columns at an x or y face of the grid (whose region the tiled copy cannot map through the
+  // boundary) stage their planes too: each thread copies its own texels of the plane after the
+  // next into the staging area by asynchronous copies (cp.async, through the boundary mapping) and
+  // converts them a plane later, so that the loads are in flight during a plane's work.
+  auto stage_plane = [&](int pl) {
+    float fz = 1.f;
+    const bool zhalo = (pl < 0 && P.bc_lo[2] == BC_HALO) || (pl >= nz && P.bc_hi[2] == BC_HALO);
+    const int gz = zhalo ? pl : bc_map(pl, nz, P.bc_lo[2], P.bc_hi[2], fz);
+    stage_fz = fz;
+    const ptrdiff_t zoff = (ptrdiff_t)gz * ny * nx;
+    float4* s1 = reinterpret_cast<float4*>(smem + G::STAGE_OFS);
+    float4* s2 = reinterpret_cast<float4*>(smem + G::STAGE_OFS + G::STAGE_BOX);
+    for (int idx = tid; idx < WN; idx += G::NT) {
+      const int lx = idx % G::WX, ly = idx / G::WX;
+      float fx, fy;
+      const int sx = bc_map(x0 - H + lx, nx, P.bc_lo[0], P.bc_hi[0], fx);
+      const int sy = bc_map(y0 - H + ly, ny, P.bc_lo[1], P.bc_hi[1], fy);
+      const ptrdiff_t o = zoff + (ptrdiff_t)sy * nx + sx;
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(tma::smem_u32(s1 + idx)), "l"(u1 + o) : "memory");
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(tma::smem_u32(s2 + idx)), "l"(u2 + o) : "memory");
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  auto land_plane = [&](float* dst) {
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    for (int idx = tid; idx < WN; idx += G::NT) {
+      const int lx = idx % G::WX, ly = idx / G::WX;
+      float fx, fy;
+      bc_map(x0 - H + lx, nx, P.bc_lo[0], P.bc_hi[0], fx);
+      bc_map(y0 - H + ly, ny, P.bc_lo[1], P.bc_hi[1], fy);
+      float w[6];
+      prim6_from_cons(stage1[idx], stage2[idx], P, fx, fy, stage_fz, w);
+#pragma unroll
+      for (int c = 0; c < 3; c++) reinterpret_cast<float2*>(dst)[c * WN + idx] = make_float2(w[2 * c], w[2 * c + 1]);
+    }
+  };
   if constexpr (DIM == 3) {
     if (tma_tile) {
       if (tid == 0) {
@@ -273,6 +309,7 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, REC
     // the planes below the first that the predictor reads along z
     for (int pl = z0 - 1 - ZH; pl <= z0 - 2 + ZH; pl++) load_w_plane<DIM, RECON>(P, u1, u2, x0, y0, pl, ring(pl));
     if (tma_tile) issue_plane(z0 - 1 + ZH);
+    else stage_plane(z0 - 1 + ZH);
   }
 
   const int jb = (DIM == 3) ? z0 - 1 : 0;
@@ -312,8 +349,12 @@ __global__ void __launch_bounds__(Geo<DIM, RECON>::NT) __maxnreg__((Geo<DIM, REC
       __syncthreads();
       // the staging area is free again: the next plane's copy overlaps this plane's work
       if (j + 1 <= je) issue_plane(j + 1 + ZH);
+    } else if constexpr (DIM == 3) {
+      land_plane(ringk(ZH));
+      if (j + 1 <= je) stage_plane(j + 1 + ZH);
+      __syncthreads();
     } else {
-      load_w_plane<DIM, RECON>(P, u1, u2, x0, y0, lp, ringk((DIM == 3) ? ZH : 0));
+      load_w_plane<DIM, RECON>(P, u1, u2, x0, y0, lp, ringk(0));
       __syncthreads();
     }
     const float* sWj = ringk(0);
