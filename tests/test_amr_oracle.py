@@ -1,4 +1,4 @@
-"""The block-grid oracle (oracle/amr_ref.cpp) pinned on the CPU before it judges the GPU.
+"""The block-grid oracle (oracle/amr_ref.cpp) pinned on the CPU before it checks the GPU.
 
 - On a mesh with no refinement its step is the uniform-grid oracle's step (oracle/ref_hydro.cpp,
   itself pinned to the reference's own tests/unit/reference.test.ts), to float64 rounding, for
