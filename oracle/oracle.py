@@ -75,6 +75,14 @@ def limiter(kind: str, a: float, b: float, scale: float = 0.0) -> float:
     return load().orc_limiter(RECON[kind], a, b, scale)
 
 
+def ppm_edges(a2m: float, am: float, a: float, ap: float, a2p: float) -> tuple[float, float]:
+    """The parabola's lower and upper edge values of the middle cell of five (Colella & Woodward
+    1984, eqs. 1.6, 1.8 and 1.10): the oracle's PPM, which has no reference counterpart."""
+    lo, hi = C.c_double(), C.c_double()
+    load().orc_ppm_edges(a2m, am, a, ap, a2p, C.byref(lo), C.byref(hi))
+    return lo.value, hi.value
+
+
 def exact_riemann(left, right, gamma: float, xi) -> np.ndarray:
     """riemann_exact.ts exactRiemann(L, R, gamma)(xi) for each xi: rows (rho, u, p)."""
     xi = np.ascontiguousarray(np.atleast_1d(xi), dtype=np.float64)
