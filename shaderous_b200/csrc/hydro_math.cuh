@@ -70,6 +70,35 @@ __device__ __forceinline__ float limit(float a, float b, float scale) {
   }
 }
 
+// Both of a cell's edge increments at once, lim(a, b) toward the upper face and lim(b, a) from the
+// lower one. Koren's smoothness measure (far^2 + near^2) / scale^2 and its weight are symmetric in
+// the two differences, as the reference computes them in float64: formed once for the pair (a
+// single rounding order, where forming it per call let a fused multiply-add round the two orders
+// apart), as are the sign test and the twice-the-smaller bound. Other limiters: two calls.
+template <int R>
+__device__ __forceinline__ void limit_pair(float a, float b, float scale, float& up, float& dn) {
+  if constexpr (R != R_KOREN) {
+    up = limit<R>(a, b, scale);
+    dn = limit<R>(b, a, scale);
+  } else {
+    const float fu = (a + 2.f * b) * (1.f / 3.f), fd = (b + 2.f * a) * (1.f / 3.f);
+    const bool same = same_sign(a, b);
+    const float m2 = fminf(2.f * fabsf(a), 2.f * fabsf(b));
+    const float lu = same ? copysignf(fminf(m2, fabsf(fu)), b) : 0.f;
+    const float ld = same ? copysignf(fminf(m2, fabsf(fd)), a) : 0.f;
+    const float s = 0.01f * scale;
+    const float s2 = s * s;
+    const bool as_is = ((s2 >= 1e-30f) & (s2 < 1e30f)) | (s == 0.f);
+    const float eta_as_is = (a * a + b * b) / fmaxf(s2, 1e-30f);
+    const float k = 1.f / fabsf(s);
+    const float eta_scaled = (a * k) * (a * k) + (b * k) * (b * k);
+    const float eta = as_is ? eta_as_is : eta_scaled;
+    const float w = fminf(fmaxf(1.5f - eta, 0.f), 1.f);
+    up = lu + (fu - lu) * w;
+    dn = ld + (fd - ld) * w;
+  }
+}
+
 // The limiters whose edge increment is the same slope at both faces (lim(a, b) == lim(b, a)).
 template <int R>
 __host__ __device__ constexpr bool symmetric_limiter() { return R == R_MINMOD || R == R_MC || R == R_VANLEER; }
@@ -78,7 +107,7 @@ __host__ __device__ constexpr bool symmetric_limiter() { return R == R_MINMOD ||
 // increments toward the face (up) and from the lower face (dn) toward those along the adiabat,
 // by the shared bound at most. m, c, p: (rho, vx, vy, vz, p, s, cs) of the lower neighbour, the
 // cell and the upper neighbour; pu, pd: the cell's pressure increments at the two faces.
-template <int R>
+template <int R, bool PAIR = true>
 __device__ __forceinline__ void isen_blend(const float* m, const float* c, const float* p, float pu, float pd,
                                            float inv_gamma, float& up, float& dn) {
   const float rl = m[0], pl = m[4], rc = c[0], pc = c[4], rr = p[0], pr = p[4];
@@ -94,15 +123,22 @@ __device__ __forceinline__ void isen_blend(const float* m, const float* c, const
   const float dvl = sqrtf((c[1] - m[1]) * (c[1] - m[1]) + (c[2] - m[2]) * (c[2] - m[2]) + (c[3] - m[3]) * (c[3] - m[3]));
   const float fade_v = fminf(fmaxf(2.f - fmaxf(dvr, dvl) / (0.1f * fmaxf(c[6], 1e-30f)), 0.f), 1.f);
   const float bound = fmaxf(0.25f * fminf(fabsf(rc - rl), fabsf(rr - rc)), 0.01f * rc * fade_s * fade_a * fade_v);
+  float d_up, d_dn;
+  if constexpr (PAIR) {
+    limit_pair<R>(-tl, tr, rc, d_up, d_dn);
+  } else {
+    d_up = limit<R>(-tl, tr, rc);
+    d_dn = limit<R>(tr, -tl, rc);
+  }
   {
-    const float d = limit<R>(-tl, tr, rc);
+    const float d = d_up;
     const float pf = pc + 0.5f * pu;
     const float rf = fminf(fmaxf((rc + 0.5f * d) * powf(fmaxf(pf, 1e-30f) / pc, gi), fminf(rc, rr)), fmaxf(rc, rr));
     const float inc = 2.f * (rf - rc);
     up += ok ? fminf(fmaxf(inc - up, -bound), bound) : 0.f;
   }
   {
-    const float d = limit<R>(tr, -tl, rc);
+    const float d = d_dn;
     const float pf = pc - 0.5f * pd;
     const float rf = fminf(fmaxf((rc - 0.5f * d) * powf(fmaxf(pf, 1e-30f) / pc, gi), fminf(rc, rl)), fmaxf(rc, rl));
     const float inc = -2.f * (rf - rc);
@@ -147,8 +183,10 @@ __device__ __forceinline__ void ppm_incs(float a2m, float am, float a, float ap,
 
 // The edge increments of one cell along one axis (hydro.ts:282-293; the ghost form :347-356):
 // su toward the upper face, sd from the lower face, for (rho, vx, vy, vz, p, s).
-// m2, p2 (two cells away) are read by PPM only.
-template <int R, bool ISEN>
+// m2, p2 (two cells away) are read by PPM only. PAIR (Koren): a cell's two increments formed as a
+// pair (limit_pair) rather than by two calls; the 2D row march keeps two calls, which its register
+// budget schedules better.
+template <int R, bool ISEN, bool PAIR = true>
 __device__ __forceinline__ void axis_edges(const float* m2, const float* m, const float* c, const float* p, const float* p2,
                                            float inv_gamma, float* su, float* sd) {
   if constexpr (R == R_PPM) {
@@ -159,10 +197,17 @@ __device__ __forceinline__ void axis_edges(const float* m2, const float* m, cons
     const float sc[6] = {c[0], c[6], c[6], c[6], c[4], 0.f};
 #pragma unroll
     for (int v = 0; v < 6; v++) {
-      su[v] = limit<R>(c[v] - m[v], p[v] - c[v], sc[v]);
-      sd[v] = symmetric_limiter<R>() ? su[v] : limit<R>(p[v] - c[v], c[v] - m[v], sc[v]);
+      if constexpr (symmetric_limiter<R>()) {
+        su[v] = limit<R>(c[v] - m[v], p[v] - c[v], sc[v]);
+        sd[v] = su[v];
+      } else if constexpr (PAIR) {
+        limit_pair<R>(c[v] - m[v], p[v] - c[v], sc[v], su[v], sd[v]);
+      } else {
+        su[v] = limit<R>(c[v] - m[v], p[v] - c[v], sc[v]);
+        sd[v] = limit<R>(p[v] - c[v], c[v] - m[v], sc[v]);
+      }
     }
-    if constexpr (ISEN) isen_blend<R>(m, c, p, su[4], sd[4], inv_gamma, su[0], sd[0]);
+    if constexpr (ISEN) isen_blend<R, PAIR>(m, c, p, su[4], sd[4], inv_gamma, su[0], sd[0]);
   }
 }
 

@@ -818,7 +818,7 @@ __global__ void __launch_bounds__(RowGeo<RECON>::NT, 5)
         (void)p2;
         y_edges(m, c, p, su, sd);
       } else {
-        axis_edges<RECON, ISEN>(m2, m, c, p, p2, P.inv_gamma, su, sd);
+        axis_edges<RECON, ISEN, false>(m2, m, c, p, p2, P.inv_gamma, su, sd);
       }
       if (yg_lo) {
 #pragma unroll
@@ -860,7 +860,7 @@ __global__ void __launch_bounds__(RowGeo<RECON>::NT, 5)
         read_row<RECON>(sWj, wx - 2, m2);
         read_row<RECON>(sWj, wx + 2, p2);
       }
-      axis_edges<RECON, ISEN>(m2, m, c, p, p2, P.inv_gamma, su[0], sd[0]);
+      axis_edges<RECON, ISEN, false>(m2, m, c, p, p2, P.inv_gamma, su[0], sd[0]);
       conv += p[1] - m[1];
       jump = fmaxf(jump, jump_excess(m[4], p[4], P.shock_thresh));
       read_row<RECON>(ringk(-1), wx, m);
@@ -868,7 +868,7 @@ __global__ void __launch_bounds__(RowGeo<RECON>::NT, 5)
       if constexpr (YCARRY) {
         y_edges(m, c, p, su[1], sd[1]);
       } else {
-        axis_edges<RECON, ISEN>(m2, m, c, p, p2, P.inv_gamma, su[1], sd[1]);
+        axis_edges<RECON, ISEN, false>(m2, m, c, p, p2, P.inv_gamma, su[1], sd[1]);
       }
       conv += p[2] - m[2];
       jump = fmaxf(jump, jump_excess(m[4], p[4], P.shock_thresh));
